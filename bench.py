@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Throughput of population fitness evaluation on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one step = one generation's evaluation of the whole population):
+2^20 seeded random LGP programs, lengths U[16,256] with ~40% introns by
+construction, 5 input features U[-3,3], 4,096 fitness cases, target = a
+seeded random 16-effective-instruction program + N(0, 0.01^2); reference ISA,
+16 registers.  Synthetic data of the reference's shapes (no datasets ship).
+
+Metric: GPop/s = (effective instructions x fitness cases) / second, whole job.
+``value``: population resident in HBM when the clock starts (intron pre-pass,
+interpreter and fitness reduction on the device).  ``e2e``: the same through
+the host-pointer C call (galop_evaluate_csr): H2D of the raw population from
+pinned memory, pre-pass, interpretation, D2H of fitness, every step.
+
+Multi-GPU (torchrun, one rank per GPU): every rank evaluates its own
+population of the same size on the shared dataset (programs are independent,
+so there is no collective on the data path; torch.distributed is used only for
+the barrier and the max-over-ranks of the timings).  ``--impl reference``
+times the reference's own CPU evaluator (Evaluator::evaluate_sr_mse built from
+its sources, OpenMP over programs on every host core) on a bounded sample of
+the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "GPop/s (eff. instr x cases/s) vs FP32-issue roofline; p50/p99 eval latency"
+UNIT = "GPop/s"
+WORKLOAD = ("single generation: 2^20 random programs, L~U[16,256] (~40% introns by construction), "
+            "5 features U[-3,3], 4096 cases, target = random 16-effective-instruction program + N(0,0.01^2), "
+            "reference ISA with 16 registers")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--programs", type=int, default=1 << 20)
+    ap.add_argument("--cases", type=int, default=4096)
+    ap.add_argument("--cases-per-lane", type=int, default=0)
+    ap.add_argument("--warps-per-block", type=int, default=0)
+    ap.add_argument("--reduce", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+class Dist:
+    """torch.distributed plumbing (barrier, max) when launched by torchrun."""
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.torch, self.dist = torch, dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier(device_ids=[self.local])
+
+    def max(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(", ") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower().startswith("active"):
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_workload(n_programs: int, n_cases: int, seed: int):
+    from galop_b200 import workloads as W
+    return W.single_generation(seed=seed, n_programs=n_programs, n_cases=n_cases)
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {}
+
+
+def profile_traffic():
+    """DRAM bytes per interpreter launch from the committed ncu summary."""
+    p = ROOT / "profiles" / "interp_single_generation.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("dram_bytes_per_launch_full")
+        except (ValueError, OSError):
+            return None
+    return None
+
+
+def cpu_reference_rate(wl, seconds: float, threads: int):
+    """The reference's CPU evaluator (libref_nr16: Evaluator::evaluate_sr_mse
+    + mse_to_fitness, OpenMP over programs) on successive batches of the
+    workload until `seconds` of wall time; effective-instruction GPop/s."""
+    from oracle.oracle import Oracle, RefLib
+    kind = "reference"
+    try:
+        ref = RefLib("nr16")
+        evaluate = lambda w, o: ref.evaluate_csr(w, o, wl.X, wl.y, threads=threads)  # noqa: E731
+    except (FileNotFoundError, OSError):
+        kind = "port"
+        orc = Oracle(0, 16)
+        evaluate = lambda w, o: orc.evaluate_csr(w, o, wl.X, wl.y, threads=threads)  # noqa: E731
+    orc = Oracle(0, 16)
+    batch = 256
+    done_progs, ops, t_total = 0, 0.0, 0.0
+    start = 0
+    while t_total < seconds:
+        if start >= wl.n_programs:
+            start = 0
+        idx = np.arange(start, min(start + batch, wl.n_programs))
+        sub = wl.subsample(idx)
+        eff = orc.effective_lengths(sub.words, sub.offsets)
+        t0 = time.perf_counter()
+        evaluate(sub.words, sub.offsets)
+        t_total += time.perf_counter() - t0
+        ops += float(eff.sum()) * wl.n_cases
+        done_progs += idx.size
+        start += batch
+    rate = ops / t_total / 1e9
+    return rate, kind, done_progs, t_total
+
+
+def run_reference(args, dist: Dist):
+    if dist.rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    wl = load_workload(min(args.programs, 16384), args.cases, 2)
+    per_step = max(2.0, args.cpu_seconds / max(args.steps, 1))
+    for _ in range(max(args.warmup, 0)):
+        cpu_reference_rate(wl, 0.5, threads)
+    rates, secs, progs = [], [], 0
+    kind = "reference"
+    for _ in range(args.steps):
+        r, kind, n, t = cpu_reference_rate(wl, per_step, threads)
+        rates.append(r)
+        secs.append(t)
+        progs = n
+    value = float(np.mean(rates))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(secs)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "programs_per_step": progs, "cases": args.cases,
+                   "sample": f"first {progs} programs of the same workload per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{progs} programs x {args.cases} cases per step, ~{per_step:.0f} s each"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, dist: Dist):
+    import galop_b200 as g
+
+    wl = load_workload(args.programs, args.cases, 2 + dist.rank)
+    ds = g.Dataset(wl.X, wl.y)
+    ev = g.Evaluator(num_registers=16, device=dist.local if dist.world > 1 else 0, reduce=args.reduce,
+                     cases_per_lane=args.cases_per_lane, warps_per_block=args.warps_per_block)
+    ev.set_dataset(ds)
+    n = wl.n_programs
+    words = np.ascontiguousarray(wl.words)
+    offsets = np.ascontiguousarray(wl.offsets)
+
+    # ---- device-resident population: the `value` leg -------------------------
+    d_words = ev.device_alloc(words.nbytes)
+    d_off = ev.device_alloc(offsets.nbytes)
+    d_fit = ev.device_alloc(4 * n)
+    d_sse = ev.device_alloc(8 * n)
+    ev.h2d(d_words, words)
+    ev.h2d(d_off, offsets)
+
+    def step_device():
+        ev.evaluate_csr_device(d_words, d_off, n, d_fit, d_sse)
+        ev.synchronize()
+        st = ev.stats
+        return st
+
+    for _ in range(args.warmup):
+        step_device()
+    # counts of one evaluation (identical every step)
+    fit_check = ev.evaluate_csr(words, offsets)
+    st0 = ev.stats
+    eff_instr, raw_instr = st0.eff_instructions, st0.raw_instructions
+
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    ev.synchronize()
+    clocks.start()
+    ev.timer_record(0)
+    interp_ms, launches = [], 0
+    for _ in range(args.steps):
+        st = step_device()
+        interp_ms.append(st.interp_ms)
+        launches += st.kernels_launched
+    ev.timer_record(1)
+    ms_total = ev.timer_elapsed(0, 1)
+    clock = clocks.stop()
+    dist.barrier()
+    ms_total_max = dist.max(ms_total)
+    ops_rank = float(eff_instr) * wl.n_cases * args.steps
+    ops_all = dist.sum(ops_rank)
+    value = ops_all / (ms_total_max / 1e3) / 1e9
+
+    # ---- end to end through the host-pointer C call ---------------------------
+    pin_w = g.PinnedArray(words.shape, np.uint32)
+    pin_o = g.PinnedArray(offsets.shape, np.int64)
+    pin_f = g.PinnedArray((n,), np.float32)
+    pin_w.array[:] = words
+    pin_o.array[:] = offsets
+    ev.evaluate_csr(pin_w.array, pin_o.array, fitness_out=pin_f.array)   # warm the host path
+    dist.barrier()
+    ev.synchronize()
+    ev.timer_record(2)
+    e2e_launches = 0
+    for _ in range(args.steps):
+        ev.evaluate_csr(pin_w.array, pin_o.array, fitness_out=pin_f.array)
+        e2e_launches += ev.stats.kernels_launched
+    ev.timer_record(3)
+    e2e_ms = dist.max(ev.timer_elapsed(2, 3))
+    e2e_value = ops_all / (e2e_ms / 1e3) / 1e9
+    assert np.array_equal(pin_f.array.view(np.uint32), fit_check.view(np.uint32))
+
+    # ---- roofline of the interpreter (FP32 issue) -------------------------------
+    peaks = measured_peaks()
+    sm_count = 148
+    try:
+        import ctypes
+        cudart = ctypes.CDLL("libcudart.so")
+        v = ctypes.c_int()
+        if cudart.cudaDeviceGetAttribute(ctypes.byref(v), 16, dist.local if dist.world > 1 else 0) == 0:
+            sm_count = v.value
+    except OSError:
+        pass
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    peak_gops = sm_count * 128 * sm_max * 1e6 / 1e9
+    interp_avg_ms = float(np.mean(interp_ms))
+    achieved = eff_instr * wl.n_cases / (interp_avg_ms / 1e3) / 1e9
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, kind, progs, secs = cpu_reference_rate(wl, args.cpu_seconds, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"first {progs} programs of the workload x {wl.n_cases} cases ({secs:.1f} s wall, "
+                         f"OpenMP over programs)"}
+
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "programs_per_gpu": n, "cases": wl.n_cases,
+                       "raw_instructions_per_gpu": raw_instr, "effective_instructions_per_gpu": eff_instr,
+                       "cases_per_lane": st0.cases_per_lane, "warps_per_block": st0.warps_per_block,
+                       "reduce": ["kahan32", "fp64", "ordered"][args.reduce],
+                       "l2": "inputs larger than L2 (raw population %.2f GB per GPU)" % (words.nbytes / 1e9),
+                       "parallelism": f"programs sharded, {dist.world} rank(s), no data-path collective"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(words.nbytes + offsets.nbytes),
+                    "d2h_bytes_per_step": int(4 * n), "ms_per_step": e2e_ms / args.steps},
+            "gpu_launches": launches,
+            "raw_gpops": value * raw_instr / max(eff_instr, 1),
+            "roofline": {"bound": "fp32_issue", "achieved": achieved, "peak": peak_gops, "unit": UNIT,
+                         "frac": achieved / peak_gops, "traffic": profile_traffic(),
+                         "kernel": "interp_kernel", "kernel_ms": interp_avg_ms,
+                         "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {sm_max:.0f} MHz "
+                                        f"(sm_max_mhz of MEASURED_PEAKS.json)"},
+            "clocks": clock,
+            "latency_ms": {"p50": float(np.percentile(interp_ms, 50)), "p99": float(np.percentile(interp_ms, 99))},
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    for d in (d_words, d_off, d_fit, d_sse):
+        ev.device_free(d)
+    pin_w.free()
+    pin_o.free()
+    pin_f.free()
+    ev.close()
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist)
+        else:
+            run_b200(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

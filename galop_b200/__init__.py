@@ -1,0 +1,402 @@
+"""galop_b200 -- B200 fitness evaluator for Galop's linear-GP symbolic regression.
+
+Python view of the C ABI in ``include/galop_b200.h`` (ctypes, numpy arrays,
+no torch).  ``Evaluator`` mirrors the reference's evaluation backend:
+
+* ``Evaluator.evaluate_population(instructions, lengths, fitness_out,
+  n_programs, dataset)`` has the argument order and meaning of
+  ``EvalBackend::evaluate_population`` (src/EvalBackend.h:11-17): program ``i``
+  is ``instructions[i*stride : i*stride + lengths[i]]`` with ``stride`` the
+  engine's MAX_PROGRAM_SIZE.
+* ``Evaluator.evaluate_csr(words, offsets)`` takes the packed layout of
+  ``evaluate_kernel_packed`` (src/eval_kernels.cuh:292-303).
+* ``Dataset`` mirrors ``struct Dataset`` (src/Dataset.h:22-38): case-major
+  inputs, targets, ``N``, ``num_inputs``, ``ss_tot``.
+
+Errors raise ``GalopError`` carrying the library's status code and message
+(the reference prints and calls ``exit``, src/cuda_errors.h:3-15).  The native
+library must be present: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libgalop_b200.so"
+
+PROFILE_REF, PROFILE_BJ = 0, 1
+REDUCE_KAHAN32, REDUCE_FP64, REDUCE_ORDERED = 0, 1, 2
+
+OK = 0
+E_INVALID, E_CUDA, E_NOMEM, E_NO_DATASET, E_TIMEOUT, E_CAPACITY, E_NO_DEVICE, E_STATE = (
+    -1, -2, -3, -4, -5, -6, -7, -8)
+
+# The reference's constant pools (src/LGPConfig.h:159-168).
+REF_CONSTANTS_8 = np.array([0.0, 1.0, -1.0, 3.14159, 0.5, 2.0, 10.0, 100.0], dtype=np.float32)
+REF_CONSTANTS_16 = np.array([0.0, 1.0, -1.0, 3.14159, 0.5, 2.0, 10.0, 100.0,
+                             0.1, -0.5, 0.25, 5.0, 20.0, -2.0, 0.01, 1000.0], dtype=np.float32)
+
+# Every entry point that include/galop_b200.h declares.
+EXPORTED = (
+    "galop_options_init", "galop_create", "galop_destroy", "galop_last_error",
+    "galop_status_string", "galop_abi_version", "galop_set_dataset", "galop_set_dataset_device",
+    "galop_evaluate_population", "galop_evaluate_csr", "galop_evaluate_csr_device",
+    "galop_case_outputs_csr", "galop_trace_program", "galop_effective_csr", "galop_last_stats",
+    "galop_synchronize", "galop_host_alloc", "galop_host_free", "galop_device_alloc",
+    "galop_device_free", "galop_memcpy_h2d", "galop_memcpy_d2h", "galop_timer_record",
+    "galop_timer_elapsed",
+)
+
+
+class _Options(C.Structure):
+    _fields_ = [
+        ("profile", C.c_int32), ("num_registers", C.c_int32), ("input_protect", C.c_int32),
+        ("reduce", C.c_int32), ("constants", C.POINTER(C.c_float)), ("device", C.c_int32),
+        ("intron_prepass", C.c_int32), ("cases_per_lane", C.c_int32),
+        ("warps_per_block", C.c_int32), ("reserved", C.c_int32 * 4),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("n_programs", C.c_int64), ("n_cases", C.c_int64), ("raw_instructions", C.c_int64),
+        ("eff_instructions", C.c_int64), ("h2d_ms", C.c_double), ("prepass_ms", C.c_double),
+        ("interp_ms", C.c_double), ("finalize_ms", C.c_double), ("d2h_ms", C.c_double),
+        ("total_ms", C.c_double), ("cases_per_lane", C.c_int32), ("warps_per_block", C.c_int32),
+        ("blocks", C.c_int32), ("case_chunks", C.c_int32), ("kernels_launched", C.c_int32),
+        ("reserved", C.c_int32 * 3),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
+class GalopError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"galop status {status}: {message}")
+        self.status = status
+
+
+_lib: Optional[C.CDLL] = None
+
+_P = C.c_void_p
+_U32P = C.POINTER(C.c_uint32)
+_I64P = C.POINTER(C.c_int64)
+_F32P = C.POINTER(C.c_float)
+_F64P = C.POINTER(C.c_double)
+_U8P = C.POINTER(C.c_uint8)
+
+
+def load_library(path: Optional[Path] = None) -> C.CDLL:
+    """Load libgalop_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise GalopError(E_NO_DEVICE, f"native library missing: {p} (run python -m galop_b200.build)")
+    lib = C.CDLL(str(p))
+    sig = {
+        "galop_options_init": (C.c_int, [C.POINTER(_Options)]),
+        "galop_create": (C.c_int, [C.POINTER(_Options), C.POINTER(_P)]),
+        "galop_destroy": (None, [_P]),
+        "galop_last_error": (C.c_char_p, [_P]),
+        "galop_status_string": (C.c_char_p, [C.c_int]),
+        "galop_abi_version": (C.c_int, []),
+        "galop_set_dataset": (C.c_int, [_P, _F32P, _F32P, C.c_int64, C.c_int32]),
+        "galop_set_dataset_device": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32]),
+        "galop_evaluate_population": (C.c_int, [_P, _U32P, _U8P, C.c_int64, C.c_int64, _F32P]),
+        "galop_evaluate_csr": (C.c_int, [_P, _U32P, _I64P, C.c_int64, _F32P, _F64P]),
+        "galop_evaluate_csr_device": (C.c_int, [_P, _P, _P, C.c_int64, _P, _P, _P]),
+        "galop_case_outputs_csr": (C.c_int, [_P, _U32P, _I64P, C.c_int64, _F32P]),
+        "galop_trace_program": (C.c_int, [_P, _U32P, C.c_int64, _F32P, _I64P]),
+        "galop_effective_csr": (C.c_int, [_P, _U32P, _I64P, C.c_int64, _I64P, _U32P]),
+        "galop_last_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+        "galop_synchronize": (C.c_int, [_P]),
+        "galop_host_alloc": (C.c_int, [C.c_int64, C.POINTER(_P)]),
+        "galop_host_free": (C.c_int, [_P]),
+        "galop_device_alloc": (C.c_int, [_P, C.c_int64, C.POINTER(_P)]),
+        "galop_device_free": (C.c_int, [_P, _P]),
+        "galop_memcpy_h2d": (C.c_int, [_P, _P, _P, C.c_int64]),
+        "galop_memcpy_d2h": (C.c_int, [_P, _P, _P, C.c_int64]),
+        "galop_timer_record": (C.c_int, [_P, C.c_int32]),
+        "galop_timer_elapsed": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _ptr(a: Optional[np.ndarray], ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def status_string(status: int) -> str:
+    return load_library().galop_status_string(status).decode()
+
+
+@dataclass
+class Dataset:
+    """Mirror of the reference's Dataset (src/Dataset.h:22-38).
+
+    ``inputs`` is case-major ``(N, num_inputs)`` float32 (the reference pads the
+    row count to a multiple of 32; padding rows are never evaluated, so they
+    are not stored here); ``targets`` is ``(N,)`` float32.
+    """
+    inputs: np.ndarray
+    targets: np.ndarray
+    ss_tot: float = field(default=0.0)
+
+    def __post_init__(self):
+        self.inputs = np.ascontiguousarray(self.inputs, dtype=np.float32)
+        if self.inputs.ndim == 1:
+            self.inputs = self.inputs.reshape(-1, 1)
+        self.targets = np.ascontiguousarray(self.targets, dtype=np.float32).reshape(-1)
+        if self.inputs.shape[0] != self.targets.shape[0]:
+            raise ValueError("inputs and targets disagree on the case count")
+        # Two-pass SS_tot over the valid targets (src/Dataset.cpp:35-47).
+        if self.N > 0:
+            t = self.targets.astype(np.float64)
+            mean = float(np.sum(t)) / self.N
+            self.ss_tot = float(np.sum((t - mean) ** 2))
+
+    @property
+    def N(self) -> int:
+        return int(self.targets.shape[0])
+
+    @property
+    def num_inputs(self) -> int:
+        return int(self.inputs.shape[1])
+
+
+class Evaluator:
+    """One evaluator context on one GPU (replaces CudaEvaluator,
+    src/EvaluatorCuda.h:11-99)."""
+
+    def __init__(self, profile: int = PROFILE_REF, num_registers: int = 8, input_protect: bool = False,
+                 reduce: int = REDUCE_KAHAN32, constants: Optional[Sequence[float]] = None,
+                 device: int = 0, intron_prepass: bool = True, cases_per_lane: int = 0,
+                 warps_per_block: int = 0):
+        self._lib = load_library()
+        opt = _Options()
+        self._lib.galop_options_init(C.byref(opt))
+        opt.profile = profile
+        opt.num_registers = num_registers
+        opt.input_protect = int(bool(input_protect))
+        opt.reduce = reduce
+        opt.device = device
+        opt.intron_prepass = int(bool(intron_prepass))
+        opt.cases_per_lane = cases_per_lane
+        opt.warps_per_block = warps_per_block
+        self.constants = None
+        if constants is not None:
+            self.constants = np.ascontiguousarray(constants, dtype=np.float32)
+            if self.constants.shape != (num_registers,):
+                raise ValueError("constant pool must have num_registers entries")
+            opt.constants = _ptr(self.constants, C.c_float)
+        self.options = opt
+        self.num_registers = num_registers
+        self.profile = profile
+        self.input_protect = bool(input_protect)
+        self._ctx = C.c_void_p()
+        rc = self._lib.galop_create(C.byref(opt), C.byref(self._ctx))
+        if rc != OK:
+            raise GalopError(rc, f"galop_create failed: {status_string(rc)}")
+        self._dataset_key = None
+        self.dataset: Optional[Dataset] = None
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_ctx", None) and self._ctx.value:
+            self._lib.galop_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._ctx
+
+    def _check(self, rc: int):
+        if rc != OK:
+            msg = self._lib.galop_last_error(self._ctx)
+            raise GalopError(rc, (msg or b"").decode() or status_string(rc))
+
+    # -- dataset ----------------------------------------------------------------
+    def set_dataset(self, dataset: Dataset):
+        self._check(self._lib.galop_set_dataset(self._ctx, _ptr(dataset.inputs, C.c_float),
+                                                _ptr(dataset.targets, C.c_float), dataset.N,
+                                                dataset.num_inputs))
+        self.dataset = dataset
+        self._dataset_key = (id(dataset), dataset.N, dataset.num_inputs)
+
+    def _ensure_dataset(self, dataset: Optional[Dataset]):
+        if dataset is None:
+            if self.dataset is None:
+                raise GalopError(E_NO_DATASET, "no dataset")
+            return
+        if self._dataset_key != (id(dataset), dataset.N, dataset.num_inputs) or dataset is not self.dataset:
+            self.set_dataset(dataset)
+
+    # -- evaluation -------------------------------------------------------------
+    def evaluate_population(self, instructions: np.ndarray, lengths: np.ndarray,
+                            fitness_out: Optional[np.ndarray] = None, n_programs: Optional[int] = None,
+                            dataset: Optional[Dataset] = None, stride: Optional[int] = None) -> np.ndarray:
+        """EvalBackend::evaluate_population (src/EvalBackend.h:11-17)."""
+        self._ensure_dataset(dataset)
+        lengths = np.ascontiguousarray(lengths, dtype=np.uint8)
+        n = int(lengths.shape[0] if n_programs is None else n_programs)
+        instructions = np.ascontiguousarray(instructions, dtype=np.uint32)
+        if stride is None:
+            stride = instructions.shape[1] if instructions.ndim == 2 else (instructions.size // max(n, 1))
+        if instructions.size < n * stride:
+            raise ValueError("instructions buffer shorter than n_programs * stride")
+        if fitness_out is None:
+            fitness_out = np.empty(n, dtype=np.float32)
+        self._check(self._lib.galop_evaluate_population(self._ctx, _ptr(instructions, C.c_uint32),
+                                                        _ptr(lengths, C.c_uint8), stride, n,
+                                                        _ptr(fitness_out, C.c_float)))
+        return fitness_out
+
+    def evaluate_csr(self, words: np.ndarray, offsets: np.ndarray, dataset: Optional[Dataset] = None,
+                     with_sse: bool = False, fitness_out: Optional[np.ndarray] = None,
+                     sse_out: Optional[np.ndarray] = None):
+        self._ensure_dataset(dataset)
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        n = offsets.shape[0] - 1
+        fit = fitness_out if fitness_out is not None else np.empty(n, dtype=np.float32)
+        sse = sse_out if sse_out is not None else (np.empty(n, dtype=np.float64) if with_sse else None)
+        self._check(self._lib.galop_evaluate_csr(self._ctx, _ptr(words, C.c_uint32), _ptr(offsets, C.c_int64),
+                                                 n, _ptr(fit, C.c_float), _ptr(sse, C.c_double)))
+        return (fit, sse) if with_sse else fit
+
+    def evaluate_csr_device(self, d_words: int, d_offsets: int, n_programs: int, d_fitness: int,
+                            d_sse: int = 0, stream: int = 0):
+        self._check(self._lib.galop_evaluate_csr_device(self._ctx, d_words, d_offsets, n_programs,
+                                                        d_fitness, d_sse or None, stream or None))
+
+    def case_outputs(self, words: np.ndarray, offsets: np.ndarray, dataset: Optional[Dataset] = None):
+        self._ensure_dataset(dataset)
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        n = offsets.shape[0] - 1
+        out = np.empty((n, self.dataset.N), dtype=np.float32)
+        self._check(self._lib.galop_case_outputs_csr(self._ctx, _ptr(words, C.c_uint32),
+                                                     _ptr(offsets, C.c_int64), n, _ptr(out, C.c_float)))
+        return out
+
+    def trace(self, program: np.ndarray, dataset: Optional[Dataset] = None) -> np.ndarray:
+        """Register file after each instruction: array (L+1, NR, n_traced)."""
+        self._ensure_dataset(dataset)
+        program = np.ascontiguousarray(program, dtype=np.uint32)
+        L = program.shape[0]
+        state = np.empty(((L + 1) * self.num_registers * 1024,), dtype=np.float32)
+        nt = C.c_int64(0)
+        self._check(self._lib.galop_trace_program(self._ctx, _ptr(program, C.c_uint32), L,
+                                                  _ptr(state, C.c_float), C.byref(nt)))
+        n = nt.value
+        return state[: (L + 1) * self.num_registers * n].reshape(L + 1, self.num_registers, n)
+
+    def effective(self, words: np.ndarray, offsets: np.ndarray):
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        n = offsets.shape[0] - 1
+        eff_len = np.empty(n, dtype=np.int64)
+        eff_words = np.empty(max(int(offsets[-1]), 1), dtype=np.uint32)
+        self._check(self._lib.galop_effective_csr(self._ctx, _ptr(words, C.c_uint32), _ptr(offsets, C.c_int64),
+                                                  n, _ptr(eff_len, C.c_int64), _ptr(eff_words, C.c_uint32)))
+        return eff_len, eff_words[: int(eff_len.sum())]
+
+    @property
+    def stats(self) -> Stats:
+        s = Stats()
+        self._check(self._lib.galop_last_stats(self._ctx, C.byref(s)))
+        return s
+
+    def synchronize(self):
+        self._check(self._lib.galop_synchronize(self._ctx))
+
+    def timer_record(self, slot: int):
+        self._check(self._lib.galop_timer_record(self._ctx, slot))
+
+    def timer_elapsed(self, a: int, b: int) -> float:
+        ms = C.c_double()
+        self._check(self._lib.galop_timer_elapsed(self._ctx, a, b, C.byref(ms)))
+        return ms.value
+
+    # -- memory helpers -------------------------------------------------------
+    def device_alloc(self, nbytes: int) -> int:
+        p = C.c_void_p()
+        self._check(self._lib.galop_device_alloc(self._ctx, nbytes, C.byref(p)))
+        return p.value or 0
+
+    def device_free(self, p: int):
+        self._check(self._lib.galop_device_free(self._ctx, p))
+
+    def h2d(self, dst: int, src: np.ndarray):
+        self._check(self._lib.galop_memcpy_h2d(self._ctx, dst, src.ctypes.data, src.nbytes))
+
+    def d2h(self, dst: np.ndarray, src: int):
+        self._check(self._lib.galop_memcpy_d2h(self._ctx, dst.ctypes.data, src, dst.nbytes))
+
+
+class PinnedArray:
+    """numpy view over page-locked host memory from galop_host_alloc."""
+
+    def __init__(self, shape, dtype):
+        self._lib = load_library()
+        dtype = np.dtype(dtype)
+        nbytes = int(np.prod(shape)) * dtype.itemsize
+        p = C.c_void_p()
+        rc = self._lib.galop_host_alloc(nbytes, C.byref(p))
+        if rc != OK:
+            raise GalopError(rc, "galop_host_alloc failed")
+        self._p = p
+        buf = (C.c_char * max(nbytes, 1)).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+    def free(self):
+        if self._p and self._p.value:
+            self.array = None
+            self._lib.galop_host_free(self._p)
+            self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def csr_from_dense(instructions: np.ndarray, lengths: np.ndarray, stride: int):
+    """Pack the engine's dense layout into CSR (the reference's host pack,
+    src/EvaluatorCuda.cu:335-373)."""
+    lengths = np.asarray(lengths, dtype=np.int64)
+    offsets = np.zeros(lengths.shape[0] + 1, dtype=np.int64)
+    np.cumsum(lengths, out=offsets[1:])
+    flat = np.asarray(instructions, dtype=np.uint32).reshape(-1)
+    idx = (np.repeat(np.arange(lengths.shape[0], dtype=np.int64) * stride, lengths)
+           + (np.arange(offsets[-1], dtype=np.int64) - np.repeat(offsets[:-1], lengths)))
+    return flat[idx], offsets

@@ -1,0 +1,93 @@
+// isa.cuh -- device-side view of Galop's instruction encoding and op
+// semantics.
+//
+// Raw word (src/ISA.h:20-41):  [31:24 SRC2 mode|idx][23:16 SRC1][15:8 DEST][7:0 OP]
+// Only the low 3 bits of OP (src/LGPConfig.h:189-191) and the low log2(NR)
+// bits of each register field are meaningful; bit 31 selects the constant
+// pool for src2 (src/ISA.h:84, :201-206).
+//
+// The pre-pass rewrites every interpreted instruction into a "micro-op" with
+// the same byte layout but every field already masked, the INPUT_PROTECT dest
+// fold (src/ISA.h:181-187) applied, and bit 6 of the OP byte set for unary
+// ops, so the interpreter decodes with plain byte extracts.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace galop {
+
+constexpr int kMaxRegisters = 16;
+
+enum Profile : int { kProfileRef = 0, kProfileBj = 1 };
+enum Op : uint32_t { kAdd = 0, kSub, kMul, kDiv, kSin, kCos, kOp6, kOp7 };
+
+// Runtime ISA parameters shared by the pre-pass kernels.
+struct IsaParams {
+    int profile;
+    int num_registers;   // power of two <= kMaxRegisters
+    int input_protect;
+    int output_reg;      // 0, or num_registers/2 under input protection
+};
+
+// Constant pool passed by value as a kernel parameter (it lands in the
+// constant bank, so a warp-uniform index is a single broadcast load).
+struct ConstPool {
+    float c[kMaxRegisters];
+};
+
+struct Decoded {
+    uint32_t op, dest, src1, src2, is_const, unary;
+};
+
+__host__ __device__ __forceinline__ bool op_is_unary(int profile, uint32_t op) {
+    return op == kSin || op == kCos || (profile == kProfileBj && (op == kOp6 || op == kOp7));
+}
+
+// src/ISA.h:176-206 with runtime NR / INPUT_PROTECT.
+__host__ __device__ __forceinline__ Decoded decode_raw(const IsaParams& p, uint32_t w) {
+    const uint32_t rmask = (uint32_t)p.num_registers - 1u;
+    Decoded d;
+    d.op = w & 7u;
+    d.dest = p.input_protect ? (uint32_t)p.output_reg + ((w >> 8) & (rmask >> 1))
+                             : ((w >> 8) & rmask);
+    d.src1 = (w >> 16) & rmask;
+    d.src2 = (w >> 24) & rmask;
+    d.is_const = (w >> 31) & 1u;
+    d.unary = op_is_unary(p.profile, d.op) ? 1u : 0u;
+    return d;
+}
+
+// Micro-op: byte0 = op | unary<<6, byte1 = dest, byte2 = src1,
+// byte3 = src2 | const<<7.
+__host__ __device__ __forceinline__ uint32_t encode_uop(const Decoded& d) {
+    return (d.op | (d.unary << 6)) | (d.dest << 8) | (d.src1 << 16) | ((d.src2 | (d.is_const << 7)) << 24);
+}
+
+__device__ __forceinline__ uint32_t uop_op(uint32_t u) { return u & 7u; }
+__device__ __forceinline__ uint32_t uop_dest(uint32_t u) { return (u >> 8) & 0xffu; }
+__device__ __forceinline__ uint32_t uop_src1(uint32_t u) { return (u >> 16) & 0xffu; }
+__device__ __forceinline__ uint32_t uop_src2(uint32_t u) { return (u >> 24) & 0x7fu; }
+__device__ __forceinline__ bool uop_is_const(uint32_t u) { return (u >> 31) != 0u; }
+
+// Op semantics, src/ISA.h:219-231 (REF) and the BJ profile's EXP/LOG.
+// Explicit round-to-nearest intrinsics: no FMA contraction, IEEE division,
+// matching the CPU build (ISO C++, no contraction, SSE2 arithmetic).
+template <int PROFILE>
+__device__ __forceinline__ float apply_op(uint32_t op, float a, float b) {
+    switch (op) {
+        case kAdd: return __fadd_rn(a, b);
+        case kSub: return __fsub_rn(a, b);
+        case kMul: return __fmul_rn(a, b);
+        case kDiv: return (b != 0.0f) ? __fdiv_rn(a, b) : 1.0f;
+        case kSin: return sinf(b);
+        case kCos: return cosf(b);
+        case kOp6:
+            if constexpr (PROFILE == kProfileBj) return expf(b);
+            else return (a < b) ? 1.0f : 0.0f;
+        default:
+            if constexpr (PROFILE == kProfileBj) return (b != 0.0f) ? logf(fabsf(b)) : 0.0f;
+            else return (a > b) ? 1.0f : 0.0f;
+    }
+}
+
+}  // namespace galop

@@ -1,0 +1,279 @@
+// prepass.cuh -- GPU intron removal, compaction and scheduling.
+//
+// Structural introns (src/Introns.h:28-46): one backward liveness pass over
+// straight-line code is exact, so interpreting only the effective
+// instructions yields bit-identical outputs.  The reference runs it on the
+// host with OpenMP at the H2D boundary (src/EvaluatorCuda.cu:374-422); here
+// it runs on the device, one thread per program, with the live set as a
+// bitmask in a register:
+//
+//   count    eff_len[i] = number of effective instructions (or the raw
+//            length when the pass is off)
+//   scan     eff_off = exclusive prefix sum (int64), three phases
+//   compact  write the micro-ops of the effective instructions, program
+//            order preserved, at eff_off[i]
+//   order    counting sort of program indices by interpreted length,
+//            longest first, for longest-processing-time-first scheduling
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "isa.cuh"
+
+namespace galop {
+
+// Programs as the reference packs them (src/eval_kernels.cuh:292-303).
+struct CsrSource {
+    const uint32_t* words;
+    const int64_t* off;
+    __device__ __forceinline__ int64_t start(int64_t i) const { return off[i]; }
+    __device__ __forceinline__ int64_t length(int64_t i) const { return off[i + 1] - off[i]; }
+};
+
+// The engine's dense layout (src/EvalBackend.h:10-17): stride words per
+// program, uint8 lengths.
+struct DenseSource {
+    const uint32_t* words;
+    const uint8_t* lens;
+    int64_t stride;
+    __device__ __forceinline__ int64_t start(int64_t i) const { return i * stride; }
+    __device__ __forceinline__ int64_t length(int64_t i) const { return (int64_t)lens[i]; }
+};
+
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 4;                       // per thread
+constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr int kOrderBins = 4096;                    // lengths >= kOrderBins-1 share a bin
+
+template <class Src>
+__global__ void prepass_count_kernel(Src src, int64_t n, IsaParams isa, int strip,
+                                     int32_t* __restrict__ eff_len,
+                                     unsigned long long* __restrict__ totals) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t raw = 0, cnt = 0;
+    if (i < n) {
+        const int64_t s = src.start(i);
+        raw = src.length(i);
+        if (!strip) {
+            cnt = raw;
+        } else {
+            uint32_t live = 1u << isa.output_reg;
+            for (int64_t pc = raw - 1; pc >= 0; --pc) {
+                const Decoded d = decode_raw(isa, __ldg(src.words + s + pc));
+                if (!((live >> d.dest) & 1u)) continue;
+                ++cnt;
+                live &= ~(1u << d.dest);
+                if (!d.unary) live |= 1u << d.src1;
+                if (!d.is_const) live |= 1u << d.src2;
+            }
+        }
+        eff_len[i] = (int32_t)cnt;
+    }
+    // Block totals of raw and effective lengths (for the stats).
+    __shared__ unsigned long long sraw, seff;
+    if (threadIdx.x == 0) { sraw = 0; seff = 0; }
+    __syncthreads();
+    if (raw) atomicAdd(&sraw, (unsigned long long)raw);
+    if (cnt) atomicAdd(&seff, (unsigned long long)cnt);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (sraw) atomicAdd(&totals[0], sraw);
+        if (seff) atomicAdd(&totals[1], seff);
+    }
+}
+
+// Phase 1: per-tile sums.
+__global__ void scan_tile_sums_kernel(const int32_t* __restrict__ in, int64_t n,
+                                      int64_t* __restrict__ tile_sums) {
+    __shared__ int64_t warp_sums[kScanThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    int64_t s = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        const int64_t i = base + (int64_t)j * kScanThreads + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int64_t v = threadIdx.x < kScanThreads / 32 ? warp_sums[threadIdx.x] : 0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (threadIdx.x == 0) tile_sums[blockIdx.x] = v;
+    }
+}
+
+// Phase 2: exclusive scan of the tile sums in one block (serial over chunks
+// of kScanThreads), total written at tile_sums[n_tiles].
+__global__ void scan_tile_offsets_kernel(int64_t* __restrict__ tile_sums, int64_t n_tiles) {
+    __shared__ int64_t buf[kScanThreads];
+    __shared__ int64_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int64_t b = 0; b < n_tiles; b += kScanThreads) {
+        const int64_t i = b + threadIdx.x;
+        const int64_t v = i < n_tiles ? tile_sums[i] : 0;
+        buf[threadIdx.x] = v;
+        __syncthreads();
+        for (int off = 1; off < kScanThreads; off <<= 1) {
+            const int64_t t = threadIdx.x >= off ? buf[threadIdx.x - off] : 0;
+            __syncthreads();
+            buf[threadIdx.x] += t;
+            __syncthreads();
+        }
+        const int64_t incl = buf[threadIdx.x];
+        const int64_t c = carry;
+        if (i < n_tiles) tile_sums[i] = c + incl - v;
+        __syncthreads();
+        if (threadIdx.x == kScanThreads - 1) carry = c + incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) tile_sums[n_tiles] = carry;
+}
+
+// Phase 3: exclusive scan inside each tile plus the tile offset; out[n] = total.
+__global__ void scan_apply_kernel(const int32_t* __restrict__ in, int64_t n,
+                                  const int64_t* __restrict__ tile_offsets, int64_t n_tiles,
+                                  int64_t* __restrict__ out) {
+    __shared__ int64_t warp_tot[kScanThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int64_t v[kScanItems];
+    int64_t s = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        const int64_t i = base + j;
+        v[j] = i < n ? in[i] : 0;
+        s += v[j];
+    }
+    // Inclusive warp scan of per-thread sums.
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int64_t incl = s;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int64_t t = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += t;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int64_t x = lane < kScanThreads / 32 ? warp_tot[lane] : 0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int64_t t = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += t;
+        }
+        if (lane < kScanThreads / 32) warp_tot[lane] = x;  // inclusive
+    }
+    __syncthreads();
+    int64_t run = tile_offsets[blockIdx.x] + (w ? warp_tot[w - 1] : 0) + (incl - s);
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        const int64_t i = base + j;
+        if (i < n) out[i] = run;
+        run += v[j];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tile_offsets[n_tiles];
+}
+
+// Write micro-ops of the interpreted instructions of program i at eff_off[i].
+// raw_out (optional) receives the raw words of the same instructions.
+template <class Src>
+__global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int strip,
+                                       const int64_t* __restrict__ eff_off,
+                                       uint32_t* __restrict__ uops,
+                                       uint32_t* __restrict__ raw_out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t s = src.start(i);
+    const int64_t raw = src.length(i);
+    const int64_t o = eff_off[i];
+    if (!strip) {
+        for (int64_t pc = 0; pc < raw; ++pc) {
+            const uint32_t w = __ldg(src.words + s + pc);
+            uops[o + pc] = encode_uop(decode_raw(isa, w));
+            if (raw_out) raw_out[o + pc] = w;
+        }
+        return;
+    }
+    int64_t pos = eff_off[i + 1];   // fill backwards
+    uint32_t live = 1u << isa.output_reg;
+    for (int64_t pc = raw - 1; pc >= 0; --pc) {
+        const uint32_t w = __ldg(src.words + s + pc);
+        const Decoded d = decode_raw(isa, w);
+        if (!((live >> d.dest) & 1u)) continue;
+        --pos;
+        uops[pos] = encode_uop(d);
+        if (raw_out) raw_out[pos] = w;
+        live &= ~(1u << d.dest);
+        if (!d.unary) live |= 1u << d.src1;
+        if (!d.is_const) live |= 1u << d.src2;
+    }
+}
+
+// Longest-first order: histogram of bins (bin 0 = longest), scan, scatter.
+__global__ void order_hist_kernel(const int32_t* __restrict__ len, int64_t n,
+                                  unsigned int* __restrict__ hist) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int l = len[i];
+    if (l > kOrderBins - 1) l = kOrderBins - 1;
+    atomicAdd(&hist[kOrderBins - 1 - l], 1u);
+}
+
+__global__ void order_scan_kernel(unsigned int* __restrict__ hist) {
+    // Single block of 1024 threads, 4 bins per thread, exclusive in place.
+    __shared__ unsigned int buf[1024];
+    const int t = threadIdx.x;
+    unsigned int v[4], s = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) { v[j] = hist[t * 4 + j]; s += v[j]; }
+    buf[t] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const unsigned int x = t >= off ? buf[t - off] : 0u;
+        __syncthreads();
+        buf[t] += x;
+        __syncthreads();
+    }
+    unsigned int run = buf[t] - s;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) { hist[t * 4 + j] = run; run += v[j]; }
+}
+
+__global__ void order_scatter_kernel(const int32_t* __restrict__ len, int64_t n,
+                                     unsigned int* __restrict__ cursor,
+                                     int32_t* __restrict__ order) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int l = len[i];
+    if (l > kOrderBins - 1) l = kOrderBins - 1;
+    const unsigned int pos = atomicAdd(&cursor[kOrderBins - 1 - l], 1u);
+    order[pos] = (int32_t)i;
+}
+
+// Case-major (AoS) dataset to feature-major (SoA) with zero padding to Np.
+__global__ void dataset_transpose_kernel(const float* __restrict__ aos, const float* __restrict__ y_in,
+                                         int64_t n, int k, int64_t np,
+                                         float* __restrict__ X, float* __restrict__ y) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= np) return;
+    const bool in = c < n;
+    for (int f = 0; f < k; ++f) X[(int64_t)f * np + c] = in ? aos[c * k + f] : 0.0f;
+    y[c] = in ? y_in[c] : 0.0f;
+}
+
+// Sum of chunk partials in chunk order, then fitness.
+__global__ void finalize_kernel(const double* __restrict__ partial, int64_t n_programs,
+                                int n_chunks, int64_t n_cases, float* __restrict__ fitness,
+                                double* __restrict__ sse_out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_programs) return;
+    double s = 0.0;
+    for (int c = 0; c < n_chunks; ++c) s += partial[i * n_chunks + c];
+    const float mse = (float)(s / (double)n_cases);
+    fitness[i] = isfinite(mse) ? __fdiv_rn(1.0f, __fadd_rn(1.0f, mse)) : 0.0f;
+    if (sse_out) sse_out[i] = s;
+}
+
+}  // namespace galop

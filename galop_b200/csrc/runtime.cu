@@ -1,0 +1,740 @@
+// runtime.cu -- evaluator context and the C ABI (include/galop_b200.h).
+//
+// Replaces CudaEvaluator (src/EvaluatorCuda.{h,cu}):
+//   - dataset uploaded once and kept resident (src/EvaluatorCuda.cu:96-110),
+//     transposed to feature-major on the device;
+//   - population buffers grow to a high-water mark and are reused
+//     (src/EvaluatorCuda.cu:69-81);
+//   - the host pack + intron strip (src/EvaluatorCuda.cu:335-422) becomes
+//     the device pre-pass of prepass.cuh;
+//   - one stream, CUDA-event timings, status codes instead of exit().
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/galop_b200.h"
+#include "interp.cuh"
+#include "prepass.cuh"
+
+namespace galop {
+const void* interp_kernel_nr8(int k, int profile, int reduce, int mode);
+const void* interp_kernel_nr16(int k, int profile, int reduce, int mode);
+}  // namespace galop
+
+using namespace galop;
+
+namespace {
+
+// Reference constant pools (src/LGPConfig.h:159-168).
+const float kRefPool8[8] = {0.0f, 1.0f, -1.0f, 3.14159f, 0.5f, 2.0f, 10.0f, 100.0f};
+const float kRefPool16[16] = {0.0f, 1.0f, -1.0f, 3.14159f, 0.5f, 2.0f, 10.0f, 100.0f,
+                              0.1f, -0.5f, 0.25f, 5.0f, 20.0f, -2.0f, 0.01f, 1000.0f};
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t cap = 0;  // elements
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        size_t want = std::max<size_t>(n, cap + cap / 4);
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        if (e != cudaSuccess) { p = nullptr; return e; }
+        cap = want;
+        return cudaSuccess;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+enum Ev { kEvStart = 0, kEvH2D, kEvPrepass, kEvInterp, kEvFinalize, kEvD2H, kEvCount };
+
+}  // namespace
+
+struct galop_ctx {
+    galop_options opt{};
+    IsaParams isa{};
+    ConstPool pool{};
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[kEvCount] = {};
+    cudaEvent_t timers[8] = {};
+    std::string err;
+
+    // resident dataset (feature-major, padded)
+    DevBuf<float> X, y;
+    DevBuf<float> stage_aos, stage_y;
+    int64_t N = -1, Np = 0;
+    int num_inputs = 0;
+
+    // population buffers (high-water)
+    DevBuf<uint32_t> raw_words, uops, eff_raw;
+    DevBuf<uint8_t> raw_lens8;
+    DevBuf<int64_t> raw_off, eff_off, tiles;
+    DevBuf<int32_t> eff_len, order;
+    DevBuf<float> fitness, outputs, trace;
+    DevBuf<double> sse, partial;
+    DevBuf<unsigned long long> counters;   // [0] queue head, [1..2] totals
+    DevBuf<unsigned int> hist;
+    std::vector<int64_t> host_tmp;
+
+    galop_stats stats{};
+    int launches = 0;
+
+    int fail(int code, const char* fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        err = buf;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* what) {
+        return fail(e == cudaErrorMemoryAllocation ? GALOP_E_NOMEM : GALOP_E_CUDA,
+                    "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+    }
+};
+
+#define GALOP_CK(call, what)                                   \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return ctx->cuda_fail(_e, what); \
+    } while (0)
+
+namespace {
+
+int pick_k(const galop_ctx* ctx) {
+    const int k = ctx->opt.cases_per_lane;
+    if (k == 1 || k == 2 || k == 4 || k == 8) return k;
+    return ctx->isa.num_registers >= 16 ? 2 : 4;
+}
+
+int pick_wpb(const galop_ctx* ctx) {
+    const int w = ctx->opt.warps_per_block;
+    return (w >= 1 && w <= 8) ? w : 4;
+}
+
+const void* kernel_for(const galop_ctx* ctx, int k, int mode) {
+    const int reduce = ctx->opt.reduce;
+    if (ctx->isa.num_registers == 8) return interp_kernel_nr8(k, ctx->isa.profile, reduce, mode);
+    if (ctx->isa.num_registers == 16) return interp_kernel_nr16(k, ctx->isa.profile, reduce, mode);
+    return nullptr;
+}
+
+float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) return 0.0f;
+    return ms;
+}
+
+// Pre-pass over `src` into ctx->uops / eff_off (and order when sched).
+template <class Src>
+int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_total,
+                bool strip, bool sched, uint32_t* raw_out) {
+    cudaStream_t s = ctx->stream;
+    GALOP_CK(ctx->eff_len.ensure((size_t)std::max<int64_t>(n, 1)), "alloc eff_len");
+    GALOP_CK(ctx->eff_off.ensure((size_t)n + 1), "alloc eff_off");
+    const int64_t n_tiles = (n + kScanTile - 1) / kScanTile;
+    GALOP_CK(ctx->tiles.ensure((size_t)n_tiles + 1), "alloc scan tiles");
+    GALOP_CK(ctx->counters.ensure(4), "alloc counters");
+    GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), s), "memset");
+
+    const int tpb = 256;
+    const unsigned blocks = (unsigned)((n + tpb - 1) / tpb);
+    if (n > 0) {
+        prepass_count_kernel<Src><<<blocks, tpb, 0, s>>>(src, n, ctx->isa, strip ? 1 : 0,
+                                                         ctx->eff_len.p, ctx->counters.p + 1);
+        scan_tile_sums_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(ctx->eff_len.p, n, ctx->tiles.p);
+        scan_tile_offsets_kernel<<<1, kScanThreads, 0, s>>>(ctx->tiles.p, n_tiles);
+        scan_apply_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(ctx->eff_len.p, n, ctx->tiles.p,
+                                                                     n_tiles, ctx->eff_off.p);
+        ctx->launches += 4;
+    } else {
+        GALOP_CK(cudaMemsetAsync(ctx->eff_off.p, 0, sizeof(int64_t), s), "memset eff_off");
+    }
+    GALOP_CK(cudaGetLastError(), "pre-pass count/scan launch");
+    // Device buffer for micro-ops sized by the raw total (an upper bound).
+    GALOP_CK(ctx->uops.ensure((size_t)std::max<int64_t>(raw_words_total, 1)), "alloc uops");
+    if (n > 0) {
+        prepass_compact_kernel<Src><<<blocks, tpb, 0, s>>>(src, n, ctx->isa, strip ? 1 : 0,
+                                                           ctx->eff_off.p, ctx->uops.p, raw_out);
+        ctx->launches += 1;
+    }
+    GALOP_CK(cudaGetLastError(), "pre-pass compact launch");
+    if (sched && n > 1) {
+        GALOP_CK(ctx->order.ensure((size_t)n), "alloc order");
+        GALOP_CK(ctx->hist.ensure(kOrderBins), "alloc hist");
+        GALOP_CK(cudaMemsetAsync(ctx->hist.p, 0, kOrderBins * sizeof(unsigned int), s), "memset hist");
+        order_hist_kernel<<<blocks, tpb, 0, s>>>(ctx->eff_len.p, n, ctx->hist.p);
+        order_scan_kernel<<<1, 1024, 0, s>>>(ctx->hist.p);
+        order_scatter_kernel<<<blocks, tpb, 0, s>>>(ctx->eff_len.p, n, ctx->hist.p, ctx->order.p);
+        ctx->launches += 3;
+        GALOP_CK(cudaGetLastError(), "order launch");
+    }
+    return GALOP_OK;
+}
+
+// Interpreter launch over the pre-passed population.
+int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness, double* d_sse,
+               float* d_outputs, float* d_trace, int32_t* chunks_out) {
+    cudaStream_t s = ctx->stream;
+    const int k = pick_k(ctx);
+    const int wpb = pick_wpb(ctx);
+    const int threads = 32 * wpb;
+    const void* fn = kernel_for(ctx, k, mode);
+    if (!fn) return ctx->fail(GALOP_E_INVALID, "no interpreter kernel for NR=%d K=%d",
+                              ctx->isa.num_registers, k);
+    int per_sm = 0;
+    GALOP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0), "occupancy");
+    if (per_sm < 1) per_sm = 1;
+    const int64_t resident_warps = (int64_t)ctx->sm_count * per_sm * wpb;
+
+    // Case chunking: enough work items to keep every resident warp busy.
+    const int64_t pass = 32LL * k;
+    const int64_t passes = std::max<int64_t>(1, (ctx->N + pass - 1) / pass);
+    int64_t n_chunks = 1;
+    if (mode == kModeFitness && ctx->opt.reduce != GALOP_REDUCE_ORDERED && n > 0 &&
+        n < 4 * resident_warps) {
+        n_chunks = std::min<int64_t>(passes, (4 * resident_warps + n - 1) / n);
+    }
+    if (mode != kModeFitness) n_chunks = 1;
+    const int64_t chunk_passes = (passes + n_chunks - 1) / n_chunks;
+    const int64_t chunk_cases = chunk_passes * pass;
+    n_chunks = std::max<int64_t>(1, (std::max<int64_t>(ctx->N, 1) + chunk_cases - 1) / chunk_cases);
+
+    InterpArgs a{};
+    a.uops = ctx->uops.p;
+    a.eff_off = ctx->eff_off.p;
+    a.order = (sched && n > 1) ? ctx->order.p : nullptr;
+    a.n_programs = n;
+    a.n_chunks = (int32_t)n_chunks;
+    a.chunk_cases = chunk_cases;
+    a.X = ctx->X.p;
+    a.y = ctx->y.p;
+    a.N = ctx->N;
+    a.Np = ctx->Np;
+    a.num_inputs = ctx->num_inputs;
+    a.output_reg = ctx->isa.output_reg;
+    a.consts = ctx->pool;
+    a.counter = ctx->counters.p;
+    a.fitness = d_fitness;
+    a.sse = d_sse;
+    a.outputs = d_outputs;
+    a.trace = d_trace;
+    if (n_chunks > 1) {
+        GALOP_CK(ctx->partial.ensure((size_t)(n * n_chunks)), "alloc partial");
+        a.partial = ctx->partial.p;
+    }
+    const int64_t items = n * n_chunks;
+    int64_t blocks = (int64_t)ctx->sm_count * per_sm;
+    const int64_t need = (items + wpb - 1) / wpb;
+    if (blocks > need) blocks = std::max<int64_t>(need, 1);
+    GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned long long), s), "memset queue");
+    if (n > 0) {
+        void* params[] = {&a};
+        GALOP_CK(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(threads), params, 0, s),
+                 "interpreter launch");
+        ctx->launches += 1;
+    }
+    ctx->stats.cases_per_lane = k;
+    ctx->stats.warps_per_block = wpb;
+    ctx->stats.blocks = (int32_t)blocks;
+    ctx->stats.case_chunks = (int32_t)n_chunks;
+    if (chunks_out) *chunks_out = (int32_t)n_chunks;
+    return GALOP_OK;
+}
+
+int finalize(galop_ctx* ctx, int64_t n, int32_t n_chunks, float* d_fitness, double* d_sse) {
+    if (n_chunks <= 1 || n == 0) return GALOP_OK;
+    finalize_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(
+        ctx->partial.p, n, n_chunks, ctx->N, d_fitness, d_sse);
+    ctx->launches += 1;
+    GALOP_CK(cudaGetLastError(), "finalize launch");
+    return GALOP_OK;
+}
+
+int check_ready(galop_ctx* ctx) {
+    if (!ctx) return GALOP_E_INVALID;
+    if (ctx->N < 0) return ctx->fail(GALOP_E_NO_DATASET, "no dataset: call galop_set_dataset first");
+    return GALOP_OK;
+}
+
+void begin_call(galop_ctx* ctx, int64_t n) {
+    ctx->stats = galop_stats{};
+    ctx->stats.n_programs = n;
+    ctx->stats.n_cases = ctx->N;
+    ctx->launches = 0;
+}
+
+int end_call(galop_ctx* ctx) {
+    GALOP_CK(cudaStreamSynchronize(ctx->stream), "evaluate (device execution)");
+    galop_stats& st = ctx->stats;
+    st.h2d_ms = ev_ms(ctx->ev[kEvStart], ctx->ev[kEvH2D]);
+    st.prepass_ms = ev_ms(ctx->ev[kEvH2D], ctx->ev[kEvPrepass]);
+    st.interp_ms = ev_ms(ctx->ev[kEvPrepass], ctx->ev[kEvInterp]);
+    st.finalize_ms = ev_ms(ctx->ev[kEvInterp], ctx->ev[kEvFinalize]);
+    st.d2h_ms = ev_ms(ctx->ev[kEvFinalize], ctx->ev[kEvD2H]);
+    st.total_ms = ev_ms(ctx->ev[kEvStart], ctx->ev[kEvD2H]);
+    unsigned long long tot[2] = {0, 0};
+    if (ctx->counters.p)
+        GALOP_CK(cudaMemcpy(tot, ctx->counters.p + 1, sizeof tot, cudaMemcpyDeviceToHost), "stats D2H");
+    st.raw_instructions = (int64_t)tot[0];
+    st.eff_instructions = (int64_t)tot[1];
+    st.kernels_launched = ctx->launches;
+    return GALOP_OK;
+}
+
+int validate_offsets(galop_ctx* ctx, const int64_t* off, int64_t n) {
+    if (off[0] != 0) return ctx->fail(GALOP_E_INVALID, "offsets[0] must be 0 (got %lld)", (long long)off[0]);
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t l = off[i + 1] - off[i];
+        if (l < 0) return ctx->fail(GALOP_E_INVALID, "offsets not non-decreasing at program %lld", (long long)i);
+        if (l > (int64_t)1 << 30) return ctx->fail(GALOP_E_CAPACITY, "program %lld longer than 2^30", (long long)i);
+    }
+    return GALOP_OK;
+}
+
+// Upload a host CSR population into raw_words/raw_off.
+int upload_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets, int64_t n) {
+    if (!offsets || (n > 0 && !words && offsets[n] > 0))
+        return ctx->fail(GALOP_E_INVALID, "null words/offsets");
+    if (int rc = validate_offsets(ctx, offsets, n)) return rc;
+    const int64_t total = offsets[n];
+    GALOP_CK(ctx->raw_words.ensure((size_t)std::max<int64_t>(total, 1)), "alloc raw words");
+    GALOP_CK(ctx->raw_off.ensure((size_t)n + 1), "alloc raw offsets");
+    if (total > 0)
+        GALOP_CK(cudaMemcpyAsync(ctx->raw_words.p, words, (size_t)total * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, ctx->stream), "H2D words");
+    GALOP_CK(cudaMemcpyAsync(ctx->raw_off.p, offsets, (size_t)(n + 1) * sizeof(int64_t),
+                             cudaMemcpyHostToDevice, ctx->stream), "H2D offsets");
+    return GALOP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int galop_abi_version(void) { return GALOP_ABI_VERSION; }
+
+const char* galop_status_string(int s) {
+    switch (s) {
+        case GALOP_OK: return "ok";
+        case GALOP_E_INVALID: return "invalid argument";
+        case GALOP_E_CUDA: return "CUDA error";
+        case GALOP_E_NOMEM: return "out of memory";
+        case GALOP_E_NO_DATASET: return "no dataset";
+        case GALOP_E_TIMEOUT: return "device wait timed out";
+        case GALOP_E_CAPACITY: return "capacity exceeded";
+        case GALOP_E_NO_DEVICE: return "no suitable device";
+        case GALOP_E_STATE: return "invalid state";
+        default: return "unknown status";
+    }
+}
+
+int galop_options_init(galop_options* opt) {
+    if (!opt) return GALOP_E_INVALID;
+    std::memset(opt, 0, sizeof *opt);
+    opt->profile = GALOP_PROFILE_REF;
+    opt->num_registers = 8;
+    opt->input_protect = 0;
+    opt->reduce = GALOP_REDUCE_KAHAN32;
+    opt->constants = nullptr;
+    opt->device = 0;
+    opt->intron_prepass = 1;
+    opt->cases_per_lane = 0;
+    opt->warps_per_block = 0;
+    return GALOP_OK;
+}
+
+int galop_create(const galop_options* opt, galop_ctx** out) {
+    if (!opt || !out) return GALOP_E_INVALID;
+    *out = nullptr;
+    if (opt->num_registers != 8 && opt->num_registers != 16) return GALOP_E_INVALID;
+    if (opt->profile != GALOP_PROFILE_REF && opt->profile != GALOP_PROFILE_BJ) return GALOP_E_INVALID;
+    if (opt->reduce < GALOP_REDUCE_KAHAN32 || opt->reduce > GALOP_REDUCE_ORDERED) return GALOP_E_INVALID;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return GALOP_E_NO_DEVICE;
+    }
+    if (opt->device < 0 || opt->device >= ndev) return GALOP_E_NO_DEVICE;
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, opt->device) != cudaSuccess) return GALOP_E_NO_DEVICE;
+    if (prop.major != 10) return GALOP_E_NO_DEVICE;   // built for sm_100a only
+
+    galop_ctx* ctx = new galop_ctx();
+    ctx->opt = *opt;
+    ctx->opt.constants = nullptr;
+    ctx->device = opt->device;
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->isa.profile = opt->profile;
+    ctx->isa.num_registers = opt->num_registers;
+    ctx->isa.input_protect = opt->input_protect ? 1 : 0;
+    ctx->isa.output_reg = opt->input_protect ? opt->num_registers / 2 : 0;
+    const float* pool = opt->constants ? opt->constants
+                                       : (opt->num_registers == 16 ? kRefPool16 : kRefPool8);
+    for (int i = 0; i < kMaxRegisters; ++i) ctx->pool.c[i] = i < opt->num_registers ? pool[i] : 0.0f;
+
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    for (int i = 0; e == cudaSuccess && i < kEvCount; ++i) e = cudaEventCreate(&ctx->ev[i]);
+    for (int i = 0; e == cudaSuccess && i < 8; ++i) e = cudaEventCreate(&ctx->timers[i]);
+    if (e == cudaSuccess) e = ctx->counters.ensure(4);
+    if (e != cudaSuccess) {
+        galop_destroy(ctx);
+        return e == cudaErrorMemoryAllocation ? GALOP_E_NOMEM : GALOP_E_CUDA;
+    }
+    *out = ctx;
+    return GALOP_OK;
+}
+
+void galop_destroy(galop_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->X.release(); ctx->y.release(); ctx->stage_aos.release(); ctx->stage_y.release();
+    ctx->raw_words.release(); ctx->uops.release(); ctx->eff_raw.release(); ctx->raw_lens8.release();
+    ctx->raw_off.release(); ctx->eff_off.release(); ctx->tiles.release();
+    ctx->eff_len.release(); ctx->order.release();
+    ctx->fitness.release(); ctx->outputs.release(); ctx->trace.release();
+    ctx->sse.release(); ctx->partial.release(); ctx->counters.release(); ctx->hist.release();
+    for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->timers) if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* galop_last_error(const galop_ctx* ctx) {
+    if (!ctx) return "null context";
+    return ctx->err.c_str();
+}
+
+int galop_last_stats(const galop_ctx* ctx, galop_stats* out) {
+    if (!ctx || !out) return GALOP_E_INVALID;
+    *out = ctx->stats;
+    return GALOP_OK;
+}
+
+int galop_synchronize(galop_ctx* ctx) {
+    if (!ctx) return GALOP_E_INVALID;
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    GALOP_CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return GALOP_OK;
+}
+
+int galop_timer_record(galop_ctx* ctx, int32_t slot) {
+    if (!ctx || slot < 0 || slot >= 8) return GALOP_E_INVALID;
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    GALOP_CK(cudaEventRecord(ctx->timers[slot], ctx->stream), "timer record");
+    return GALOP_OK;
+}
+
+int galop_timer_elapsed(galop_ctx* ctx, int32_t a, int32_t b, double* ms) {
+    if (!ctx || !ms || a < 0 || a >= 8 || b < 0 || b >= 8) return GALOP_E_INVALID;
+    GALOP_CK(cudaEventSynchronize(ctx->timers[b]), "timer sync");
+    float f = 0.0f;
+    GALOP_CK(cudaEventElapsedTime(&f, ctx->timers[a], ctx->timers[b]), "timer elapsed");
+    *ms = f;
+    return GALOP_OK;
+}
+
+int galop_host_alloc(int64_t bytes, void** out) {
+    if (!out || bytes < 0) return GALOP_E_INVALID;
+    *out = nullptr;
+    cudaError_t e = cudaMallocHost(out, (size_t)std::max<int64_t>(bytes, 1));
+    if (e != cudaSuccess) { cudaGetLastError(); *out = nullptr; return GALOP_E_NOMEM; }
+    return GALOP_OK;
+}
+
+int galop_host_free(void* p) {
+    if (p && cudaFreeHost(p) != cudaSuccess) return GALOP_E_CUDA;
+    return GALOP_OK;
+}
+
+int galop_device_alloc(galop_ctx* ctx, int64_t bytes, void** out) {
+    if (!ctx || !out || bytes < 0) return GALOP_E_INVALID;
+    *out = nullptr;
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    GALOP_CK(cudaMalloc(out, (size_t)std::max<int64_t>(bytes, 1)), "device alloc");
+    return GALOP_OK;
+}
+
+int galop_device_free(galop_ctx* ctx, void* p) {
+    if (!ctx) return GALOP_E_INVALID;
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    if (p) GALOP_CK(cudaFree(p), "device free");
+    return GALOP_OK;
+}
+
+int galop_memcpy_h2d(galop_ctx* ctx, void* dst, const void* src, int64_t bytes) {
+    if (!ctx || bytes < 0) return GALOP_E_INVALID;
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    if (bytes) GALOP_CK(cudaMemcpyAsync(dst, src, (size_t)bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    GALOP_CK(cudaStreamSynchronize(ctx->stream), "H2D sync");
+    return GALOP_OK;
+}
+
+int galop_memcpy_d2h(galop_ctx* ctx, void* dst, const void* src, int64_t bytes) {
+    if (!ctx || bytes < 0) return GALOP_E_INVALID;
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    if (bytes) GALOP_CK(cudaMemcpyAsync(dst, src, (size_t)bytes, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    GALOP_CK(cudaStreamSynchronize(ctx->stream), "D2H sync");
+    return GALOP_OK;
+}
+
+static int set_dataset_common(galop_ctx* ctx, const float* src_aos, const float* src_y,
+                              int64_t n_cases, int32_t num_inputs) {
+    const int64_t np = std::max<int64_t>(1024, (n_cases + 1023) / 1024 * 1024);
+    GALOP_CK(ctx->X.ensure((size_t)(np * std::max(num_inputs, 1))), "alloc dataset X");
+    GALOP_CK(ctx->y.ensure((size_t)np), "alloc dataset y");
+    const unsigned blocks = (unsigned)((np + 255) / 256);
+    dataset_transpose_kernel<<<blocks, 256, 0, ctx->stream>>>(src_aos, src_y, n_cases, num_inputs, np,
+                                                              ctx->X.p, ctx->y.p);
+    GALOP_CK(cudaGetLastError(), "dataset transpose launch");
+    GALOP_CK(cudaStreamSynchronize(ctx->stream), "dataset upload");
+    ctx->N = n_cases;
+    ctx->Np = np;
+    ctx->num_inputs = num_inputs;
+    return GALOP_OK;
+}
+
+int galop_set_dataset(galop_ctx* ctx, const float* inputs, const float* targets, int64_t n_cases,
+                      int32_t num_inputs) {
+    if (!ctx) return GALOP_E_INVALID;
+    if (n_cases < 0 || num_inputs < 0 || num_inputs > ctx->isa.num_registers)
+        return ctx->fail(GALOP_E_INVALID, "bad dataset shape: n_cases=%lld num_inputs=%d (NR=%d)",
+                         (long long)n_cases, num_inputs, ctx->isa.num_registers);
+    if (n_cases > 0 && (!targets || (num_inputs > 0 && !inputs)))
+        return ctx->fail(GALOP_E_INVALID, "null dataset pointer");
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    const size_t nx = (size_t)n_cases * (size_t)num_inputs;
+    GALOP_CK(ctx->stage_aos.ensure(std::max<size_t>(nx, 1)), "alloc dataset staging");
+    GALOP_CK(ctx->stage_y.ensure(std::max<size_t>((size_t)n_cases, 1)), "alloc dataset staging");
+    if (nx) GALOP_CK(cudaMemcpyAsync(ctx->stage_aos.p, inputs, nx * sizeof(float), cudaMemcpyHostToDevice,
+                                     ctx->stream), "H2D dataset inputs");
+    if (n_cases) GALOP_CK(cudaMemcpyAsync(ctx->stage_y.p, targets, (size_t)n_cases * sizeof(float),
+                                          cudaMemcpyHostToDevice, ctx->stream), "H2D dataset targets");
+    int rc = set_dataset_common(ctx, ctx->stage_aos.p, ctx->stage_y.p, n_cases, num_inputs);
+    ctx->stage_aos.release();
+    ctx->stage_y.release();
+    return rc;
+}
+
+int galop_set_dataset_device(galop_ctx* ctx, const float* d_inputs, const float* d_targets,
+                             int64_t n_cases, int32_t num_inputs) {
+    if (!ctx) return GALOP_E_INVALID;
+    if (n_cases < 0 || num_inputs < 0 || num_inputs > ctx->isa.num_registers)
+        return ctx->fail(GALOP_E_INVALID, "bad dataset shape");
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    return set_dataset_common(ctx, d_inputs, d_targets, n_cases, num_inputs);
+}
+
+}  // extern "C"
+
+// Shared body of the host-pointer evaluate calls, after the raw population
+// is on the device (in raw_words/raw_off or raw_words/raw_lens8).
+template <class Src>
+static int evaluate_uploaded(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_total,
+                             float* fitness_out, double* sse_out) {
+    cudaStream_t s = ctx->stream;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvH2D], s), "event");
+    if (int rc = run_prepass(ctx, src, n, raw_total, ctx->opt.intron_prepass != 0, true, nullptr)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvPrepass], s), "event");
+    GALOP_CK(ctx->fitness.ensure((size_t)std::max<int64_t>(n, 1)), "alloc fitness");
+    GALOP_CK(ctx->sse.ensure((size_t)std::max<int64_t>(n, 1)), "alloc sse");
+    int32_t chunks = 1;
+    if (int rc = run_interp(ctx, n, kModeFitness, true, ctx->fitness.p, ctx->sse.p, nullptr, nullptr, &chunks))
+        return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvInterp], s), "event");
+    if (int rc = finalize(ctx, n, chunks, ctx->fitness.p, ctx->sse.p)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvFinalize], s), "event");
+    if (n > 0) {
+        GALOP_CK(cudaMemcpyAsync(fitness_out, ctx->fitness.p, (size_t)n * sizeof(float),
+                                 cudaMemcpyDeviceToHost, s), "D2H fitness");
+        if (sse_out)
+            GALOP_CK(cudaMemcpyAsync(sse_out, ctx->sse.p, (size_t)n * sizeof(double),
+                                     cudaMemcpyDeviceToHost, s), "D2H sse");
+    }
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvD2H], s), "event");
+    return end_call(ctx);
+}
+
+extern "C" {
+
+int galop_evaluate_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets, int64_t n_programs,
+                       float* fitness_out, double* sse_out) {
+    if (int rc = check_ready(ctx)) return rc;
+    if (n_programs < 0) return ctx->fail(GALOP_E_INVALID, "n_programs < 0");
+    if (n_programs > INT32_MAX) return ctx->fail(GALOP_E_CAPACITY, "n_programs > 2^31-1");
+    if (n_programs > 0 && !fitness_out) return ctx->fail(GALOP_E_INVALID, "null fitness_out");
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    begin_call(ctx, n_programs);
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], ctx->stream), "event");
+    if (int rc = upload_csr(ctx, words, offsets, n_programs)) return rc;
+    CsrSource src{ctx->raw_words.p, ctx->raw_off.p};
+    return evaluate_uploaded(ctx, src, n_programs, offsets[n_programs], fitness_out, sse_out);
+}
+
+int galop_evaluate_population(galop_ctx* ctx, const uint32_t* instructions, const uint8_t* lengths,
+                              int64_t stride, int64_t n_programs, float* fitness_out) {
+    if (int rc = check_ready(ctx)) return rc;
+    if (n_programs < 0 || stride < 0) return ctx->fail(GALOP_E_INVALID, "negative size");
+    if (n_programs > INT32_MAX) return ctx->fail(GALOP_E_CAPACITY, "n_programs > 2^31-1");
+    if (n_programs > 0 && (!instructions || !lengths || !fitness_out))
+        return ctx->fail(GALOP_E_INVALID, "null pointer");
+    for (int64_t i = 0; i < n_programs; ++i)
+        if ((int64_t)lengths[i] > stride)
+            return ctx->fail(GALOP_E_INVALID, "lengths[%lld]=%d exceeds stride %lld", (long long)i,
+                             (int)lengths[i], (long long)stride);
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    begin_call(ctx, n_programs);
+    cudaStream_t s = ctx->stream;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], s), "event");
+    const int64_t total = n_programs * stride;
+    GALOP_CK(ctx->raw_words.ensure((size_t)std::max<int64_t>(total, 1)), "alloc raw words");
+    GALOP_CK(ctx->raw_lens8.ensure((size_t)std::max<int64_t>(n_programs, 1)), "alloc lengths");
+    if (total > 0)
+        GALOP_CK(cudaMemcpyAsync(ctx->raw_words.p, instructions, (size_t)total * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, s), "H2D instructions");
+    if (n_programs > 0)
+        GALOP_CK(cudaMemcpyAsync(ctx->raw_lens8.p, lengths, (size_t)n_programs, cudaMemcpyHostToDevice, s),
+                 "H2D lengths");
+    DenseSource src{ctx->raw_words.p, ctx->raw_lens8.p, stride};
+    return evaluate_uploaded(ctx, src, n_programs, total, fitness_out, nullptr);
+}
+
+int galop_evaluate_csr_device(galop_ctx* ctx, const uint32_t* d_words, const int64_t* d_offsets,
+                              int64_t n_programs, float* d_fitness, double* d_sse, void* stream) {
+    if (int rc = check_ready(ctx)) return rc;
+    if (n_programs < 0 || !d_offsets) return ctx->fail(GALOP_E_INVALID, "bad arguments");
+    if (n_programs > 0 && (!d_words || !d_fitness)) return ctx->fail(GALOP_E_INVALID, "null pointer");
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    begin_call(ctx, n_programs);
+    cudaStream_t user = (cudaStream_t)stream;
+    cudaStream_t s = ctx->stream;
+    if (user && user != s) {
+        GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], user), "event");
+        GALOP_CK(cudaStreamWaitEvent(s, ctx->ev[kEvStart], 0), "stream wait");
+    } else {
+        GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], s), "event");
+    }
+    // Total words from the device offsets (one 8-byte read).
+    int64_t total = 0;
+    GALOP_CK(cudaMemcpyAsync(&total, d_offsets + n_programs, sizeof(int64_t), cudaMemcpyDeviceToHost, s),
+             "read total");
+    GALOP_CK(cudaStreamSynchronize(s), "read total");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvH2D], s), "event");
+    CsrSource src{d_words, d_offsets};
+    if (int rc = run_prepass(ctx, src, n_programs, total, ctx->opt.intron_prepass != 0, true, nullptr)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvPrepass], s), "event");
+    int32_t chunks = 1;
+    if (int rc = run_interp(ctx, n_programs, kModeFitness, true, d_fitness, d_sse, nullptr, nullptr, &chunks))
+        return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvInterp], s), "event");
+    if (int rc = finalize(ctx, n_programs, chunks, d_fitness, d_sse)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvFinalize], s), "event");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvD2H], s), "event");
+    if (user && user != s) GALOP_CK(cudaStreamWaitEvent(user, ctx->ev[kEvD2H], 0), "stream wait");
+    ctx->stats.kernels_launched = ctx->launches;
+    return GALOP_OK;
+}
+
+int galop_case_outputs_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets,
+                           int64_t n_programs, float* outputs) {
+    if (int rc = check_ready(ctx)) return rc;
+    if (n_programs < 0) return ctx->fail(GALOP_E_INVALID, "n_programs < 0");
+    if (n_programs > 0 && !outputs) return ctx->fail(GALOP_E_INVALID, "null outputs");
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    begin_call(ctx, n_programs);
+    cudaStream_t s = ctx->stream;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], s), "event");
+    if (int rc = upload_csr(ctx, words, offsets, n_programs)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvH2D], s), "event");
+    CsrSource src{ctx->raw_words.p, ctx->raw_off.p};
+    if (int rc = run_prepass(ctx, src, n_programs, offsets[n_programs], ctx->opt.intron_prepass != 0, true,
+                             nullptr)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvPrepass], s), "event");
+    const size_t total = (size_t)n_programs * (size_t)std::max<int64_t>(ctx->N, 0);
+    GALOP_CK(ctx->outputs.ensure(std::max<size_t>(total, 1)), "alloc outputs");
+    if (int rc = run_interp(ctx, n_programs, kModeOutputs, true, nullptr, nullptr, ctx->outputs.p, nullptr,
+                            nullptr)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvInterp], s), "event");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvFinalize], s), "event");
+    if (total)
+        GALOP_CK(cudaMemcpyAsync(outputs, ctx->outputs.p, total * sizeof(float), cudaMemcpyDeviceToHost, s),
+                 "D2H outputs");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvD2H], s), "event");
+    return end_call(ctx);
+}
+
+int galop_trace_program(galop_ctx* ctx, const uint32_t* words, int64_t len, float* state, int64_t* n_traced) {
+    if (int rc = check_ready(ctx)) return rc;
+    if (len < 0 || (len > 0 && !words) || !state) return ctx->fail(GALOP_E_INVALID, "bad arguments");
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    const int k = pick_k(ctx);
+    const int64_t pass = 32LL * k;
+    const int64_t nt = std::min<int64_t>(pass, ctx->N);
+    if (n_traced) *n_traced = nt;
+    if (nt <= 0) return GALOP_OK;
+    begin_call(ctx, 1);
+    cudaStream_t s = ctx->stream;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], s), "event");
+    int64_t off[2] = {0, len};
+    if (int rc = upload_csr(ctx, words, off, 1)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvH2D], s), "event");
+    CsrSource src{ctx->raw_words.p, ctx->raw_off.p};
+    if (int rc = run_prepass(ctx, src, 1, len, false, false, nullptr)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvPrepass], s), "event");
+    const int nr = ctx->isa.num_registers;
+    const size_t cells = (size_t)(len + 1) * nr * pass;
+    GALOP_CK(ctx->trace.ensure(cells), "alloc trace");
+    if (int rc = run_interp(ctx, 1, kModeTrace, false, nullptr, nullptr, nullptr, ctx->trace.p, nullptr))
+        return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvInterp], s), "event");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvFinalize], s), "event");
+    std::vector<float> tmp(cells);
+    GALOP_CK(cudaMemcpyAsync(tmp.data(), ctx->trace.p, cells * sizeof(float), cudaMemcpyDeviceToHost, s),
+             "D2H trace");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvD2H], s), "event");
+    if (int rc = end_call(ctx)) return rc;
+    for (int64_t row = 0; row < (len + 1) * nr; ++row)
+        std::memcpy(state + row * nt, tmp.data() + row * pass, (size_t)nt * sizeof(float));
+    return GALOP_OK;
+}
+
+int galop_effective_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets, int64_t n_programs,
+                        int64_t* eff_len, uint32_t* eff_words) {
+    if (!ctx || !eff_len) return GALOP_E_INVALID;
+    if (n_programs < 0) return ctx->fail(GALOP_E_INVALID, "n_programs < 0");
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    begin_call(ctx, n_programs);
+    cudaStream_t s = ctx->stream;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], s), "event");
+    if (int rc = upload_csr(ctx, words, offsets, n_programs)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvH2D], s), "event");
+    GALOP_CK(ctx->eff_raw.ensure((size_t)std::max<int64_t>(offsets[n_programs], 1)), "alloc eff words");
+    CsrSource src{ctx->raw_words.p, ctx->raw_off.p};
+    if (int rc = run_prepass(ctx, src, n_programs, offsets[n_programs], true, false, ctx->eff_raw.p)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvPrepass], s), "event");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvInterp], s), "event");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvFinalize], s), "event");
+    std::vector<int64_t> off((size_t)n_programs + 1);
+    GALOP_CK(cudaMemcpyAsync(off.data(), ctx->eff_off.p, off.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, s),
+             "D2H eff offsets");
+    GALOP_CK(cudaStreamSynchronize(s), "sync");
+    for (int64_t i = 0; i < n_programs; ++i) eff_len[i] = off[i + 1] - off[i];
+    if (eff_words && off[n_programs] > 0)
+        GALOP_CK(cudaMemcpyAsync(eff_words, ctx->eff_raw.p, (size_t)off[n_programs] * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, s), "D2H eff words");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvD2H], s), "event");
+    return end_call(ctx);
+}
+
+}  // extern "C"

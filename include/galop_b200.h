@@ -1,0 +1,202 @@
+/*
+ * galop_b200.h -- C ABI of the B200 fitness evaluator for Galop's linear-GP
+ * symbolic regression.
+ *
+ * Plain C: pointers, sizes and status codes only.  Every call returns a
+ * galop_status (0 = success, negative = error; the message is in
+ * galop_last_error()).  No call terminates the process; the reference's
+ * ERR()/exit() convention (src/cuda_errors.h:3-15) is replaced by these codes.
+ *
+ * Semantics follow the reference exactly:
+ *   - instruction word layout  src/ISA.h:20-41 ([SRC2 mode|idx][SRC1][DEST][OP])
+ *   - op semantics             src/ISA.h:219-231 (REF profile)
+ *   - register init / output   src/Interpreter.cpp:36-59
+ *   - fitness                  src/Evaluator.cpp:11-45 + :88-91
+ *                              fitness = non-finite(mse) ? 0 : 1/(1+mse),
+ *                              mse = float(sse / N)
+ * Per-case outputs are bit-identical to the CPU interpreter for ADD, SUB,
+ * MUL, protected DIV, LT and GT; SIN, COS, EXP and LOG use CUDA's sinf,
+ * cosf, expf, logf (at most 2 ulp from the CPU's libm).
+ */
+#ifndef GALOP_B200_H
+#define GALOP_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GALOP_API __attribute__((visibility("default")))
+#else
+#define GALOP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GALOP_ABI_VERSION 1
+
+typedef enum {
+    GALOP_OK            = 0,
+    GALOP_E_INVALID     = -1,  /* bad argument (sizes, nulls, options)          */
+    GALOP_E_CUDA        = -2,  /* CUDA runtime error; see galop_last_error()    */
+    GALOP_E_NOMEM       = -3,  /* device or pinned allocation failed            */
+    GALOP_E_NO_DATASET  = -4,  /* evaluate called before galop_set_dataset()    */
+    GALOP_E_TIMEOUT     = -5,  /* a bounded device-side wait gave up            */
+    GALOP_E_CAPACITY    = -6,  /* request exceeds an admission or size limit    */
+    GALOP_E_NO_DEVICE   = -7,  /* no CUDA device / wrong architecture           */
+    GALOP_E_STATE       = -8   /* call not valid in the object's current state  */
+} galop_status;
+
+/* ISA profiles.  Both use the reference's 32-bit encoding and 3-bit opcode.
+ *   REF: ADD SUB MUL DIV SIN COS LT GT      (src/ISA.h:69-72)
+ *   BJ : ADD SUB MUL DIV SIN COS EXP LOG    (EXP, LOG unary on src2;
+ *        LOG(b) = b != 0 ? logf(|b|) : 0)                                    */
+typedef enum { GALOP_PROFILE_REF = 0, GALOP_PROFILE_BJ = 1 } galop_profile;
+
+/* SSE accumulation.
+ *   KAHAN32 : per-lane compensated FP32 sum of FP32 squared errors, FP64
+ *             across lanes, warps and case chunks.
+ *   FP64    : per-case error and square in FP64 (as src/Evaluator.cpp:38-39),
+ *             FP64 sums; only the summation order differs from the CPU.
+ *   ORDERED : FP64 terms summed strictly in case order 0..N-1, exactly as
+ *             src/Evaluator.cpp:23-42: fitness is bit-identical to the CPU
+ *             whenever the per-case outputs are.                             */
+typedef enum {
+    GALOP_REDUCE_KAHAN32 = 0,
+    GALOP_REDUCE_FP64    = 1,
+    GALOP_REDUCE_ORDERED = 2
+} galop_reduce;
+
+typedef struct {
+    int32_t profile;          /* galop_profile                                  */
+    int32_t num_registers;    /* 8 or 16 (src/LGPConfig.h:132-140)              */
+    int32_t input_protect;    /* 1: dest folded to the upper half, output
+                                 register NR/2 (src/LGPConfig.h:289-300)        */
+    int32_t reduce;           /* galop_reduce                                   */
+    const float* constants;   /* num_registers floats; NULL selects the
+                                 reference pool (src/LGPConfig.h:159-168)       */
+    int32_t device;           /* CUDA device ordinal                            */
+    int32_t intron_prepass;   /* 1: interpret only effective instructions
+                                 (src/Introns.h:28-57); outputs unchanged       */
+    int32_t cases_per_lane;   /* 0 = tuned default; else 1, 2, 4 or 8          */
+    int32_t warps_per_block;  /* 0 = tuned default; else 1..32                 */
+    int32_t reserved[4];
+} galop_options;
+
+typedef struct galop_ctx galop_ctx;
+
+/* Timings (CUDA events on the context's stream) and counts of the most
+ * recent evaluate call. */
+typedef struct {
+    int64_t n_programs;
+    int64_t n_cases;
+    int64_t raw_instructions;      /* sum of program lengths                    */
+    int64_t eff_instructions;      /* sum of interpreted (effective) lengths    */
+    double  h2d_ms;                /* host->device copies of the call           */
+    double  prepass_ms;            /* intron pass, compaction, scheduling       */
+    double  interp_ms;             /* interpreter kernel(s)                     */
+    double  finalize_ms;           /* cross-chunk reduction + fitness           */
+    double  d2h_ms;                /* device->host copies of the call           */
+    double  total_ms;              /* first to last event of the call           */
+    int32_t cases_per_lane;        /* configuration that ran                    */
+    int32_t warps_per_block;
+    int32_t blocks;
+    int32_t case_chunks;           /* work items per program                    */
+    int32_t kernels_launched;      /* this library's kernel launches            */
+    int32_t reserved[3];
+} galop_stats;
+
+/* ---- lifetime ------------------------------------------------------------ */
+
+/* Fill *opt with defaults: REF profile, 8 registers, no input protection,
+ * KAHAN32, reference constant pool, device 0, intron pre-pass on, tuned tile. */
+GALOP_API int galop_options_init(galop_options* opt);
+
+/* Replaces `new CudaEvaluator(...)` (src/EvaluatorCuda.cu:21-62): binds the
+ * device, creates a stream and events, uploads the constant pool. */
+GALOP_API int galop_create(const galop_options* opt, galop_ctx** out);
+GALOP_API void galop_destroy(galop_ctx* ctx);
+GALOP_API const char* galop_last_error(const galop_ctx* ctx);
+GALOP_API const char* galop_status_string(int status);
+GALOP_API int galop_abi_version(void);
+
+/* ---- dataset ------------------------------------------------------------- */
+
+/* Replaces CudaEvaluator::upload_dataset (src/EvaluatorCuda.cu:96-110).
+ * inputs: case-major, inputs[c*num_inputs + i] (src/Dataset.h:22-24);
+ * targets[c]; n_cases >= 0; 0 <= num_inputs <= num_registers.  The data are
+ * transposed on the device to feature-major and stay resident until the next
+ * call.  Host buffers are not retained. */
+GALOP_API int galop_set_dataset(galop_ctx* ctx, const float* inputs, const float* targets,
+                      int64_t n_cases, int32_t num_inputs);
+
+/* Same, with device pointers already holding the case-major data. */
+GALOP_API int galop_set_dataset_device(galop_ctx* ctx, const float* d_inputs, const float* d_targets,
+                             int64_t n_cases, int32_t num_inputs);
+
+/* ---- evaluation ---------------------------------------------------------- */
+
+/* The EvalBackend::evaluate_population boundary (src/EvalBackend.h:11-17,
+ * src/EvaluatorCuda.cu:298-469).  Program i is instructions[i*stride ..
+ * i*stride + lengths[i]).  Host pointers; returns with fitness_out filled. */
+GALOP_API int galop_evaluate_population(galop_ctx* ctx, const uint32_t* instructions,
+                              const uint8_t* lengths, int64_t stride, int64_t n_programs,
+                              float* fitness_out);
+
+/* Packed (CSR) layout of the reference (src/eval_kernels.cuh:292-303):
+ * program i is words[offsets[i] .. offsets[i+1]), int64 offsets, any length.
+ * Host pointers.  sse_out (may be NULL) receives the per-program SSE. */
+GALOP_API int galop_evaluate_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets,
+                       int64_t n_programs, float* fitness_out, double* sse_out);
+
+/* Device-resident form: all pointers are device memory on the context's
+ * device; work is ordered on `stream` (a cudaStream_t, or NULL for the
+ * context's own stream) and the call returns without synchronizing. */
+GALOP_API int galop_evaluate_csr_device(galop_ctx* ctx, const uint32_t* d_words, const int64_t* d_offsets,
+                              int64_t n_programs, float* d_fitness, double* d_sse, void* stream);
+
+/* Per-case outputs r[OUTPUT_REG] (src/Interpreter.cpp:54-57), host pointers:
+ * outputs[i*n_cases + c] for program i, case c. */
+GALOP_API int galop_case_outputs_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets,
+                           int64_t n_programs, float* outputs);
+
+/* Register-file trace of one program over the first min(32*cases_per_lane,
+ * n_cases) cases: state[(pc*num_registers + j)*n + c] = r_j of case c after
+ * pc instructions (pc = 0 is the initial file), n = number of traced cases.
+ * Runs the raw program (no intron pass).  For instruction-level parity. */
+GALOP_API int galop_trace_program(galop_ctx* ctx, const uint32_t* words, int64_t len,
+                        float* state, int64_t* n_traced);
+
+/* Intron pass only (src/Introns.h:28-57): eff_len[i] and the effective
+ * instructions of every program, packed program after program, in program
+ * order (raw encoding).  eff_words may be NULL. */
+GALOP_API int galop_effective_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets,
+                        int64_t n_programs, int64_t* eff_len, uint32_t* eff_words);
+
+GALOP_API int galop_last_stats(const galop_ctx* ctx, galop_stats* out);
+
+/* Blocks until the context's stream is idle. */
+GALOP_API int galop_synchronize(galop_ctx* ctx);
+
+/* CUDA-event timers on the context's stream: record marker `slot` (0..7);
+ * elapsed milliseconds between two recorded markers (waits for `slot_b`). */
+GALOP_API int galop_timer_record(galop_ctx* ctx, int32_t slot);
+GALOP_API int galop_timer_elapsed(galop_ctx* ctx, int32_t slot_a, int32_t slot_b, double* ms);
+
+/* Page-locked host memory for staging populations and fitness (the
+ * reference's cudaMallocHost staging, src/EvaluatorCuda.cu:40-51): copies
+ * from it run at full link speed and overlap with device work. */
+GALOP_API int galop_host_alloc(int64_t bytes, void** out);
+GALOP_API int galop_host_free(void* p);
+
+/* Device memory on the context's device (for callers that keep populations
+ * resident and use galop_evaluate_csr_device). */
+GALOP_API int galop_device_alloc(galop_ctx* ctx, int64_t bytes, void** out);
+GALOP_API int galop_device_free(galop_ctx* ctx, void* p);
+GALOP_API int galop_memcpy_h2d(galop_ctx* ctx, void* dst, const void* src, int64_t bytes);
+GALOP_API int galop_memcpy_d2h(galop_ctx* ctx, void* dst, const void* src, int64_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GALOP_B200_H */

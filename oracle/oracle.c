@@ -1,0 +1,323 @@
+/*
+ * oracle.c -- CPU restatement of Galop's linear-GP fitness evaluation.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA path is
+ * compared against; it is never linked into, loaded by, or called from the
+ * product library (galop_b200/csrc).  Only tests/, the smoke check in
+ * __graft_entry__.py and the cpu_baseline / --impl reference legs of bench.py
+ * load it.
+ *
+ * It restates, with runtime parameters instead of compile-time ones, the
+ * reference's evaluation path:
+ *
+ *   decode           src/ISA.h:176-206   (get_op, get_dest_index incl. the
+ *                                         INPUT_PROTECT fold :183-185,
+ *                                         get_src1_index, get_src2_index,
+ *                                         is_src2_constant)
+ *   apply_op         src/ISA.h:219-231
+ *   run_stateless    src/Interpreter.cpp:36-59 (inputs -> r0..k-1, the rest
+ *                                         0, output register OUTPUT_REG)
+ *   execute          src/Interpreter.cpp:11-34
+ *   evaluate_sr_mse  src/Evaluator.cpp:11-45 (double SSE summed in case
+ *                                         order, float(sse/N))
+ *   mse_to_fitness   src/Evaluator.cpp:88-91
+ *   evaluate_pop.    src/EvaluatorCpu.cpp:7-15
+ *   effective_mask   src/Introns.h:28-46
+ *   extract_effect.  src/Introns.h:50-57
+ *
+ * Two ISA profiles share the reference's 32-bit encoding (src/ISA.h:20-41):
+ *   REF: ops ADD SUB MUL DIV SIN COS LT GT  (src/ISA.h:69-72), bit-compatible
+ *        with the reference; parity pinned by its tests and golden files.
+ *   BJ : ops ADD SUB MUL DIV SIN COS EXP LOG, runtime constant pool.  EXP and
+ *        LOG are unary like SIN/COS (they read src2 only).  Protected log is
+ *        LOG(b) = (b != 0) ? logf(|b|) : 0.  No reference test covers EXP/LOG:
+ *        parity for those two opcodes is unpinned.
+ *
+ * Build: see oracle/Makefile.  Compiled with -O2 -ffp-contract=off and no
+ * fast-math so that float arithmetic rounds exactly like the reference's
+ * g++ -std=c++20 -O2 build (ISO mode, no FMA contraction, SSE2 arithmetic).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+enum { ORC_PROFILE_REF = 0, ORC_PROFILE_BJ = 1 };
+enum { OP_ADD = 0, OP_SUB, OP_MUL, OP_DIV, OP_SIN, OP_COS, OP_6, OP_7 };
+
+typedef struct {
+    int32_t profile;        /* ORC_PROFILE_REF or ORC_PROFILE_BJ             */
+    int32_t num_registers;  /* power of two, 2..128                          */
+    int32_t input_protect;  /* 1: dest folded into the upper register half   */
+    int32_t reserved;
+    const float* constants; /* num_registers entries (pool size == NR)       */
+} orc_isa_t;
+
+typedef struct {
+    uint8_t op, dest, src1, src2, is_const, unary;
+} orc_ins_t;
+
+/* Output register: r0, or the first scratch register NR/2 under
+ * INPUT_PROTECT (src/LGPConfig.h:294-300). */
+int orc_output_reg(const orc_isa_t* isa) {
+    return isa->input_protect ? isa->num_registers / 2 : 0;
+}
+
+/* Field extraction, src/ISA.h:176-206.  The opcode field is 3 bits wide
+ * (OPERATION_MASK = 7, src/LGPConfig.h:189-191); register fields are masked
+ * with NR-1; src2's index uses the same mask, its bit 7 is the mode flag. */
+static inline orc_ins_t orc_decode_word(const orc_isa_t* isa, uint32_t w) {
+    const uint32_t rmask = (uint32_t)isa->num_registers - 1u;
+    orc_ins_t d;
+    d.op = (uint8_t)(w & 7u);
+    if (isa->input_protect)
+        d.dest = (uint8_t)(orc_output_reg(isa) + ((w >> 8) & (rmask >> 1)));
+    else
+        d.dest = (uint8_t)((w >> 8) & rmask);
+    d.src1 = (uint8_t)((w >> 16) & rmask);
+    d.src2 = (uint8_t)((w >> 24) & rmask);
+    d.is_const = (uint8_t)(((w >> 24) & 0x80u) != 0);
+    d.unary = (uint8_t)(d.op == OP_SIN || d.op == OP_COS ||
+                        (isa->profile == ORC_PROFILE_BJ && (d.op == OP_6 || d.op == OP_7)));
+    return d;
+}
+
+int orc_decode(const orc_isa_t* isa, uint32_t w, int32_t* out5) {
+    orc_ins_t d = orc_decode_word(isa, w);
+    out5[0] = d.op; out5[1] = d.dest; out5[2] = d.src1; out5[3] = d.src2; out5[4] = d.is_const;
+    return d.unary;
+}
+
+/* Op semantics, src/ISA.h:219-231 for REF; BJ swaps LT/GT for EXP/LOG. */
+float orc_apply_op(int profile, int op, float a, float b) {
+    switch (op) {
+        case OP_ADD: return a + b;
+        case OP_SUB: return a - b;
+        case OP_MUL: return a * b;
+        case OP_DIV: return (b != 0.0f) ? a / b : 1.0f;
+        case OP_SIN: return sinf(b);
+        case OP_COS: return cosf(b);
+        case OP_6:
+            if (profile == ORC_PROFILE_BJ) return expf(b);
+            return (a < b) ? 1.0f : 0.0f;
+        default:
+            if (profile == ORC_PROFILE_BJ) return (b != 0.0f) ? logf(fabsf(b)) : 0.0f;
+            return (a > b) ? 1.0f : 0.0f;
+    }
+}
+
+/* The same op semantics in double precision: the precision-stability probe
+ * the reference's differential test uses (tests/cuda_diff.cu:92-144). */
+static inline double orc_apply_op_f64(int profile, int op, double a, double b) {
+    switch (op) {
+        case OP_ADD: return a + b;
+        case OP_SUB: return a - b;
+        case OP_MUL: return a * b;
+        case OP_DIV: return (b != 0.0) ? a / b : 1.0;
+        case OP_SIN: return sin(b);
+        case OP_COS: return cos(b);
+        case OP_6:
+            if (profile == ORC_PROFILE_BJ) return exp(b);
+            return (a < b) ? 1.0 : 0.0;
+        default:
+            if (profile == ORC_PROFILE_BJ) return (b != 0.0) ? log(fabs(b)) : 0.0;
+            return (a > b) ? 1.0 : 0.0;
+    }
+}
+
+static orc_ins_t* orc_decode_program(const orc_isa_t* isa, const uint32_t* prog, int64_t len) {
+    orc_ins_t* p = (orc_ins_t*)malloc(sizeof(orc_ins_t) * (size_t)(len > 0 ? len : 1));
+    for (int64_t i = 0; i < len; ++i) p[i] = orc_decode_word(isa, prog[i]);
+    return p;
+}
+
+/* One fitness case: registers r0..k-1 = inputs, the rest 0
+ * (src/Interpreter.cpp:47-56), run every instruction (execute,
+ * src/Interpreter.cpp:11-34), return r[OUTPUT_REG]. */
+static inline float orc_run_case(const orc_isa_t* isa, const orc_ins_t* p, int64_t len,
+                                 const float* x, int num_inputs) {
+    float r[128];
+    const int nr = isa->num_registers;
+    for (int i = 0; i < num_inputs; ++i) r[i] = x[i];
+    for (int i = num_inputs; i < nr; ++i) r[i] = 0.0f;
+    for (int64_t pc = 0; pc < len; ++pc) {
+        const orc_ins_t in = p[pc];
+        const float a = r[in.src1];
+        const float b = in.is_const ? isa->constants[in.src2] : r[in.src2];
+        r[in.dest] = orc_apply_op(isa->profile, in.op, a, b);
+    }
+    return r[orc_output_reg(isa)];
+}
+
+static inline double orc_run_case_f64(const orc_isa_t* isa, const orc_ins_t* p, int64_t len,
+                                      const float* x, int num_inputs) {
+    double r[128];
+    const int nr = isa->num_registers;
+    for (int i = 0; i < num_inputs; ++i) r[i] = (double)x[i];
+    for (int i = num_inputs; i < nr; ++i) r[i] = 0.0;
+    for (int64_t pc = 0; pc < len; ++pc) {
+        const orc_ins_t in = p[pc];
+        const double a = r[in.src1];
+        const double b = in.is_const ? (double)isa->constants[in.src2] : r[in.src2];
+        r[in.dest] = orc_apply_op_f64(isa->profile, in.op, a, b);
+    }
+    return r[orc_output_reg(isa)];
+}
+
+/* Per-case outputs of one program; inputs are case-major (AoS),
+ * inputs[c*num_inputs + i] as in src/Dataset.h:22-24. */
+void orc_case_outputs(const orc_isa_t* isa, const uint32_t* prog, int64_t len,
+                      const float* inputs, int num_inputs, int64_t n_cases, float* out) {
+    orc_ins_t* p = orc_decode_program(isa, prog, len);
+    for (int64_t c = 0; c < n_cases; ++c)
+        out[c] = orc_run_case(isa, p, len, inputs + c * num_inputs, num_inputs);
+    free(p);
+}
+
+void orc_case_outputs_f64(const orc_isa_t* isa, const uint32_t* prog, int64_t len,
+                          const float* inputs, int num_inputs, int64_t n_cases, double* out) {
+    orc_ins_t* p = orc_decode_program(isa, prog, len);
+    for (int64_t c = 0; c < n_cases; ++c)
+        out[c] = orc_run_case_f64(isa, p, len, inputs + c * num_inputs, num_inputs);
+    free(p);
+}
+
+/* Register-file trace: state[(pc+1)*nr + j] = r_j after instruction pc, with
+ * state[0..nr) the initial file.  One case.  Used to replay each instruction
+ * of a GPU trace in isolation. */
+void orc_trace_case(const orc_isa_t* isa, const uint32_t* prog, int64_t len,
+                    const float* x, int num_inputs, float* state) {
+    const int nr = isa->num_registers;
+    float r[128];
+    for (int i = 0; i < num_inputs; ++i) r[i] = x[i];
+    for (int i = num_inputs; i < nr; ++i) r[i] = 0.0f;
+    memcpy(state, r, sizeof(float) * (size_t)nr);
+    for (int64_t pc = 0; pc < len; ++pc) {
+        const orc_ins_t in = orc_decode_word(isa, prog[pc]);
+        const float a = r[in.src1];
+        const float b = in.is_const ? isa->constants[in.src2] : r[in.src2];
+        r[in.dest] = orc_apply_op(isa->profile, in.op, a, b);
+        memcpy(state + (size_t)(pc + 1) * nr, r, sizeof(float) * (size_t)nr);
+    }
+}
+
+/* SSE in double, accumulated in case order 0..N-1 (src/Evaluator.cpp:20-42):
+ * err = double(out) - double(target); sse += err*err. */
+double orc_sse(const orc_isa_t* isa, const uint32_t* prog, int64_t len,
+               const float* inputs, const float* targets, int num_inputs, int64_t n_cases) {
+    orc_ins_t* p = orc_decode_program(isa, prog, len);
+    double sse = 0.0;
+    for (int64_t c = 0; c < n_cases; ++c) {
+        const float o = orc_run_case(isa, p, len, inputs + c * num_inputs, num_inputs);
+        const double err = (double)o - (double)targets[c];
+        sse += err * err;
+    }
+    free(p);
+    return sse;
+}
+
+/* src/Evaluator.cpp:44: float(sse / double(N)). */
+float orc_evaluate_sr_mse(const orc_isa_t* isa, const uint32_t* prog, int64_t len,
+                          const float* inputs, const float* targets, int num_inputs,
+                          int64_t n_cases) {
+    const double sse = orc_sse(isa, prog, len, inputs, targets, num_inputs, n_cases);
+    return (float)(sse / (double)n_cases);
+}
+
+/* src/Evaluator.cpp:88-91. */
+float orc_mse_to_fitness(float mse) {
+    if (!isfinite(mse)) return 0.0f;
+    return 1.0f / (1.0f + mse);
+}
+
+/* Population evaluation over CSR programs: program i is
+ * words[offsets[i] : offsets[i+1]].  The loop over programs follows
+ * src/EvaluatorCpu.cpp:7-15; `threads` > 1 runs it as an OpenMP parallel for
+ * (each program is still evaluated serially, so results do not depend on the
+ * thread count).  sse_out may be NULL. */
+void orc_evaluate_population_csr(const orc_isa_t* isa, const uint32_t* words,
+                                 const int64_t* offsets, int64_t n_programs,
+                                 const float* inputs, const float* targets, int num_inputs,
+                                 int64_t n_cases, float* fitness_out, double* sse_out,
+                                 int threads) {
+#ifdef _OPENMP
+    if (threads < 1) threads = omp_get_max_threads();
+    #pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
+#endif
+    for (int64_t i = 0; i < n_programs; ++i) {
+        const double sse = orc_sse(isa, words + offsets[i], offsets[i + 1] - offsets[i],
+                                   inputs, targets, num_inputs, n_cases);
+        if (sse_out) sse_out[i] = sse;
+        fitness_out[i] = orc_mse_to_fitness((float)(sse / (double)n_cases));
+    }
+    (void)threads;
+}
+
+/* Dense layout of the EvalBackend boundary (src/EvalBackend.h:11-17):
+ * program i at instructions + i*stride, lengths[i] instructions. */
+void orc_evaluate_population_dense(const orc_isa_t* isa, const uint32_t* instructions,
+                                   const uint8_t* lengths, int64_t stride, int64_t n_programs,
+                                   const float* inputs, const float* targets, int num_inputs,
+                                   int64_t n_cases, float* fitness_out) {
+    for (int64_t i = 0; i < n_programs; ++i) {
+        const float mse = orc_evaluate_sr_mse(isa, instructions + i * stride, lengths[i],
+                                              inputs, targets, num_inputs, n_cases);
+        fitness_out[i] = orc_mse_to_fitness(mse);
+    }
+}
+
+/* Backward liveness, src/Introns.h:28-46.  live = {OUTPUT_REG}; an
+ * instruction is effective iff its dest is live; then dest is killed and the
+ * registers it reads become live (unary ops read only src2; a constant src2
+ * reads no register). */
+int64_t orc_effective_mask(const orc_isa_t* isa, const uint32_t* prog, int64_t len,
+                           uint8_t* mask) {
+    uint8_t live[128];
+    memset(live, 0, sizeof(live));
+    live[orc_output_reg(isa)] = 1;
+    int64_t cnt = 0;
+    for (int64_t i = len - 1; i >= 0; --i) {
+        const orc_ins_t in = orc_decode_word(isa, prog[i]);
+        if (!live[in.dest]) { mask[i] = 0; continue; }
+        mask[i] = 1; ++cnt;
+        live[in.dest] = 0;
+        if (!in.unary) live[in.src1] = 1;
+        if (!in.is_const) live[in.src2] = 1;
+    }
+    return cnt;
+}
+
+/* src/Introns.h:50-57: effective instructions in program order. */
+int64_t orc_extract_effective(const orc_isa_t* isa, const uint32_t* prog, int64_t len,
+                              uint32_t* out) {
+    uint8_t* mask = (uint8_t*)malloc((size_t)(len > 0 ? len : 1));
+    const int64_t cnt = orc_effective_mask(isa, prog, len, mask);
+    int64_t k = 0;
+    for (int64_t i = 0; i < len; ++i)
+        if (mask[i]) out[k++] = prog[i];
+    free(mask);
+    return cnt;
+}
+
+/* Effective lengths of a CSR population (OpenMP over programs). */
+void orc_effective_lengths_csr(const orc_isa_t* isa, const uint32_t* words,
+                               const int64_t* offsets, int64_t n_programs, int64_t* eff_len) {
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n_programs; ++i) {
+        const int64_t len = offsets[i + 1] - offsets[i];
+        uint8_t* mask = (uint8_t*)malloc((size_t)(len > 0 ? len : 1));
+        eff_len[i] = orc_effective_mask(isa, words + offsets[i], len, mask);
+        free(mask);
+    }
+}
+
+int orc_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

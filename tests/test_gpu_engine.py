@@ -1,0 +1,49 @@
+"""The reference's LGPEngine driving the B200 backend (galop::B200Evaluator,
+include/galop_b200_backend.hpp) on the 9 golden cells (3 Nguyen targets x 3
+seeds, 1000 generations, P=1000, 32 cases).
+
+The backend runs in ORDERED mode, so fitness is bit-identical to the CPU's
+whenever the per-case outputs are.  SIN and COS may differ from glibc by up
+to 2 ulp, so a history can legitimately part from the golden one once such
+a difference changes a selection decision; the test reports how far each
+cell matches and requires the initial generation of every cell, and the
+whole history of most cells, to match byte for byte."""
+from __future__ import annotations
+
+import gzip
+
+import pytest
+
+from conftest import GOLDEN, ROOT
+from test_oracle import _golden_cells, run_golden
+
+pytestmark = pytest.mark.gpu
+
+EXE = ROOT / "oracle" / "_ref" / "lgp_run_b200"
+
+
+def _lines(p):
+    return p.read_text().splitlines() if hasattr(p, "read_text") else p.splitlines()
+
+
+@pytest.mark.skipif(not EXE.exists(), reason="oracle/_ref/lgp_run_b200 not built")
+def test_golden_cells_with_b200_backend(tmp_path, capsys):
+    cells = _golden_cells()
+    run_golden(EXE, tmp_path, cells)
+    full = 0
+    report = []
+    for t, s in cells:
+        gold = gzip.open(GOLDEN / "histories" / f"hist_{t}_s{s}.csv.gz").read().decode().splitlines()
+        mine = (tmp_path / f"hist_{t}_s{s}.csv").read_text().splitlines()
+        assert len(mine) == len(gold)
+        same = 0
+        for a, b in zip(mine, gold):
+            if a != b:
+                break
+            same += 1
+        assert same >= 2, f"{t} s{s}: header or generation 0 differs"
+        full += same == len(gold)
+        report.append(f"{t} s{s}: {same - 1}/{len(gold) - 1} generations identical")
+    with capsys.disabled():
+        print("\n" + "\n".join(report))
+    assert full >= 5, report

@@ -1,0 +1,339 @@
+"""Parity of the CUDA path (called through the C ABI) with the reference.
+
+Bar (the same one the C ABI header states):
+* per-case outputs bit-identical for ADD, SUB, MUL, protected DIV, LT, GT
+  (NaN results compare as NaN: the payload bits are not part of the ISA);
+* SIN, COS, EXP, LOG within 2 ulp of the CPU's libm result, checked one
+  instruction at a time by replaying a GPU register-file trace;
+* fitness bit-identical in ORDERED mode whenever the outputs are; within
+  1e-6 relative in KAHAN32/FP64 mode;
+* programs whose effective code has transcendental ops are held to the
+  reference's own GPU gate (tests/cuda_diff.cu:82-182): |d fitness| < 1e-4
+  unless the program is precision-chaotic (its float and double CPU fitness
+  differ by more than 1e-4), and at most 1% of programs over tolerance.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import galop_b200 as g
+from galop_b200 import workloads as W
+from conftest import GOLDEN, bits, load_vectors
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = {"nr8": (8, False), "nr16": (16, False), "ip16": (16, True)}
+IEEE_REF = {0, 1, 2, 3, 6, 7}
+IEEE_BJ = {0, 1, 2, 3}
+
+
+def ordered(x: np.ndarray) -> np.ndarray:
+    i = np.ascontiguousarray(x, dtype=np.float32).view(np.int32).astype(np.int64)
+    return np.where(i < 0, -(i & 0x7FFFFFFF), i)
+
+
+def ulp_dist(a, b) -> np.ndarray:
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    d = np.abs(ordered(a) - ordered(b))
+    both_nan = np.isnan(a) & np.isnan(b)
+    one_nan = np.isnan(a) ^ np.isnan(b)
+    return np.where(both_nan, 0, np.where(one_nan, 1 << 40, d))
+
+
+def same_or_nan(a, b) -> np.ndarray:
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    return (bits(a) == bits(b)) | (np.isnan(a) & np.isnan(b))
+
+
+@pytest.fixture(scope="module")
+def orc(oracle_lib):
+    return oracle_lib
+
+
+def program_is_ieee(o, prog, profile) -> bool:
+    m = o.effective_mask(prog)
+    ops = set((prog[m] & 7).tolist())
+    return ops <= (IEEE_REF if profile == g.PROFILE_REF else IEEE_BJ)
+
+
+# --- single instructions ----------------------------------------------------------
+
+@pytest.mark.parametrize("k", [1, 4])
+def test_apply_op_against_reference_vectors(native, k):
+    """Every opcode on special and random operands (golden values recorded
+    from the reference's ISA::apply_op)."""
+    with np.load(GOLDEN / "ops_ref.npz") as z:
+        a, b, out = z["a"], z["b"], z["out"]
+    X = np.stack([a, b], axis=1)
+    ds = g.Dataset(X, np.zeros(a.size, np.float32))
+    with g.Evaluator(num_registers=8, cases_per_lane=k, intron_prepass=False) as ev:
+        ev.set_dataset(ds)
+        for op in range(8):
+            prog = W.encode([op], [0], [0], [1], [0])
+            got = ev.case_outputs(prog, np.array([0, 1], np.int64))[0]
+            if op in (4, 5):
+                d = ulp_dist(got, out[op])
+                assert d.max() <= 2, (op, int(d.max()))
+            else:
+                ok = same_or_nan(got, out[op])
+                assert ok.all(), (op, a[~ok][:5], b[~ok][:5], got[~ok][:5], out[op][~ok][:5])
+
+
+def test_bj_exp_log_within_2ulp(native, orc):
+    rng = np.random.default_rng(5)
+    x = np.concatenate([rng.uniform(-100, 100, 20000), rng.standard_normal(20000) * 1e3,
+                        np.array([0.0, -0.0, 1e-40, -1e-40, np.inf, -np.inf, np.nan, 88.72, 88.73, -103.9])
+                        ]).astype(np.float32)
+    o = orc.Oracle(orc.PROFILE_BJ, 8)
+    ds = g.Dataset(x.reshape(-1, 1), np.zeros_like(x))
+    with g.Evaluator(profile=g.PROFILE_BJ, num_registers=8) as ev:
+        ev.set_dataset(ds)
+        for op in (6, 7):
+            prog = W.encode([op], [0], [3], [0], [0])
+            got = ev.case_outputs(prog, np.array([0, 1], np.int64))[0]
+            want = o.case_outputs(prog, x.reshape(-1, 1))
+            assert ulp_dist(got, want).max() <= 2, op
+
+
+# --- golden vectors recorded from the reference ---------------------------------
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+@pytest.mark.parametrize("k", [2, 8])
+def test_golden_vectors_outputs_and_fitness(native, orc, variant, k):
+    v = load_vectors(variant)
+    nr, ip = VARIANTS[variant]
+    o = orc.Oracle(orc.PROFILE_REF, nr, ip)
+    words, off = v["words"], v["offsets"]
+    n = len(off) - 1
+    ieee = np.array([program_is_ieee(o, words[off[i]:off[i + 1]], g.PROFILE_REF) for i in range(n)])
+    assert ieee.sum() > 100
+    with g.Evaluator(num_registers=nr, input_protect=ip, reduce=g.REDUCE_ORDERED, cases_per_lane=k) as ev, \
+            g.Evaluator(num_registers=nr, input_protect=ip, reduce=g.REDUCE_KAHAN32, cases_per_lane=k) as ek:
+        for d in ("d1", "d2", "d3", "d4"):
+            ds = g.Dataset(v[f"{d}_X"], v[f"{d}_y"])
+            outs = ev.case_outputs(words, off, ds)
+            ref = v[f"{d}_outputs"]
+            ok = same_or_nan(outs, ref).all(axis=1)
+            assert ok[ieee].all(), (d, np.nonzero(ieee & ~ok)[0][:10])
+            fit = ev.evaluate_csr(words, off, ds)
+            reff = v[f"{d}_fitness"]
+            exact = bits(fit) == bits(reff)
+            assert exact[ieee].all(), (d, np.nonzero(ieee & ~exact)[0][:10])
+            # programs with transcendental effective code: identical outputs give
+            # identical fitness; otherwise the reference's GPU gate applies
+            assert exact[ok].all()
+            fk = ek.evaluate_csr(words, off, ds)
+            rel = np.abs(fk.astype(np.float64) - reff) / np.maximum(np.abs(reff), 1e-30)
+            assert (rel[ieee] <= 1e-6).all(), d
+            over = np.abs(fit.astype(np.float64) - reff) > 1e-4
+            assert over.sum() <= max(1, n // 100), d
+
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+def test_dense_layout_matches_csr_bitwise(native, variant):
+    """EvalBackend dense layout (stride MAX_PROGRAM_SIZE, uint8 lengths) and
+    the packed layout give bit-identical fitness (tests/cuda_diff.cu:194-203)."""
+    v = load_vectors(variant)
+    nr, ip = VARIANTS[variant]
+    words, off = v["words"], v["offsets"]
+    stride = int(v["max_program_size"])
+    n = len(off) - 1
+    dense = np.zeros((n, stride), np.uint32)
+    lens = np.diff(off).astype(np.uint8)
+    for i in range(n):
+        dense[i, :lens[i]] = words[off[i]:off[i + 1]]
+    ds = g.Dataset(v["d3_X"], v["d3_y"])
+    with g.Evaluator(num_registers=nr, input_protect=ip) as ev:
+        a = ev.evaluate_csr(words, off, ds)
+        b = ev.evaluate_population(dense, lens, None, n, ds)
+    assert np.array_equal(bits(a), bits(b))
+    w2, off2 = g.csr_from_dense(dense, lens, stride)
+    assert np.array_equal(w2, words) and np.array_equal(off2, off)
+
+
+# --- instruction-level replay -------------------------------------------------------
+
+@pytest.mark.parametrize("profile,nr", [(g.PROFILE_REF, 8), (g.PROFILE_REF, 16), (g.PROFILE_BJ, 8),
+                                        (g.PROFILE_BJ, 16)])
+def test_trace_replay_every_instruction(native, orc, profile, nr):
+    """Each GPU instruction, fed the GPU's own register file, reproduces the
+    CPU's apply_op: bit-exact for IEEE ops, <= 2 ulp for SIN/COS/EXP/LOG."""
+    rng = np.random.default_rng(7 + nr + profile)
+    o = orc.Oracle(profile, nr)
+    X = rng.uniform(-4, 4, size=(256, min(5, nr))).astype(np.float32)
+    ds = g.Dataset(X, np.zeros(256, np.float32))
+    with g.Evaluator(profile=profile, num_registers=nr, cases_per_lane=4) as ev:
+        ev.set_dataset(ds)
+        for _ in range(12):
+            prog = W.random_words(rng, int(rng.integers(1, 120)), nr)
+            st = ev.trace(prog)                       # (L+1, NR, n)
+            n = st.shape[2]
+            k = X.shape[1]
+            init = np.zeros((nr, n), np.float32)
+            init[:k] = X[:n].T
+            assert same_or_nan(st[0], init).all()
+            for pc, w in enumerate(prog):
+                op, d, s1, s2, kc, _ = o.decode(int(w))
+                a = st[pc, s1]
+                b = np.full(n, o.constants[s2], np.float32) if kc else st[pc, s2]
+                want = np.array([o.apply_op(op, float(x), float(y)) for x, y in zip(a, b)], np.float32)
+                got = st[pc + 1, d]
+                exact_op = op in (IEEE_REF if profile == g.PROFILE_REF else IEEE_BJ)
+                if exact_op:
+                    assert same_or_nan(got, want).all(), (pc, op)
+                else:
+                    assert ulp_dist(got, want).max() <= 2, (pc, op)
+                other = np.ones(nr, bool)
+                other[d] = False
+                assert same_or_nan(st[pc + 1][other], st[pc][other]).all()
+
+
+# --- the intron pre-pass ---------------------------------------------------------------
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+def test_gpu_intron_pass_matches_reference_masks(native, variant):
+    v = load_vectors(variant)
+    nr, ip = VARIANTS[variant]
+    words, off, masks = v["words"], v["offsets"], v["masks"].astype(bool)
+    with g.Evaluator(num_registers=nr, input_protect=ip) as ev:
+        eff_len, eff_words = ev.effective(words, off)
+    want_len = np.array([masks[off[i]:off[i + 1]].sum() for i in range(len(off) - 1)])
+    assert np.array_equal(eff_len, want_len)
+    assert np.array_equal(eff_words, words[masks])
+
+
+def test_prepass_on_off_and_tile_shapes_bitwise(native):
+    """Intron removal and every cases-per-lane / warps-per-block choice give
+    bit-identical per-case outputs and fitness."""
+    wl = W.single_generation(seed=9, n_programs=600, n_cases=777)
+    ds = g.Dataset(wl.X, wl.y)
+    base = None
+    for pre in (True, False):
+        for k in (1, 2, 4, 8):
+            for wpb in (1, 4, 8):
+                with g.Evaluator(num_registers=16, intron_prepass=pre, cases_per_lane=k, warps_per_block=wpb,
+                                 reduce=g.REDUCE_ORDERED) as ev:
+                    outs = ev.case_outputs(wl.words, wl.offsets, ds)
+                    fit = ev.evaluate_csr(wl.words, wl.offsets, ds)
+                if base is None:
+                    base = (outs, fit)
+                assert np.array_equal(bits(outs), bits(base[0])), (pre, k, wpb)
+                assert np.array_equal(bits(fit), bits(base[1])), (pre, k, wpb)
+
+
+# --- reductions ------------------------------------------------------------------------
+
+def test_reduction_modes_against_fp64_sum_of_gpu_outputs(native):
+    """With per-case outputs fixed (the GPU's own), ORDERED equals the CPU's
+    case-order double sum bit for bit; FP64 and KAHAN32 are within 1e-12 and
+    1e-6 relative of it.  Targets of magnitude ~1e4 stress the accumulation."""
+    rng = np.random.default_rng(3)
+    n_cases = 70001
+    X = (rng.standard_normal((n_cases, 4)) * 10).astype(np.float32)
+    isa = W.IsaSpec(g.PROFILE_REF, 16)
+    y = (rng.standard_normal(n_cases) * 1e4 + 3e4).astype(np.float32)
+    lens = W.uniform_lengths(rng, 300, 4, 60)
+    words, off = W.structured_population(rng, lens, isa, 0.7)
+    ds = g.Dataset(X, y)
+    res = {}
+    for mode in (g.REDUCE_ORDERED, g.REDUCE_FP64, g.REDUCE_KAHAN32):
+        with g.Evaluator(num_registers=16, reduce=mode) as ev:
+            outs = ev.case_outputs(words, off, ds)
+            res[mode] = ev.evaluate_csr(words, off, ds, with_sse=True)
+    err = outs.astype(np.float64) - y.astype(np.float64)
+    seq = np.zeros(len(off) - 1)
+    for i in range(len(off) - 1):
+        s = 0.0
+        for e in err[i]:
+            s += e * e
+        seq[i] = s
+    fin = np.isfinite(seq)
+    assert np.array_equal(res[g.REDUCE_ORDERED][1][fin], seq[fin])
+    rel64 = np.abs(res[g.REDUCE_FP64][1][fin] - seq[fin]) / seq[fin]
+    rel32 = np.abs(res[g.REDUCE_KAHAN32][1][fin] - seq[fin]) / seq[fin]
+    assert rel64.max() <= 1e-12
+    assert rel32.max() <= 1e-6
+
+
+# --- edge cases ------------------------------------------------------------------------
+
+def test_edge_cases(native, orc):
+    o = orc.Oracle(orc.PROFILE_REF, 8)
+    rng = np.random.default_rng(4)
+    words, off = W.random_population(rng, np.array([0, 1, 5, 0, 50]), 8)
+    with g.Evaluator(num_registers=8, reduce=g.REDUCE_ORDERED) as ev:
+        with pytest.raises(g.GalopError) as e:
+            ev.evaluate_csr(words, off)
+        assert e.value.status == g.E_NO_DATASET
+        for n_cases, k in ((0, 1), (1, 1), (31, 2), (33, 0), (1025, 8)):
+            X = rng.uniform(-1, 1, (n_cases, k)).astype(np.float32)
+            y = rng.uniform(-1, 1, n_cases).astype(np.float32)
+            ds = g.Dataset(X, y)
+            fit = ev.evaluate_csr(words, off, ds)
+            want = o.evaluate_csr(words, off, X, y)
+            ieee = np.array([program_is_ieee(o, words[off[i]:off[i + 1]], 0) for i in range(len(off) - 1)])
+            assert np.array_equal(bits(fit)[ieee], bits(want)[ieee]), n_cases
+            if n_cases == 0:
+                assert np.all(fit == 0.0)
+        empty = ev.evaluate_csr(np.zeros(0, np.uint32), np.zeros(1, np.int64))
+        assert empty.shape == (0,)
+        with pytest.raises(g.GalopError) as e:
+            ev.set_dataset(g.Dataset(np.zeros((4, 9), np.float32), np.zeros(4, np.float32)))
+        assert e.value.status == g.E_INVALID
+        ev.set_dataset(g.Dataset(np.zeros((4, 1), np.float32), np.zeros(4, np.float32)))
+        with pytest.raises(g.GalopError) as e:
+            ev.evaluate_csr(words, np.array([0, 3, 2, 5, 5, 56], np.int64))
+        assert e.value.status == g.E_INVALID
+        with pytest.raises(g.GalopError) as e:
+            ev.evaluate_population(np.zeros((2, 4), np.uint32), np.array([3, 5], np.uint8), stride=4)
+        assert e.value.status == g.E_INVALID
+
+
+def test_case_chunking_large_n_few_programs(native, orc):
+    """Few programs over many cases split each program into case chunks
+    whose partial sums are combined in chunk order."""
+    rng = np.random.default_rng(8)
+    isa = W.IsaSpec(g.PROFILE_REF, 8)
+    n_cases = 300_000
+    X = rng.uniform(-2, 2, (n_cases, 2)).astype(np.float32)
+    y = rng.uniform(-1, 1, n_cases).astype(np.float32)
+    words, off = W.structured_population(rng, W.uniform_lengths(rng, 8, 5, 40), isa, 0.8)
+    o = orc.Oracle(orc.PROFILE_REF, 8)
+    want, sse = o.evaluate_csr(words, off, X, y, with_sse=True)
+    with g.Evaluator(num_registers=8, reduce=g.REDUCE_FP64) as ev:
+        fit, gsse = ev.evaluate_csr(words, off, g.Dataset(X, y), with_sse=True)
+        assert ev.stats.case_chunks > 1
+    ieee = np.array([program_is_ieee(o, words[off[i]:off[i + 1]], 0) for i in range(len(off) - 1)])
+    fin = np.isfinite(sse) & ieee
+    assert np.all(np.abs(gsse[fin] - sse[fin]) <= 1e-12 * sse[fin])
+
+
+# --- a sample of the single-generation workload -------------------------------------
+
+def test_single_generation_subsample_against_cpu(native, orc):
+    """4,096 programs of the single-generation workload (lengths U[16,256],
+    ~40% introns, 5 features, 4,096 cases): per-case outputs bit-exact for
+    IEEE-only effective code (checked on 256 programs), fitness on all 4,096
+    within the reference's GPU gate."""
+    wl = W.single_generation(seed=2, n_programs=4096)
+    o = orc.Oracle(orc.PROFILE_REF, 16)
+    ds = g.Dataset(wl.X, wl.y)
+    with g.Evaluator(num_registers=16, reduce=g.REDUCE_ORDERED) as ev:
+        fit = ev.evaluate_csr(wl.words, wl.offsets, ds)
+        st = ev.stats
+        sub = wl.subsample(np.arange(256))
+        outs = ev.case_outputs(sub.words, sub.offsets, ds)
+    assert st.eff_instructions < 0.65 * st.raw_instructions
+    want = o.evaluate_csr(wl.words, wl.offsets, wl.X, wl.y)
+    ieee = np.array([program_is_ieee(o, wl.words[wl.offsets[i]:wl.offsets[i + 1]], 0) for i in range(4096)])
+    assert np.array_equal(bits(fit)[ieee], bits(want)[ieee])
+    over = np.abs(fit.astype(np.float64) - want) > 1e-4
+    assert over.sum() <= 40
+    for i in range(256):
+        p = sub.words[sub.offsets[i]:sub.offsets[i + 1]]
+        ref = o.case_outputs(p, wl.X)
+        if ieee[i]:
+            assert same_or_nan(outs[i], ref).all(), i
