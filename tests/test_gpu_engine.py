@@ -11,6 +11,7 @@ whole history of most cells, to match byte for byte."""
 from __future__ import annotations
 
 import gzip
+import os
 
 import pytest
 
@@ -29,7 +30,7 @@ def _lines(p):
 @pytest.mark.skipif(not EXE.exists(), reason="oracle/_ref/lgp_run_b200 not built")
 def test_golden_cells_with_b200_backend(tmp_path, capsys):
     cells = _golden_cells()
-    run_golden(EXE, tmp_path, cells)
+    run_golden(EXE, tmp_path, cells, dict(os.environ, OMP_NUM_THREADS="1"))
     full = 0
     report = []
     for t, s in cells:
