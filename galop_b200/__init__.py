@@ -58,7 +58,7 @@ class _Options(C.Structure):
         ("profile", C.c_int32), ("num_registers", C.c_int32), ("input_protect", C.c_int32),
         ("reduce", C.c_int32), ("constants", C.POINTER(C.c_float)), ("device", C.c_int32),
         ("intron_prepass", C.c_int32), ("cases_per_lane", C.c_int32),
-        ("warps_per_block", C.c_int32), ("reserved", C.c_int32 * 4),
+        ("warps_per_block", C.c_int32), ("dispatch", C.c_int32), ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -187,7 +187,7 @@ class Evaluator:
     def __init__(self, profile: int = PROFILE_REF, num_registers: int = 8, input_protect: bool = False,
                  reduce: int = REDUCE_KAHAN32, constants: Optional[Sequence[float]] = None,
                  device: int = 0, intron_prepass: bool = True, cases_per_lane: int = 0,
-                 warps_per_block: int = 0):
+                 warps_per_block: int = 0, dispatch: Optional[int] = None):
         self._lib = load_library()
         opt = _Options()
         self._lib.galop_options_init(C.byref(opt))
@@ -199,6 +199,8 @@ class Evaluator:
         opt.intron_prepass = int(bool(intron_prepass))
         opt.cases_per_lane = cases_per_lane
         opt.warps_per_block = warps_per_block
+        if dispatch is not None:
+            opt.dispatch = dispatch
         self.constants = None
         if constants is not None:
             self.constants = np.ascontiguousarray(constants, dtype=np.float32)

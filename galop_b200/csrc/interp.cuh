@@ -151,6 +151,123 @@ __device__ __forceinline__ void step(float (&r)[NR][K], uint32_t u, const ConstP
     write_reg<NR, K>(r, uop_dest(u), t);
 }
 
+// ---- dispatch strategy 1: (op, dest)-specialized cheap binary ops ------------
+//
+// ADD, SUB, MUL (and LT, GT in the REF profile) are one FP32 instruction per
+// case, so moving their result from a temporary into r[dest] (K moves through
+// a switch) would cost as much as the op.  Instead one switch on op*16+dest
+// selects an arm that computes straight into the destination row, and a
+// constant src2 stays a single scalar.  Unary ops and DIV keep the
+// gather / compute / scatter shape: their own cost dwarfs the moves.
+
+template <int OP>
+__device__ __forceinline__ float cheap_op(float a, float b) {
+    if constexpr (OP == kAdd) return __fadd_rn(a, b);
+    else if constexpr (OP == kSub) return __fsub_rn(a, b);
+    else if constexpr (OP == kMul) return __fmul_rn(a, b);
+    else if constexpr (OP == kOp6) return (a < b) ? 1.0f : 0.0f;
+    else return (a > b) ? 1.0f : 0.0f;
+}
+
+template <int PROFILE>
+__host__ __device__ constexpr bool is_cheap(int op) {
+    return op == kAdd || op == kSub || op == kMul ||
+           (PROFILE == kProfileRef && (op == kOp6 || op == kOp7));
+}
+
+template <int K>
+__device__ __forceinline__ float operand(const float (&b)[K], int k) { return b[k]; }
+template <int K>
+__device__ __forceinline__ float operand(float b, int) { return b; }
+
+#define GALOP_OD_CASE(OPV, D)                                                  \
+    case (OPV) * 16 + (D):                                                     \
+        if constexpr ((D) < NR && is_cheap<PROFILE>(OPV)) {                    \
+            _Pragma("unroll") for (int k = 0; k < K; ++k)                      \
+                r[D][k] = cheap_op<OPV>(a[k], operand<K>(b, k));               \
+        }                                                                      \
+        break;
+#define GALOP_OD_OP(OPV)                                                       \
+    GALOP_OD_CASE(OPV, 0) GALOP_OD_CASE(OPV, 1) GALOP_OD_CASE(OPV, 2)          \
+    GALOP_OD_CASE(OPV, 3) GALOP_OD_CASE(OPV, 4) GALOP_OD_CASE(OPV, 5)          \
+    GALOP_OD_CASE(OPV, 6) GALOP_OD_CASE(OPV, 7) GALOP_OD_CASE(OPV, 8)          \
+    GALOP_OD_CASE(OPV, 9) GALOP_OD_CASE(OPV, 10) GALOP_OD_CASE(OPV, 11)        \
+    GALOP_OD_CASE(OPV, 12) GALOP_OD_CASE(OPV, 13) GALOP_OD_CASE(OPV, 14)       \
+    GALOP_OD_CASE(OPV, 15)
+
+template <int NR, int K, int PROFILE, class B>
+__device__ __forceinline__ void cheap_into_dest(float (&r)[NR][K], uint32_t op_dest,
+                                                const float (&a)[K], const B& b) {
+    switch (op_dest) {
+        GALOP_OD_OP(0) GALOP_OD_OP(1) GALOP_OD_OP(2) GALOP_OD_OP(6) GALOP_OD_OP(7)
+        default: break;
+    }
+}
+#undef GALOP_OD_OP
+#undef GALOP_OD_CASE
+
+template <int NR, int K, int PROFILE>
+__device__ __forceinline__ void step_spec(float (&r)[NR][K], uint32_t u, const ConstPool& cp) {
+    const uint32_t op = uop_op(u);
+    const uint32_t dest = uop_dest(u);
+    const bool konst = uop_is_const(u);
+    if (u & 0x40u) {                       // unary: reads src2 only
+        float b[K], t[K];
+        if (konst) {
+            const float c = cp.c[uop_src2(u)];
+#pragma unroll
+            for (int k = 0; k < K; ++k) b[k] = c;
+        } else {
+            read_reg<NR, K>(r, uop_src2(u), b);
+        }
+        switch (op) {
+            case kSin:
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[k] = sinf(b[k]);
+                break;
+            case kCos:
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[k] = cosf(b[k]);
+                break;
+            case kOp6:
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp6, 0.0f, b[k]);
+                break;
+            default:
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp7, 0.0f, b[k]);
+                break;
+        }
+        write_reg<NR, K>(r, dest, t);
+        return;
+    }
+    float a[K];
+    read_reg<NR, K>(r, uop_src1(u), a);
+    if (op == kDiv) {
+        float b[K], t[K];
+        if (konst) {
+            const float c = cp.c[uop_src2(u)];
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = (c != 0.0f) ? __fdiv_rn(a[k], c) : 1.0f;
+        } else {
+            read_reg<NR, K>(r, uop_src2(u), b);
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = (b[k] != 0.0f) ? __fdiv_rn(a[k], b[k]) : 1.0f;
+        }
+        write_reg<NR, K>(r, dest, t);
+        return;
+    }
+    const uint32_t od = op * 16u + dest;
+    if (konst) {
+        const float c = cp.c[uop_src2(u)];
+        cheap_into_dest<NR, K, PROFILE>(r, od, a, c);
+    } else {
+        float b[K];
+        read_reg<NR, K>(r, uop_src2(u), b);
+        cheap_into_dest<NR, K, PROFILE>(r, od, a, b);
+    }
+}
+
 __device__ __forceinline__ double warp_sum_f64(double v) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -164,7 +281,7 @@ __device__ __forceinline__ float fitness_from_sse(double sse, int64_t n_cases) {
     return __fdiv_rn(1.0f, __fadd_rn(1.0f, mse));
 }
 
-template <int NR, int K, int PROFILE, int REDUCE, int MODE>
+template <int NR, int K, int PROFILE, int REDUCE, int MODE, int DISPATCH>
 __global__ void __launch_bounds__(256)
 interp_kernel(InterpArgs args) {
     const int lane = threadIdx.x & 31;
@@ -216,7 +333,8 @@ interp_kernel(InterpArgs args) {
                 const int n = (L - wb < 32) ? (int)(L - wb) : 32;
                 for (int j = 0; j < n; ++j) {
                     const uint32_t u = __shfl_sync(0xffffffffu, win, j);
-                    step<NR, K, PROFILE>(r, u, args.consts);
+                    if constexpr (DISPATCH == 1) step_spec<NR, K, PROFILE>(r, u, args.consts);
+                    else step<NR, K, PROFILE>(r, u, args.consts);
                     if constexpr (MODE == kModeTrace) {
                         const int64_t row = (wb + j + 1) * NR;
 #pragma unroll

@@ -3,31 +3,37 @@
 
 namespace galop {
 
-template <int K, int P>
+template <int K, int P, int D>
 static const void* pick_mode(int reduce, int mode) {
-    if (mode == kModeOutputs) return (const void*)&interp_kernel<16, K, P, kReduceFp64, kModeOutputs>;
-    if (mode == kModeTrace) return (const void*)&interp_kernel<16, K, P, kReduceFp64, kModeTrace>;
+    if (mode == kModeOutputs) return (const void*)&interp_kernel<16, K, P, kReduceFp64, kModeOutputs, D>;
+    if (mode == kModeTrace) return (const void*)&interp_kernel<16, K, P, kReduceFp64, kModeTrace, D>;
     switch (reduce) {
-        case kReduceKahan32: return (const void*)&interp_kernel<16, K, P, kReduceKahan32, kModeFitness>;
-        case kReduceFp64: return (const void*)&interp_kernel<16, K, P, kReduceFp64, kModeFitness>;
-        case kReduceOrdered: return (const void*)&interp_kernel<16, K, P, kReduceOrdered, kModeFitness>;
+        case kReduceKahan32: return (const void*)&interp_kernel<16, K, P, kReduceKahan32, kModeFitness, D>;
+        case kReduceFp64: return (const void*)&interp_kernel<16, K, P, kReduceFp64, kModeFitness, D>;
+        case kReduceOrdered: return (const void*)&interp_kernel<16, K, P, kReduceOrdered, kModeFitness, D>;
         default: return nullptr;
     }
 }
 
-template <int K>
+template <int K, int D>
 static const void* pick_profile(int profile, int reduce, int mode) {
-    if (profile == kProfileRef) return pick_mode<K, kProfileRef>(reduce, mode);
-    if (profile == kProfileBj) return pick_mode<K, kProfileBj>(reduce, mode);
+    if (profile == kProfileRef) return pick_mode<K, kProfileRef, D>(reduce, mode);
+    if (profile == kProfileBj) return pick_mode<K, kProfileBj, D>(reduce, mode);
     return nullptr;
 }
 
-const void* interp_kernel_nr16(int k, int profile, int reduce, int mode) {
+template <int K>
+static const void* pick_dispatch(int dispatch, int profile, int reduce, int mode) {
+    if (dispatch == 1) return pick_profile<K, 1>(profile, reduce, mode);
+    return pick_profile<K, 0>(profile, reduce, mode);
+}
+
+const void* interp_kernel_nr16(int k, int dispatch, int profile, int reduce, int mode) {
     switch (k) {
-        case 1: return pick_profile<1>(profile, reduce, mode);
-        case 2: return pick_profile<2>(profile, reduce, mode);
-        case 4: return pick_profile<4>(profile, reduce, mode);
-        case 8: return pick_profile<8>(profile, reduce, mode);
+        case 1: return pick_dispatch<1>(dispatch, profile, reduce, mode);
+        case 2: return pick_dispatch<2>(dispatch, profile, reduce, mode);
+        case 4: return pick_dispatch<4>(dispatch, profile, reduce, mode);
+        case 8: return pick_dispatch<8>(dispatch, profile, reduce, mode);
         default: return nullptr;
     }
 }

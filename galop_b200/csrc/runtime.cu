@@ -21,8 +21,8 @@
 #include "prepass.cuh"
 
 namespace galop {
-const void* interp_kernel_nr8(int k, int profile, int reduce, int mode);
-const void* interp_kernel_nr16(int k, int profile, int reduce, int mode);
+const void* interp_kernel_nr8(int k, int dispatch, int profile, int reduce, int mode);
+const void* interp_kernel_nr16(int k, int dispatch, int profile, int reduce, int mode);
 }  // namespace galop
 
 using namespace galop;
@@ -86,6 +86,7 @@ struct galop_ctx {
 
     galop_stats stats{};
     int launches = 0;
+    bool stats_pending = false;   // device-path call whose timings are not read yet
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];
@@ -123,8 +124,9 @@ int pick_wpb(const galop_ctx* ctx) {
 
 const void* kernel_for(const galop_ctx* ctx, int k, int mode) {
     const int reduce = ctx->opt.reduce;
-    if (ctx->isa.num_registers == 8) return interp_kernel_nr8(k, ctx->isa.profile, reduce, mode);
-    if (ctx->isa.num_registers == 16) return interp_kernel_nr16(k, ctx->isa.profile, reduce, mode);
+    const int dispatch = ctx->opt.dispatch == 0 ? 0 : 1;
+    if (ctx->isa.num_registers == 8) return interp_kernel_nr8(k, dispatch, ctx->isa.profile, reduce, mode);
+    if (ctx->isa.num_registers == 16) return interp_kernel_nr16(k, dispatch, ctx->isa.profile, reduce, mode);
     return nullptr;
 }
 
@@ -267,14 +269,15 @@ int check_ready(galop_ctx* ctx) {
 }
 
 void begin_call(galop_ctx* ctx, int64_t n) {
+    ctx->stats_pending = false;
     ctx->stats = galop_stats{};
     ctx->stats.n_programs = n;
     ctx->stats.n_cases = ctx->N;
     ctx->launches = 0;
 }
 
-int end_call(galop_ctx* ctx) {
-    GALOP_CK(cudaStreamSynchronize(ctx->stream), "evaluate (device execution)");
+// Timings and instruction counts of the last call, once its work is done.
+int finish_stats(galop_ctx* ctx) {
     galop_stats& st = ctx->stats;
     st.h2d_ms = ev_ms(ctx->ev[kEvStart], ctx->ev[kEvH2D]);
     st.prepass_ms = ev_ms(ctx->ev[kEvH2D], ctx->ev[kEvPrepass]);
@@ -288,7 +291,13 @@ int end_call(galop_ctx* ctx) {
     st.raw_instructions = (int64_t)tot[0];
     st.eff_instructions = (int64_t)tot[1];
     st.kernels_launched = ctx->launches;
+    ctx->stats_pending = false;
     return GALOP_OK;
+}
+
+int end_call(galop_ctx* ctx) {
+    GALOP_CK(cudaStreamSynchronize(ctx->stream), "evaluate (device execution)");
+    return finish_stats(ctx);
 }
 
 int validate_offsets(galop_ctx* ctx, const int64_t* off, int64_t n) {
@@ -350,6 +359,7 @@ int galop_options_init(galop_options* opt) {
     opt->intron_prepass = 1;
     opt->cases_per_lane = 0;
     opt->warps_per_block = 0;
+    opt->dispatch = 1;
     return GALOP_OK;
 }
 
@@ -416,8 +426,13 @@ const char* galop_last_error(const galop_ctx* ctx) {
     return ctx->err.c_str();
 }
 
-int galop_last_stats(const galop_ctx* ctx, galop_stats* out) {
+int galop_last_stats(galop_ctx* ctx, galop_stats* out) {
     if (!ctx || !out) return GALOP_E_INVALID;
+    if (ctx->stats_pending) {
+        GALOP_CK(cudaSetDevice(ctx->device), "set device");
+        GALOP_CK(cudaEventSynchronize(ctx->ev[kEvD2H]), "wait for last call");
+        if (int rc = finish_stats(ctx)) return rc;
+    }
     *out = ctx->stats;
     return GALOP_OK;
 }
@@ -643,6 +658,7 @@ int galop_evaluate_csr_device(galop_ctx* ctx, const uint32_t* d_words, const int
     GALOP_CK(cudaEventRecord(ctx->ev[kEvD2H], s), "event");
     if (user && user != s) GALOP_CK(cudaStreamWaitEvent(user, ctx->ev[kEvD2H], 0), "stream wait");
     ctx->stats.kernels_launched = ctx->launches;
+    ctx->stats_pending = true;
     return GALOP_OK;
 }
 

@@ -79,8 +79,11 @@ typedef struct {
     int32_t intron_prepass;   /* 1: interpret only effective instructions
                                  (src/Introns.h:28-57); outputs unchanged       */
     int32_t cases_per_lane;   /* 0 = tuned default; else 1, 2, 4 or 8          */
-    int32_t warps_per_block;  /* 0 = tuned default; else 1..32                 */
-    int32_t reserved[4];
+    int32_t warps_per_block;  /* 0 = tuned default; else 1..8                  */
+    int32_t dispatch;         /* interpreter dispatch: 0 = gather/compute/
+                                 scatter for every op, 1 = cheap binary ops
+                                 specialized on (op, dest) (default)          */
+    int32_t reserved[3];
 } galop_options;
 
 typedef struct galop_ctx galop_ctx;
@@ -173,7 +176,9 @@ GALOP_API int galop_trace_program(galop_ctx* ctx, const uint32_t* words, int64_t
 GALOP_API int galop_effective_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets,
                         int64_t n_programs, int64_t* eff_len, uint32_t* eff_words);
 
-GALOP_API int galop_last_stats(const galop_ctx* ctx, galop_stats* out);
+/* Stats of the most recent evaluate call; after galop_evaluate_csr_device
+ * this waits for that call's work to finish. */
+GALOP_API int galop_last_stats(galop_ctx* ctx, galop_stats* out);
 
 /* Blocks until the context's stream is idle. */
 GALOP_API int galop_synchronize(galop_ctx* ctx);

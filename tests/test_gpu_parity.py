@@ -109,7 +109,7 @@ def test_golden_vectors_outputs_and_fitness(native, orc, variant, k):
     words, off = v["words"], v["offsets"]
     n = len(off) - 1
     ieee = np.array([program_is_ieee(o, words[off[i]:off[i + 1]], g.PROFILE_REF) for i in range(n)])
-    assert ieee.sum() > 100
+    assert ieee.sum() > 50
     with g.Evaluator(num_registers=nr, input_protect=ip, reduce=g.REDUCE_ORDERED, cases_per_lane=k) as ev, \
             g.Evaluator(num_registers=nr, input_protect=ip, reduce=g.REDUCE_KAHAN32, cases_per_lane=k) as ek:
         for d in ("d1", "d2", "d3", "d4"):
@@ -206,22 +206,23 @@ def test_gpu_intron_pass_matches_reference_masks(native, variant):
 
 
 def test_prepass_on_off_and_tile_shapes_bitwise(native):
-    """Intron removal and every cases-per-lane / warps-per-block choice give
-    bit-identical per-case outputs and fitness."""
+    """Intron removal and every cases-per-lane / warps-per-block / dispatch
+    choice give bit-identical per-case outputs and fitness."""
     wl = W.single_generation(seed=9, n_programs=600, n_cases=777)
     ds = g.Dataset(wl.X, wl.y)
     base = None
     for pre in (True, False):
         for k in (1, 2, 4, 8):
             for wpb in (1, 4, 8):
-                with g.Evaluator(num_registers=16, intron_prepass=pre, cases_per_lane=k, warps_per_block=wpb,
-                                 reduce=g.REDUCE_ORDERED) as ev:
-                    outs = ev.case_outputs(wl.words, wl.offsets, ds)
-                    fit = ev.evaluate_csr(wl.words, wl.offsets, ds)
-                if base is None:
-                    base = (outs, fit)
-                assert np.array_equal(bits(outs), bits(base[0])), (pre, k, wpb)
-                assert np.array_equal(bits(fit), bits(base[1])), (pre, k, wpb)
+                for disp in (0, 1):
+                    with g.Evaluator(num_registers=16, intron_prepass=pre, cases_per_lane=k, warps_per_block=wpb,
+                                     reduce=g.REDUCE_ORDERED, dispatch=disp) as ev:
+                        outs = ev.case_outputs(wl.words, wl.offsets, ds)
+                        fit = ev.evaluate_csr(wl.words, wl.offsets, ds)
+                    if base is None:
+                        base = (outs, fit)
+                    assert np.array_equal(bits(outs), bits(base[0])), (pre, k, wpb, disp)
+                    assert np.array_equal(bits(fit), bits(base[1])), (pre, k, wpb, disp)
 
 
 # --- reductions ------------------------------------------------------------------------
