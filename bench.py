@@ -319,6 +319,22 @@ def run_b200(args, dist: Dist):
     interp_avg_ms = float(np.mean(interp_ms))
     achieved = eff_instr * wl.n_cases / (interp_avg_ms / 1e3) / 1e9
 
+    # ---- the reference's own GPU kernel on the same B200 (a sample) ------------
+    ref_gpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle.oracle import Oracle, RefCuda
+            m = min(n, 32768)
+            sub = wl.subsample(np.arange(m))
+            _, kms = RefCuda().evaluate_packed(sub.words, sub.offsets, wl.X, wl.y, reps=2)
+            eff = float(Oracle(0, 16).effective_lengths(sub.words, sub.offsets).sum())
+            ref_gpu = {"value": eff * wl.n_cases / (kms / 1e3) / 1e9, "unit": UNIT,
+                       "raw_gpops": float(sub.offsets[-1]) * wl.n_cases / (kms / 1e3) / 1e9,
+                       "kernel_ms": kms, "sample": f"first {m} programs x {wl.n_cases} cases",
+                       "kernel": "evaluate_kernel_packed from the reference's src/EvaluatorCuda.cu, sm_100a"}
+        except (FileNotFoundError, OSError, RuntimeError) as e:
+            ref_gpu = {"unavailable": str(e)}
+
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -352,6 +368,8 @@ def run_b200(args, dist: Dist):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if ref_gpu:
+            line["reference_gpu_same_b200"] = ref_gpu
         print(json.dumps(line), flush=True)
     for d in (d_words, d_off, d_fit, d_sse):
         ev.device_free(d)

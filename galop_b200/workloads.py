@@ -115,15 +115,16 @@ def _select_tables(bits_: int):
 
 
 def structured_population(rng, lengths, isa: IsaSpec, eff_frac: float, reg_limit: Optional[int] = None,
-                          const_limit: Optional[int] = None):
+                          const_limit: Optional[int] = None, ops=None):
     """Random programs whose effective fraction is ``eff_frac`` by
     construction.  Walking each program backwards with the liveness rule of
     src/Introns.h:28-46, an instruction drawn effective takes its destination
     from the live set, an intron from outside it; opcodes, sources and the
     constant flag are uniform (an effective unary op that would leave nothing
     live reads a register instead of a constant).  The last instruction is
-    always effective.  Vectorised over programs: programs are sorted by
-    length, so at backward step t the programs still running are a prefix."""
+    always effective.  ``ops`` restricts the opcodes drawn (default: all 8).
+    Vectorised over programs: programs are sorted by length, so at backward
+    step t the programs still running are a prefix."""
     assert not isa.input_protect, "structured programs assume the default dest decode"
     lengths = np.asarray(lengths, dtype=np.int64)
     nr = isa.num_registers
@@ -139,12 +140,13 @@ def structured_population(rng, lengths, isa: IsaSpec, eff_frac: float, reg_limit
     live = np.full(order.shape[0], np.uint32(1 << isa.output_reg), dtype=np.uint32)
     neg = -Ls
     Lmax = int(Ls[0]) if Ls.size else 0
+    op_set = np.arange(8, dtype=np.uint32) if ops is None else np.asarray(ops, dtype=np.uint32)
     for t in range(Lmax):
         a = int(np.searchsorted(neg, -t, side="left"))     # programs with L > t
         if a == 0:
             break
         lv = live[:a]
-        op = rng.integers(0, 8, size=a, dtype=np.uint32)
+        op = op_set[rng.integers(0, op_set.size, size=a)]
         s1 = rng.integers(0, rl, size=a, dtype=np.uint32)
         kc = rng.random(a) < 0.5
         s2r = rng.integers(0, rl, size=a, dtype=np.uint32)

@@ -266,3 +266,34 @@ class RefLib:
         m = C.create_string_buffer(max(prog.shape[0], 1))
         self.lib.ref_effective_mask(_p(prog, _U32), prog.shape[0], m)
         return np.frombuffer(m.raw[: prog.shape[0]], dtype=np.uint8).astype(bool)
+
+
+class RefCuda:
+    """The reference's own GPU kernel (evaluate_kernel_packed from its
+    src/EvaluatorCuda.cu, built for sm_100a, 16-register configuration)."""
+
+    def __init__(self):
+        path = REF_DIR / "libref_cuda_nr16.so"
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built")
+        lib = C.CDLL(str(path))
+        lib.refcuda_evaluate_packed.restype = C.c_int
+        lib.refcuda_evaluate_packed.argtypes = [C.POINTER(_U32), C.POINTER(_I64), C.c_int, C.POINTER(_F32),
+                                                C.POINTER(_F32), C.c_int, C.c_int, C.c_int, C.POINTER(_F32),
+                                                C.POINTER(C.c_float)]
+        self.lib = lib
+
+    def evaluate_packed(self, words, offsets, inputs, targets, reps: int = 3):
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        inputs = np.ascontiguousarray(inputs, dtype=np.float32)
+        targets = np.ascontiguousarray(targets, dtype=np.float32)
+        n = offsets.shape[0] - 1
+        fit = np.empty(n, dtype=np.float32)
+        ms = C.c_float()
+        rc = self.lib.refcuda_evaluate_packed(_p(words, _U32), _p(offsets, _I64), n, _p(inputs, _F32),
+                                              _p(targets, _F32), inputs.shape[0], inputs.shape[1], reps,
+                                              _p(fit, _F32), C.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"reference kernel failed: cudaError {rc}")
+        return fit, ms.value
