@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "isa.cuh"
+#include "dispatch_gen.cuh"
 
 namespace galop {
 
@@ -151,74 +152,31 @@ __device__ __forceinline__ void step(float (&r)[NR][K], uint32_t u, const ConstP
     write_reg<NR, K>(r, uop_dest(u), t);
 }
 
-// ---- dispatch strategy 1: (op, dest)-specialized cheap binary ops ------------
+// ---- dispatch strategy 1: jump tables (default) --------------------------------
 //
-// ADD, SUB, MUL (and LT, GT in the REF profile) are one FP32 instruction per
-// case, so moving their result from a temporary into r[dest] (K moves through
-// a switch) would cost as much as the op.  Instead one switch on op*16+dest
-// selects an arm that computes straight into the destination row, and a
-// constant src2 stays a single scalar.  Unary ops and DIV keep the
-// gather / compute / scatter shape: their own cost dwarfs the moves.
-
-template <int OP>
-__device__ __forceinline__ float cheap_op(float a, float b) {
-    if constexpr (OP == kAdd) return __fadd_rn(a, b);
-    else if constexpr (OP == kSub) return __fsub_rn(a, b);
-    else if constexpr (OP == kMul) return __fmul_rn(a, b);
-    else if constexpr (OP == kOp6) return (a < b) ? 1.0f : 0.0f;
-    else return (a > b) ? 1.0f : 0.0f;
-}
-
-template <int PROFILE>
-__host__ __device__ constexpr bool is_cheap(int op) {
-    return op == kAdd || op == kSub || op == kMul ||
-           (PROFILE == kProfileRef && (op == kOp6 || op == kOp7));
-}
-
-template <int K>
-__device__ __forceinline__ float operand(const float (&b)[K], int k) { return b[k]; }
-template <int K>
-__device__ __forceinline__ float operand(float b, int) { return b; }
-
-#define GALOP_OD_CASE(OPV, D)                                                  \
-    case (OPV) * 16 + (D):                                                     \
-        if constexpr ((D) < NR && is_cheap<PROFILE>(OPV)) {                    \
-            _Pragma("unroll") for (int k = 0; k < K; ++k)                      \
-                r[D][k] = cheap_op<OPV>(a[k], operand<K>(b, k));               \
-        }                                                                      \
-        break;
-#define GALOP_OD_OP(OPV)                                                       \
-    GALOP_OD_CASE(OPV, 0) GALOP_OD_CASE(OPV, 1) GALOP_OD_CASE(OPV, 2)          \
-    GALOP_OD_CASE(OPV, 3) GALOP_OD_CASE(OPV, 4) GALOP_OD_CASE(OPV, 5)          \
-    GALOP_OD_CASE(OPV, 6) GALOP_OD_CASE(OPV, 7) GALOP_OD_CASE(OPV, 8)          \
-    GALOP_OD_CASE(OPV, 9) GALOP_OD_CASE(OPV, 10) GALOP_OD_CASE(OPV, 11)        \
-    GALOP_OD_CASE(OPV, 12) GALOP_OD_CASE(OPV, 13) GALOP_OD_CASE(OPV, 14)       \
-    GALOP_OD_CASE(OPV, 15)
-
-template <int NR, int K, int PROFILE, class B>
-__device__ __forceinline__ void cheap_into_dest(float (&r)[NR][K], uint32_t op_dest,
-                                                const float (&a)[K], const B& b) {
-    switch (op_dest) {
-        GALOP_OD_OP(0) GALOP_OD_OP(1) GALOP_OD_OP(2) GALOP_OD_OP(6) GALOP_OD_OP(7)
-        default: break;
-    }
-}
-#undef GALOP_OD_OP
-#undef GALOP_OD_CASE
-
+// The C++ switches above are compiled into predicated select chains: every
+// register read or write costs NR*K instructions.  Strategy 1 uses the PTX
+// brx.idx helpers of dispatch_gen.cuh instead: one indirect branch per
+// access, then K moves.  Single-instruction binary ops (ADD, SUB, MUL, and
+// LT, GT in the REF profile) are fused with their destination: one branch on
+// op*NR+dest lands on K arithmetic instructions that write r[dest] directly,
+// with a constant src2 kept as one scalar.  DIV and the unary ops gather,
+// compute in C++ and scatter: their own cost dwarfs the moves.
 template <int NR, int K, int PROFILE>
-__device__ __forceinline__ void step_spec(float (&r)[NR][K], uint32_t u, const ConstPool& cp) {
+__device__ __forceinline__ void step_brx(float (&r)[NR][K], uint32_t u, const ConstPool& cp) {
+    using B = Brx<NR, K, PROFILE>;
     const uint32_t op = uop_op(u);
     const uint32_t dest = uop_dest(u);
     const bool konst = uop_is_const(u);
+    const uint32_t s2 = uop_src2(u);
     if (u & 0x40u) {                       // unary: reads src2 only
         float b[K], t[K];
         if (konst) {
-            const float c = cp.c[uop_src2(u)];
+            const float c = cp.c[s2];
 #pragma unroll
             for (int k = 0; k < K; ++k) b[k] = c;
         } else {
-            read_reg<NR, K>(r, uop_src2(u), b);
+            B::gather(r, s2, b);
         }
         switch (op) {
             case kSin:
@@ -238,33 +196,33 @@ __device__ __forceinline__ void step_spec(float (&r)[NR][K], uint32_t u, const C
                 for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp7, 0.0f, b[k]);
                 break;
         }
-        write_reg<NR, K>(r, dest, t);
+        B::scatter(r, dest, t);
         return;
     }
     float a[K];
-    read_reg<NR, K>(r, uop_src1(u), a);
+    B::gather(r, uop_src1(u), a);
     if (op == kDiv) {
-        float b[K], t[K];
+        float t[K];
         if (konst) {
-            const float c = cp.c[uop_src2(u)];
+            const float c = cp.c[s2];
 #pragma unroll
             for (int k = 0; k < K; ++k) t[k] = (c != 0.0f) ? __fdiv_rn(a[k], c) : 1.0f;
         } else {
-            read_reg<NR, K>(r, uop_src2(u), b);
+            float b[K];
+            B::gather(r, s2, b);
 #pragma unroll
             for (int k = 0; k < K; ++k) t[k] = (b[k] != 0.0f) ? __fdiv_rn(a[k], b[k]) : 1.0f;
         }
-        write_reg<NR, K>(r, dest, t);
+        B::scatter(r, dest, t);
         return;
     }
-    const uint32_t od = op * 16u + dest;
+    const uint32_t od = op * NR + dest;
     if (konst) {
-        const float c = cp.c[uop_src2(u)];
-        cheap_into_dest<NR, K, PROFILE>(r, od, a, c);
+        B::od_sca(r, od, a, cp.c[s2]);
     } else {
         float b[K];
-        read_reg<NR, K>(r, uop_src2(u), b);
-        cheap_into_dest<NR, K, PROFILE>(r, od, a, b);
+        B::gather(r, s2, b);
+        B::od_vec(r, od, a, b);
     }
 }
 
@@ -333,7 +291,7 @@ interp_kernel(InterpArgs args) {
                 const int n = (L - wb < 32) ? (int)(L - wb) : 32;
                 for (int j = 0; j < n; ++j) {
                     const uint32_t u = __shfl_sync(0xffffffffu, win, j);
-                    if constexpr (DISPATCH == 1) step_spec<NR, K, PROFILE>(r, u, args.consts);
+                    if constexpr (DISPATCH == 1) step_brx<NR, K, PROFILE>(r, u, args.consts);
                     else step<NR, K, PROFILE>(r, u, args.consts);
                     if constexpr (MODE == kModeTrace) {
                         const int64_t row = (wb + j + 1) * NR;
@@ -347,7 +305,8 @@ interp_kernel(InterpArgs args) {
             }
 
             float o[K];
-            read_reg<NR, K>(r, (uint32_t)args.output_reg, o);
+            if constexpr (DISPATCH == 1) Brx<NR, K, PROFILE>::gather(r, (uint32_t)args.output_reg, o);
+            else read_reg<NR, K>(r, (uint32_t)args.output_reg, o);
 
             if constexpr (MODE == kModeOutputs) {
 #pragma unroll
