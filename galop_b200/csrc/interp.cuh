@@ -226,6 +226,58 @@ __device__ __forceinline__ void step_brx(float (&r)[NR][K], uint32_t u, const Co
     }
 }
 
+// ---- dispatch strategy 2: jump tables, one copy of each table ------------------
+//
+// Same jump tables as strategy 1, but every helper is expanded once per
+// instruction step instead of once per op class: src2 is gathered (or the
+// constant broadcast) by one table, src1 by one, then either the fused
+// op/dest table or the C++ DIV / unary arm followed by one scatter table.
+// Less code in the instruction cache at the price of K moves for constants.
+template <int NR, int K, int PROFILE>
+__device__ __forceinline__ void step_brx_compact(float (&r)[NR][K], uint32_t u, const ConstPool& cp) {
+    using B = Brx<NR, K, PROFILE>;
+    const uint32_t op = uop_op(u);
+    float b[K];
+    if (uop_is_const(u)) {
+        const float c = cp.c[uop_src2(u)];
+#pragma unroll
+        for (int k = 0; k < K; ++k) b[k] = c;
+    } else {
+        B::gather(r, uop_src2(u), b);
+    }
+    float a[K];
+    const bool unary = (u & 0x40u) != 0;
+    if (!unary) B::gather(r, uop_src1(u), a);
+    if (!unary && op != kDiv) {
+        B::od_vec(r, op * NR + uop_dest(u), a, b);
+        return;
+    }
+    float t[K];
+    switch (op) {
+        case kDiv:
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = (b[k] != 0.0f) ? __fdiv_rn(a[k], b[k]) : 1.0f;
+            break;
+        case kSin:
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = sinf(b[k]);
+            break;
+        case kCos:
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = cosf(b[k]);
+            break;
+        case kOp6:
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp6, 0.0f, b[k]);
+            break;
+        default:
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp7, 0.0f, b[k]);
+            break;
+    }
+    B::scatter(r, uop_dest(u), t);
+}
+
 __device__ __forceinline__ double warp_sum_f64(double v) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -240,7 +292,7 @@ __device__ __forceinline__ float fitness_from_sse(double sse, int64_t n_cases) {
 }
 
 template <int NR, int K, int PROFILE, int REDUCE, int MODE, int DISPATCH>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 1)
 interp_kernel(InterpArgs args) {
     const int lane = threadIdx.x & 31;
     const int64_t total_items = args.n_programs * (int64_t)args.n_chunks;
@@ -291,7 +343,8 @@ interp_kernel(InterpArgs args) {
                 const int n = (L - wb < 32) ? (int)(L - wb) : 32;
                 for (int j = 0; j < n; ++j) {
                     const uint32_t u = __shfl_sync(0xffffffffu, win, j);
-                    if constexpr (DISPATCH == 1) step_brx<NR, K, PROFILE>(r, u, args.consts);
+                    if constexpr (DISPATCH == 2) step_brx_compact<NR, K, PROFILE>(r, u, args.consts);
+                    else if constexpr (DISPATCH == 1) step_brx<NR, K, PROFILE>(r, u, args.consts);
                     else step<NR, K, PROFILE>(r, u, args.consts);
                     if constexpr (MODE == kModeTrace) {
                         const int64_t row = (wb + j + 1) * NR;
@@ -305,7 +358,7 @@ interp_kernel(InterpArgs args) {
             }
 
             float o[K];
-            if constexpr (DISPATCH == 1) Brx<NR, K, PROFILE>::gather(r, (uint32_t)args.output_reg, o);
+            if constexpr (DISPATCH >= 1) Brx<NR, K, PROFILE>::gather(r, (uint32_t)args.output_reg, o);
             else read_reg<NR, K>(r, (uint32_t)args.output_reg, o);
 
             if constexpr (MODE == kModeOutputs) {

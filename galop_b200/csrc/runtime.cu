@@ -124,7 +124,7 @@ int pick_wpb(const galop_ctx* ctx) {
 
 const void* kernel_for(const galop_ctx* ctx, int k, int mode) {
     const int reduce = ctx->opt.reduce;
-    const int dispatch = ctx->opt.dispatch == 0 ? 0 : 1;
+    const int dispatch = (ctx->opt.dispatch >= 0 && ctx->opt.dispatch <= 2) ? ctx->opt.dispatch : 1;
     if (ctx->isa.num_registers == 8) return interp_kernel_nr8(k, dispatch, ctx->isa.profile, reduce, mode);
     if (ctx->isa.num_registers == 16) return interp_kernel_nr16(k, dispatch, ctx->isa.profile, reduce, mode);
     return nullptr;
