@@ -278,6 +278,49 @@ __device__ __forceinline__ void step_brx_compact(float (&r)[NR][K], uint32_t u, 
     B::scatter(r, uop_dest(u), t);
 }
 
+// ---- dispatch strategy 3: one direct-threaded PTX block per instruction ------
+//
+// Brx<>::fused runs src1 table -> src2 table -> op/dest table, each arm
+// jumping straight into the next table (3 indirect branches and one exit
+// jump per instruction); the micro-op carries the three table indices
+// (encode_uop_threaded).  DIV and unary ops leave the block with their
+// operands and finish here, in a single copy of the C++ code.
+template <int NR, int K, int PROFILE>
+__device__ __forceinline__ void step_threaded(float (&r)[NR][K], uint32_t u, const ConstPool& cp) {
+    using B = Brx<NR, K, PROFILE>;
+    float oa[K], ob[K];
+    const float c = cp.c[(u >> 17) & 15u];
+    B::fused(r, u & 31u, (u >> 5) & 31u, (u >> 10) & 127u, c, oa, ob);
+    if (u & (1u << 21)) {
+        const uint32_t io = (u >> 10) & 127u;
+        const uint32_t op = io >> 4;
+        float t[K];
+        switch (op) {
+            case kDiv:
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[k] = (ob[k] != 0.0f) ? __fdiv_rn(oa[k], ob[k]) : 1.0f;
+                break;
+            case kSin:
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[k] = sinf(ob[k]);
+                break;
+            case kCos:
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[k] = cosf(ob[k]);
+                break;
+            case kOp6:
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp6, 0.0f, ob[k]);
+                break;
+            default:
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp7, 0.0f, ob[k]);
+                break;
+        }
+        B::scatter(r, io & 15u, t);
+    }
+}
+
 __device__ __forceinline__ double warp_sum_f64(double v) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -343,7 +386,8 @@ interp_kernel(InterpArgs args) {
                 const int n = (L - wb < 32) ? (int)(L - wb) : 32;
                 for (int j = 0; j < n; ++j) {
                     const uint32_t u = __shfl_sync(0xffffffffu, win, j);
-                    if constexpr (DISPATCH == 2) step_brx_compact<NR, K, PROFILE>(r, u, args.consts);
+                    if constexpr (DISPATCH == 3) step_threaded<NR, K, PROFILE>(r, u, args.consts);
+                    else if constexpr (DISPATCH == 2) step_brx_compact<NR, K, PROFILE>(r, u, args.consts);
                     else if constexpr (DISPATCH == 1) step_brx<NR, K, PROFILE>(r, u, args.consts);
                     else step<NR, K, PROFILE>(r, u, args.consts);
                     if constexpr (MODE == kModeTrace) {

@@ -24,6 +24,7 @@ static const void* pick_profile(int profile, int reduce, int mode) {
 
 template <int K>
 static const void* pick_dispatch(int dispatch, int profile, int reduce, int mode) {
+    if (dispatch == 3) return pick_profile<K, 3>(profile, reduce, mode);
     if (dispatch == 2) return pick_profile<K, 2>(profile, reduce, mode);
     if (dispatch == 1) return pick_profile<K, 1>(profile, reduce, mode);
     return pick_profile<K, 0>(profile, reduce, mode);

@@ -124,7 +124,7 @@ int pick_wpb(const galop_ctx* ctx) {
 
 const void* kernel_for(const galop_ctx* ctx, int k, int mode) {
     const int reduce = ctx->opt.reduce;
-    const int dispatch = (ctx->opt.dispatch >= 0 && ctx->opt.dispatch <= 2) ? ctx->opt.dispatch : 1;
+    const int dispatch = (ctx->opt.dispatch >= 0 && ctx->opt.dispatch <= 3) ? ctx->opt.dispatch : 1;
     if (ctx->isa.num_registers == 8) return interp_kernel_nr8(k, dispatch, ctx->isa.profile, reduce, mode);
     if (ctx->isa.num_registers == 16) return interp_kernel_nr16(k, dispatch, ctx->isa.profile, reduce, mode);
     return nullptr;
@@ -165,7 +165,8 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
     // Device buffer for micro-ops sized by the raw total (an upper bound).
     GALOP_CK(ctx->uops.ensure((size_t)std::max<int64_t>(raw_words_total, 1)), "alloc uops");
     if (n > 0) {
-        prepass_compact_kernel<Src><<<blocks, tpb, 0, s>>>(src, n, ctx->isa, strip ? 1 : 0,
+        const int format = ctx->opt.dispatch == 3 ? kUopFormatThreaded : kUopFormatBytes;
+        prepass_compact_kernel<Src><<<blocks, tpb, 0, s>>>(src, n, ctx->isa, strip ? 1 : 0, format,
                                                            ctx->eff_off.p, ctx->uops.p, raw_out);
         ctx->launches += 1;
     }
