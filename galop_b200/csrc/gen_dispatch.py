@@ -9,6 +9,8 @@ costing NR*K instructions per access.  These helpers instead emit PTX
 moves (or K arithmetic instructions) in the selected arm.
 
 Emitted for NR in {8, 16} and K in {1, 2, 4, 8}:
+  cheap    t[k] = OP(a[k], b[k]) on the opcode alone (register file in
+           shared memory, operands already loaded)
   fused    one whole instruction, direct-threaded through three tables
            (see fused() below)
   gather   out[k] = r[idx][k]
@@ -159,6 +161,23 @@ def fused(nr: int, k: int, profile: int) -> str:
             + asm_block(L, outs, ins) + "    }\n")
 
 
+def cheap_table(k: int, profile: int) -> str:
+    """t[q] = OP(a[q], b[q]) for the single-instruction ops, one table on
+    the opcode (8 entries, other opcodes jump to the end)."""
+    ops = PROFILES[profile]
+    # outputs t %0..k-1 ; inputs op %k, a %(k+1+q), b %(2k+1+q)
+    L = ["T%=: .branchtargets " + ", ".join(f"C{op}_%=" if op in ops else "E%=" for op in range(8)) + ";",
+         f"brx.idx %{k}, T%=;"]
+    for op in ops:
+        body = " ".join(f"{CHEAP[op]} %{q}, %{k + 1 + q}, %{2 * k + 1 + q};" for q in range(k))
+        L.append(f"C{op}_%=: {body} bra.uni E%=;")
+    L.append("E%=:")
+    outs = [f'"=f"(t[{q}])' for q in range(k)]
+    ins = ['"r"(op)'] + [f'"f"(a[{q}])' for q in range(k)] + [f'"f"(b[{q}])' for q in range(k)]
+    return (f"    static __device__ __forceinline__ void cheap(uint32_t op, const float (&a)[{k}], "
+            f"const float (&b)[{k}], float (&t)[{k}]) {{\n" + asm_block(L, outs, ins) + "    }\n")
+
+
 def main() -> None:
     out = ["// dispatch_gen.cuh -- GENERATED by gen_dispatch.py; do not edit by hand.",
            "// Jump-table (PTX brx.idx) register access for the LGP interpreter; see",
@@ -175,6 +194,12 @@ def main() -> None:
                 out.append(od(nr, k, prof, True))
                 out.append(fused(nr, k, prof))
                 out.append("};\n")
+    out.append("template <int K, int PROFILE>\nstruct CheapOps;\n")
+    for k in KS:
+        for prof in PROFILES:
+            out.append(f"template <>\nstruct CheapOps<{k}, {prof}> {{")
+            out.append(cheap_table(k, prof))
+            out.append("};\n")
     out.append("}  // namespace galop\n")
     path = Path(__file__).resolve().parent / "dispatch_gen.cuh"
     path.write_text("\n".join(out))

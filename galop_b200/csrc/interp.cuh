@@ -470,4 +470,250 @@ interp_kernel(InterpArgs args) {
     }
 }
 
+
+// ---- dispatch strategy 4: the LGP register file in shared memory --------------
+//
+// Each lane keeps its K cases' NR registers in its own shared-memory slots:
+// register j of the warp is a block of 32*K floats, lane l owns the K
+// consecutive floats at l*V of every V-wide chunk (V = min(K, 4)), so a
+// register read or write is one conflict-free 64/128-bit LDS/STS per chunk
+// and the register index is just an address offset -- no branches, no
+// select chains.  The opcode is the only dispatch: one jump table
+// (CheapOps, 8 entries) for the single-instruction ops, a C++ switch for
+// DIV and the unary ops.  No lane reads another lane's slots, so no
+// barrier is needed.
+template <int K>
+struct SmemRegs {
+    static constexpr int V = K < 4 ? K : 4;     // floats per vector access
+    static constexpr int kStride = 32 * K;       // floats per register per warp
+    static __device__ __forceinline__ void load(const float* p, float (&v)[K]) {
+#pragma unroll
+        for (int q = 0; q < K / V; ++q) {
+            if constexpr (V == 4) {
+                const float4 x = *reinterpret_cast<const float4*>(p + q * 32 * V);
+                v[q * 4] = x.x; v[q * 4 + 1] = x.y; v[q * 4 + 2] = x.z; v[q * 4 + 3] = x.w;
+            } else if constexpr (V == 2) {
+                const float2 x = *reinterpret_cast<const float2*>(p + q * 32 * V);
+                v[q * 2] = x.x; v[q * 2 + 1] = x.y;
+            } else {
+                v[q] = p[q * 32];
+            }
+        }
+    }
+    static __device__ __forceinline__ void store(float* p, const float (&v)[K]) {
+#pragma unroll
+        for (int q = 0; q < K / V; ++q) {
+            if constexpr (V == 4) {
+                *reinterpret_cast<float4*>(p + q * 32 * V) = make_float4(v[q * 4], v[q * 4 + 1], v[q * 4 + 2],
+                                                                         v[q * 4 + 3]);
+            } else if constexpr (V == 2) {
+                *reinterpret_cast<float2*>(p + q * 32 * V) = make_float2(v[q * 2], v[q * 2 + 1]);
+            } else {
+                p[q * 32] = v[q];
+            }
+        }
+    }
+};
+
+template <int K, int PROFILE>
+__device__ __forceinline__ void slow_op(uint32_t op, const float (&a)[K], const float (&b)[K], float (&t)[K]) {
+    switch (op) {
+        case kDiv:
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = (b[k] != 0.0f) ? __fdiv_rn(a[k], b[k]) : 1.0f;
+            break;
+        case kSin:
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = sinf(b[k]);
+            break;
+        case kCos:
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = cosf(b[k]);
+            break;
+        case kOp6:
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp6, a[k], b[k]);
+            break;
+        default:
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp7, a[k], b[k]);
+            break;
+    }
+}
+
+template <int NR, int K, int PROFILE, int REDUCE, int MODE>
+__global__ void __launch_bounds__(256, 1)
+interp_smem_kernel(InterpArgs args) {
+    extern __shared__ float4 galop_smem4[];
+    using SR = SmemRegs<K>;
+    constexpr int V = SR::V;
+    constexpr int RS = SR::kStride;
+    const int lane = threadIdx.x & 31;
+    float* regs = reinterpret_cast<float*>(galop_smem4) + (threadIdx.x >> 5) * NR * RS + lane * V;
+    const int64_t total_items = args.n_programs * (int64_t)args.n_chunks;
+    constexpr int kPass = 32 * K;
+
+    for (;;) {
+        unsigned long long item = 0;
+        if (lane == 0) item = atomicAdd(args.counter, 1ull);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if ((int64_t)item >= total_items) break;
+
+        const int64_t slot = (int64_t)item / args.n_chunks;
+        const int chunk = (int)((int64_t)item % args.n_chunks);
+        const int64_t prog = args.order ? (int64_t)args.order[slot] : slot;
+        const int64_t p0 = args.eff_off[prog];
+        const int64_t L = args.eff_off[prog + 1] - p0;
+        const uint32_t* __restrict__ pw = args.uops + p0;
+        const int64_t cbeg = (int64_t)chunk * args.chunk_cases;
+        int64_t cend = cbeg + args.chunk_cases;
+        if (cend > args.N) cend = args.N;
+
+        float ks = 0.0f, kc = 0.0f;
+        double acc = 0.0;
+
+        for (int64_t base = cbeg; base < cend; base += kPass) {
+            // Case c of this lane: base + (q*32 + lane)*V + e for chunk q,
+            // element e -- the same layout as the registers, so the inputs
+            // are copied with the same vector width.
+            const int64_t c0 = base + (int64_t)lane * V;
+#pragma unroll
+            for (int f = 0; f < NR; ++f) {
+                float v[K];
+                if (f < args.num_inputs) {
+#pragma unroll
+                    for (int q = 0; q < K / V; ++q) {
+                        float w[V];
+                        load_cases<V>(args.X + (int64_t)f * args.Np + c0 + q * 32 * V, w);
+#pragma unroll
+                        for (int e = 0; e < V; ++e) v[q * V + e] = w[e];
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < K; ++k) v[k] = 0.0f;
+                }
+                SR::store(regs + f * RS, v);
+                if constexpr (MODE == kModeTrace) {
+#pragma unroll
+                    for (int q = 0; q < K / V; ++q)
+#pragma unroll
+                        for (int e = 0; e < V; ++e)
+                            args.trace[(int64_t)f * kPass + (q * 32 + lane) * V + e] = v[q * V + e];
+                }
+            }
+
+            for (int64_t wb = 0; wb < L; wb += 32) {
+                const uint32_t win = (wb + lane < L) ? __ldg(pw + wb + lane) : 0u;
+                const int n = (L - wb < 32) ? (int)(L - wb) : 32;
+                for (int j = 0; j < n; ++j) {
+                    const uint32_t u = __shfl_sync(0xffffffffu, win, j);
+                    const uint32_t op = uop_op(u);
+                    const bool unary = (u & 0x40u) != 0;
+                    float a[K], b[K], t[K];
+                    if (!unary) SR::load(regs + uop_src1(u) * RS, a);
+                    if (uop_is_const(u)) {
+                        const float c = args.consts.c[uop_src2(u)];
+#pragma unroll
+                        for (int k = 0; k < K; ++k) b[k] = c;
+                    } else {
+                        SR::load(regs + uop_src2(u) * RS, b);
+                    }
+                    if (!unary && op != kDiv) CheapOps<K, PROFILE>::cheap(op, a, b, t);
+                    else slow_op<K, PROFILE>(op, a, b, t);
+                    SR::store(regs + uop_dest(u) * RS, t);
+                    if constexpr (MODE == kModeTrace) {
+                        const int64_t row = (wb + j + 1) * NR;
+#pragma unroll
+                        for (int r2 = 0; r2 < NR; ++r2) {
+                            float v[K];
+                            SR::load(regs + r2 * RS, v);
+#pragma unroll
+                            for (int q = 0; q < K / V; ++q)
+#pragma unroll
+                                for (int e = 0; e < V; ++e)
+                                    args.trace[(row + r2) * kPass + (q * 32 + lane) * V + e] = v[q * V + e];
+                        }
+                    }
+                }
+            }
+
+            float o[K];
+            SR::load(regs + args.output_reg * RS, o);
+            // case index of element k: base + (q*32 + lane)*V + e, k = q*V + e
+            if constexpr (MODE == kModeOutputs) {
+#pragma unroll
+                for (int q = 0; q < K / V; ++q)
+#pragma unroll
+                    for (int e = 0; e < V; ++e) {
+                        const int64_t c = base + (int64_t)(q * 32 + lane) * V + e;
+                        if (c < cend) args.outputs[prog * args.N + c] = o[q * V + e];
+                    }
+            } else if constexpr (MODE == kModeFitness) {
+                float t[K];
+#pragma unroll
+                for (int q = 0; q < K / V; ++q) {
+                    float w[V];
+                    load_cases<V>(args.y + c0 + q * 32 * V, w);
+#pragma unroll
+                    for (int e = 0; e < V; ++e) t[q * V + e] = w[e];
+                }
+                if constexpr (REDUCE == kReduceKahan32) {
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const int64_t c = base + (int64_t)((k / V) * 32 + lane) * V + (k % V);
+                        const float e = __fsub_rn(o[k], t[k]);
+                        const float qv = (c < cend) ? __fmul_rn(e, e) : 0.0f;
+                        const float yk = __fsub_rn(qv, kc);
+                        const float tt = __fadd_rn(ks, yk);
+                        kc = __fsub_rn(__fsub_rn(tt, ks), yk);
+                        ks = tt;
+                    }
+                } else if constexpr (REDUCE == kReduceFp64) {
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const int64_t c = base + (int64_t)((k / V) * 32 + lane) * V + (k % V);
+                        const double e = (double)o[k] - (double)t[k];
+                        if (c < cend) acc = __dadd_rn(acc, __dmul_rn(e, e));
+                    }
+                } else {
+                    // Strict case order: chunk q, lane j, element e.
+                    double qd[K];
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const double e = (double)o[k] - (double)t[k];
+                        qd[k] = __dmul_rn(e, e);
+                    }
+#pragma unroll
+                    for (int q = 0; q < K / V; ++q) {
+                        for (int j = 0; j < 32; ++j) {
+#pragma unroll
+                            for (int e = 0; e < V; ++e) {
+                                const double v = __shfl_sync(0xffffffffu, qd[q * V + e], j);
+                                if (base + (int64_t)(q * 32 + j) * V + e < cend) acc = __dadd_rn(acc, v);
+                            }
+                        }
+                    }
+                }
+            }
+            if constexpr (MODE == kModeTrace) break;
+        }
+
+        if constexpr (MODE == kModeFitness) {
+            double sse;
+            if constexpr (REDUCE == kReduceKahan32) sse = warp_sum_f64((double)ks - (double)kc);
+            else if constexpr (REDUCE == kReduceFp64) sse = warp_sum_f64(acc);
+            else sse = acc;
+            if (lane == 0) {
+                if (args.n_chunks == 1) {
+                    args.fitness[prog] = fitness_from_sse(sse, args.N);
+                    if (args.sse) args.sse[prog] = sse;
+                } else {
+                    args.partial[prog * args.n_chunks + chunk] = sse;
+                }
+            }
+        }
+        if constexpr (MODE == kModeTrace) break;
+    }
+}
+
 }  // namespace galop

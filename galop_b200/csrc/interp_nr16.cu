@@ -15,6 +15,18 @@ static const void* pick_mode(int reduce, int mode) {
     }
 }
 
+template <int K, int P>
+static const void* pick_smem_mode(int reduce, int mode) {
+    if (mode == kModeOutputs) return (const void*)&interp_smem_kernel<16, K, P, kReduceFp64, kModeOutputs>;
+    if (mode == kModeTrace) return (const void*)&interp_smem_kernel<16, K, P, kReduceFp64, kModeTrace>;
+    switch (reduce) {
+        case kReduceKahan32: return (const void*)&interp_smem_kernel<16, K, P, kReduceKahan32, kModeFitness>;
+        case kReduceFp64: return (const void*)&interp_smem_kernel<16, K, P, kReduceFp64, kModeFitness>;
+        case kReduceOrdered: return (const void*)&interp_smem_kernel<16, K, P, kReduceOrdered, kModeFitness>;
+        default: return nullptr;
+    }
+}
+
 template <int K, int D>
 static const void* pick_profile(int profile, int reduce, int mode) {
     if (profile == kProfileRef) return pick_mode<K, kProfileRef, D>(reduce, mode);
@@ -24,6 +36,11 @@ static const void* pick_profile(int profile, int reduce, int mode) {
 
 template <int K>
 static const void* pick_dispatch(int dispatch, int profile, int reduce, int mode) {
+    if (dispatch == 4) {
+        if (profile == kProfileRef) return pick_smem_mode<K, kProfileRef>(reduce, mode);
+        if (profile == kProfileBj) return pick_smem_mode<K, kProfileBj>(reduce, mode);
+        return nullptr;
+    }
     if (dispatch == 3) return pick_profile<K, 3>(profile, reduce, mode);
     if (dispatch == 2) return pick_profile<K, 2>(profile, reduce, mode);
     if (dispatch == 1) return pick_profile<K, 1>(profile, reduce, mode);

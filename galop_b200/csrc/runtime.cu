@@ -124,7 +124,7 @@ int pick_wpb(const galop_ctx* ctx) {
 
 const void* kernel_for(const galop_ctx* ctx, int k, int mode) {
     const int reduce = ctx->opt.reduce;
-    const int dispatch = (ctx->opt.dispatch >= 0 && ctx->opt.dispatch <= 3) ? ctx->opt.dispatch : 1;
+    const int dispatch = (ctx->opt.dispatch >= 0 && ctx->opt.dispatch <= 4) ? ctx->opt.dispatch : 1;
     if (ctx->isa.num_registers == 8) return interp_kernel_nr8(k, dispatch, ctx->isa.profile, reduce, mode);
     if (ctx->isa.num_registers == 16) return interp_kernel_nr16(k, dispatch, ctx->isa.profile, reduce, mode);
     return nullptr;
@@ -194,8 +194,12 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     const void* fn = kernel_for(ctx, k, mode);
     if (!fn) return ctx->fail(GALOP_E_INVALID, "no interpreter kernel for NR=%d K=%d",
                               ctx->isa.num_registers, k);
+    // Shared-memory register file (dispatch 4): NR*K floats per lane.
+    const size_t smem = ctx->opt.dispatch == 4 ? (size_t)threads * ctx->isa.num_registers * k * sizeof(float) : 0;
+    if (smem > 48 * 1024)
+        GALOP_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
     int per_sm = 0;
-    GALOP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0), "occupancy");
+    GALOP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem), "occupancy");
     if (per_sm < 1) per_sm = 1;
     const int64_t resident_warps = (int64_t)ctx->sm_count * per_sm * wpb;
 
@@ -242,7 +246,7 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned long long), s), "memset queue");
     if (n > 0) {
         void* params[] = {&a};
-        GALOP_CK(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(threads), params, 0, s),
+        GALOP_CK(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(threads), params, smem, s),
                  "interpreter launch");
         ctx->launches += 1;
     }
