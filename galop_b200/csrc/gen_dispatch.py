@@ -11,8 +11,6 @@ moves (or K arithmetic instructions) in the selected arm.
 Emitted for NR in {8, 16} and K in {1, 2, 4, 8}:
   cheap    t[k] = OP(a[k], b[k]) on the opcode alone (register file in
            shared memory, operands already loaded)
-  fused    one whole instruction, direct-threaded through three tables
-           (see fused() below)
   gather   out[k] = r[idx][k]
   scatter  r[idx][k] = v[k]
   od_vec   r[d][k] = OP(a[k], b[k])   table index op*NR + d
@@ -103,64 +101,6 @@ def od(nr: int, k: int, profile: int, scalar: bool) -> str:
             + asm_block(lines, outs, ins) + "    }\n")
 
 
-def fused(nr: int, k: int, profile: int) -> str:
-    """One LGP instruction in one PTX block, direct-threaded:
-    A table (src1 -> ta, or skip for unary ops) jumps into the B table
-    (src2 -> tb, or the constant) which jumps into the op/dest table; a
-    single-instruction op writes r[dest] and leaves, anything else copies
-    its operands to oa/ob for the C++ arm (DIV, SIN, COS, EXP, LOG)."""
-    no = nr * k
-    # operand numbering: outputs r[j][q] "+f" %(j*k+q); oa %(no+q); ob %(no+k+q)
-    #                    inputs ia %(no+2k), ib %(no+2k+1), io %(no+2k+2), c %(no+2k+3)
-    i_ia, i_ib, i_io, i_c = no + 2 * k, no + 2 * k + 1, no + 2 * k + 2, no + 2 * k + 3
-    ops = PROFILES[profile]
-    ta = [f"ta{q}" for q in range(k)]
-    tb = [f"tb{q}" for q in range(k)]
-    L = []
-    L.append(f".reg .f32 ta<{k}>, tb<{k}>;")
-    L.append("TA%=: .branchtargets " + ", ".join([f"A{j}_%=" for j in range(nr)] + ["AS%="]) + ";")
-    L.append("TB%=: .branchtargets " + ", ".join([f"B{j}_%=" for j in range(nr)] + ["BC%="]) + ";")
-    tv, tsc = [], []
-    for op in range(8):
-        for d in range(16):
-            if op in ops and d < nr:
-                tv.append(f"V{op}_{d}_%=")
-                tsc.append(f"S{op}_{d}_%=")
-            else:
-                tv.append("XV%=")
-                tsc.append("XS%=")
-    L.append("TV%=: .branchtargets " + ", ".join(tv) + ";")
-    L.append("TS%=: .branchtargets " + ", ".join(tsc) + ";")
-    L.append(f"brx.idx %{i_ia}, TA%=;")
-    for j in range(nr):
-        movs = " ".join(f"mov.f32 {ta[q]}, %{j * k + q};" for q in range(k))
-        L.append(f"A{j}_%=: {movs} brx.idx %{i_ib}, TB%=;")
-    L.append(f"AS%=: brx.idx %{i_ib}, TB%=;")
-    for j in range(nr):
-        movs = " ".join(f"mov.f32 {tb[q]}, %{j * k + q};" for q in range(k))
-        L.append(f"B{j}_%=: {movs} brx.idx %{i_io}, TV%=;")
-    L.append(f"BC%=: brx.idx %{i_io}, TS%=;")
-    for op in ops:
-        for d in range(nr):
-            body = " ".join(f"{CHEAP[op]} %{d * k + q}, {ta[q]}, {tb[q]};" for q in range(k))
-            L.append(f"V{op}_{d}_%=: {body} bra.uni E%=;")
-    for op in ops:
-        for d in range(nr):
-            body = " ".join(f"{CHEAP[op]} %{d * k + q}, {ta[q]}, %{i_c};" for q in range(k))
-            L.append(f"S{op}_{d}_%=: {body} bra.uni E%=;")
-    L.append("XV%=: " + " ".join(f"mov.f32 %{no + q}, {ta[q]}; mov.f32 %{no + k + q}, {tb[q]};"
-                                  for q in range(k)) + " bra.uni E%=;")
-    L.append("XS%=: " + " ".join(f"mov.f32 %{no + q}, {ta[q]}; mov.f32 %{no + k + q}, %{i_c};"
-                                  for q in range(k)))
-    L.append("E%=:")
-    outs = ([f'"+f"(r[{j}][{q}])' for j in range(nr) for q in range(k)]
-            + [f'"=f"(oa[{q}])' for q in range(k)] + [f'"=f"(ob[{q}])' for q in range(k)])
-    ins = ['"r"(ia)', '"r"(ib)', '"r"(io)', '"f"(c)']
-    return (f"    static __device__ __forceinline__ void fused(float (&r)[{nr}][{k}], uint32_t ia, uint32_t ib, "
-            f"uint32_t io, float c, float (&oa)[{k}], float (&ob)[{k}]) {{\n"
-            + asm_block(L, outs, ins) + "    }\n")
-
-
 def cheap_table(k: int, profile: int) -> str:
     """t[q] = OP(a[q], b[q]) for the single-instruction ops, one table on
     the opcode (8 entries, other opcodes jump to the end)."""
@@ -192,7 +132,6 @@ def main() -> None:
                 out.append(scatter(nr, k))
                 out.append(od(nr, k, prof, False))
                 out.append(od(nr, k, prof, True))
-                out.append(fused(nr, k, prof))
                 out.append("};\n")
     out.append("template <int K, int PROFILE>\nstruct CheapOps;\n")
     for k in KS:

@@ -226,101 +226,6 @@ __device__ __forceinline__ void step_brx(float (&r)[NR][K], uint32_t u, const Co
     }
 }
 
-// ---- dispatch strategy 2: jump tables, one copy of each table ------------------
-//
-// Same jump tables as strategy 1, but every helper is expanded once per
-// instruction step instead of once per op class: src2 is gathered (or the
-// constant broadcast) by one table, src1 by one, then either the fused
-// op/dest table or the C++ DIV / unary arm followed by one scatter table.
-// Less code in the instruction cache at the price of K moves for constants.
-template <int NR, int K, int PROFILE>
-__device__ __forceinline__ void step_brx_compact(float (&r)[NR][K], uint32_t u, const ConstPool& cp) {
-    using B = Brx<NR, K, PROFILE>;
-    const uint32_t op = uop_op(u);
-    float b[K];
-    if (uop_is_const(u)) {
-        const float c = cp.c[uop_src2(u)];
-#pragma unroll
-        for (int k = 0; k < K; ++k) b[k] = c;
-    } else {
-        B::gather(r, uop_src2(u), b);
-    }
-    float a[K];
-    const bool unary = (u & 0x40u) != 0;
-    if (!unary) B::gather(r, uop_src1(u), a);
-    if (!unary && op != kDiv) {
-        B::od_vec(r, op * NR + uop_dest(u), a, b);
-        return;
-    }
-    float t[K];
-    switch (op) {
-        case kDiv:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = (b[k] != 0.0f) ? __fdiv_rn(a[k], b[k]) : 1.0f;
-            break;
-        case kSin:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = sinf(b[k]);
-            break;
-        case kCos:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = cosf(b[k]);
-            break;
-        case kOp6:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp6, 0.0f, b[k]);
-            break;
-        default:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp7, 0.0f, b[k]);
-            break;
-    }
-    B::scatter(r, uop_dest(u), t);
-}
-
-// ---- dispatch strategy 3: one direct-threaded PTX block per instruction ------
-//
-// Brx<>::fused runs src1 table -> src2 table -> op/dest table, each arm
-// jumping straight into the next table (3 indirect branches and one exit
-// jump per instruction); the micro-op carries the three table indices
-// (encode_uop_threaded).  DIV and unary ops leave the block with their
-// operands and finish here, in a single copy of the C++ code.
-template <int NR, int K, int PROFILE>
-__device__ __forceinline__ void step_threaded(float (&r)[NR][K], uint32_t u, const ConstPool& cp) {
-    using B = Brx<NR, K, PROFILE>;
-    float oa[K], ob[K];
-    const float c = cp.c[(u >> 17) & 15u];
-    B::fused(r, u & 31u, (u >> 5) & 31u, (u >> 10) & 127u, c, oa, ob);
-    if (u & (1u << 21)) {
-        const uint32_t io = (u >> 10) & 127u;
-        const uint32_t op = io >> 4;
-        float t[K];
-        switch (op) {
-            case kDiv:
-#pragma unroll
-                for (int k = 0; k < K; ++k) t[k] = (ob[k] != 0.0f) ? __fdiv_rn(oa[k], ob[k]) : 1.0f;
-                break;
-            case kSin:
-#pragma unroll
-                for (int k = 0; k < K; ++k) t[k] = sinf(ob[k]);
-                break;
-            case kCos:
-#pragma unroll
-                for (int k = 0; k < K; ++k) t[k] = cosf(ob[k]);
-                break;
-            case kOp6:
-#pragma unroll
-                for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp6, 0.0f, ob[k]);
-                break;
-            default:
-#pragma unroll
-                for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp7, 0.0f, ob[k]);
-                break;
-        }
-        B::scatter(r, io & 15u, t);
-    }
-}
-
 __device__ __forceinline__ double warp_sum_f64(double v) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -386,9 +291,7 @@ interp_kernel(InterpArgs args) {
                 const int n = (L - wb < 32) ? (int)(L - wb) : 32;
                 for (int j = 0; j < n; ++j) {
                     const uint32_t u = __shfl_sync(0xffffffffu, win, j);
-                    if constexpr (DISPATCH == 3) step_threaded<NR, K, PROFILE>(r, u, args.consts);
-                    else if constexpr (DISPATCH == 2) step_brx_compact<NR, K, PROFILE>(r, u, args.consts);
-                    else if constexpr (DISPATCH == 1) step_brx<NR, K, PROFILE>(r, u, args.consts);
+                    if constexpr (DISPATCH == 1) step_brx<NR, K, PROFILE>(r, u, args.consts);
                     else step<NR, K, PROFILE>(r, u, args.consts);
                     if constexpr (MODE == kModeTrace) {
                         const int64_t row = (wb + j + 1) * NR;
@@ -471,7 +374,7 @@ interp_kernel(InterpArgs args) {
 }
 
 
-// ---- dispatch strategy 4: the LGP register file in shared memory --------------
+// ---- dispatch strategy 2 (default): the LGP register file in shared memory -----
 //
 // Each lane keeps its K cases' NR registers in its own shared-memory slots:
 // register j of the warp is a block of 32*K floats, lane l owns the K
@@ -541,15 +444,25 @@ __device__ __forceinline__ void slow_op(uint32_t op, const float (&a)[K], const 
     }
 }
 
+// 64 registers per thread (8 blocks of 128 threads per SM) hold every
+// instantiation without spills; residency is then bounded by shared memory.
 template <int NR, int K, int PROFILE, int REDUCE, int MODE>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(128, 8)
 interp_smem_kernel(InterpArgs args) {
+    // Shared memory: [constant pool: NR registers x 32 lanes x K][warp 0
+    // registers][warp 1 registers]...  The pool is written once per block
+    // with every value in every lane slot, so "src2 = constant i" is just a
+    // load of pool register i: operand fetch has no branch.
     extern __shared__ float4 galop_smem4[];
     using SR = SmemRegs<K>;
     constexpr int V = SR::V;
     constexpr int RS = SR::kStride;
     const int lane = threadIdx.x & 31;
-    float* regs = reinterpret_cast<float*>(galop_smem4) + (threadIdx.x >> 5) * NR * RS + lane * V;
+    float* pool = reinterpret_cast<float*>(galop_smem4) + lane * V;
+    float* regs = reinterpret_cast<float*>(galop_smem4) + NR * RS + (threadIdx.x >> 5) * NR * RS + lane * V;
+    for (int i = threadIdx.x; i < NR * RS; i += blockDim.x)
+        reinterpret_cast<float*>(galop_smem4)[i] = args.consts.c[i / RS];
+    __syncthreads();
     const int64_t total_items = args.n_programs * (int64_t)args.n_chunks;
     constexpr int kPass = 32 * K;
 
@@ -608,17 +521,11 @@ interp_smem_kernel(InterpArgs args) {
                 for (int j = 0; j < n; ++j) {
                     const uint32_t u = __shfl_sync(0xffffffffu, win, j);
                     const uint32_t op = uop_op(u);
-                    const bool unary = (u & 0x40u) != 0;
                     float a[K], b[K], t[K];
-                    if (!unary) SR::load(regs + uop_src1(u) * RS, a);
-                    if (uop_is_const(u)) {
-                        const float c = args.consts.c[uop_src2(u)];
-#pragma unroll
-                        for (int k = 0; k < K; ++k) b[k] = c;
-                    } else {
-                        SR::load(regs + uop_src2(u) * RS, b);
-                    }
-                    if (!unary && op != kDiv) CheapOps<K, PROFILE>::cheap(op, a, b, t);
+                    // src1 is loaded for unary ops too (ignored): no branch.
+                    SR::load(regs + uop_src1(u) * RS, a);
+                    SR::load((uop_is_const(u) ? pool : regs) + uop_src2(u) * RS, b);
+                    if ((u & 0x40u) == 0 && op != kDiv) CheapOps<K, PROFILE>::cheap(op, a, b, t);
                     else slow_op<K, PROFILE>(op, a, b, t);
                     SR::store(regs + uop_dest(u) * RS, t);
                     if constexpr (MODE == kModeTrace) {

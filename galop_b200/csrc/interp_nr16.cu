@@ -1,6 +1,7 @@
 // Instantiations of the interpreter for 16-register ISAs.
 #include "interp.cuh"
 
+
 namespace galop {
 
 template <int K, int P, int D>
@@ -36,13 +37,11 @@ static const void* pick_profile(int profile, int reduce, int mode) {
 
 template <int K>
 static const void* pick_dispatch(int dispatch, int profile, int reduce, int mode) {
-    if (dispatch == 4) {
+    if (dispatch == 2) {
         if (profile == kProfileRef) return pick_smem_mode<K, kProfileRef>(reduce, mode);
         if (profile == kProfileBj) return pick_smem_mode<K, kProfileBj>(reduce, mode);
         return nullptr;
     }
-    if (dispatch == 3) return pick_profile<K, 3>(profile, reduce, mode);
-    if (dispatch == 2) return pick_profile<K, 2>(profile, reduce, mode);
     if (dispatch == 1) return pick_profile<K, 1>(profile, reduce, mode);
     return pick_profile<K, 0>(profile, reduce, mode);
 }

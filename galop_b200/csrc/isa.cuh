@@ -63,24 +63,6 @@ __host__ __device__ __forceinline__ uint32_t encode_uop(const Decoded& d) {
     return (d.op | (d.unary << 6)) | (d.dest << 8) | (d.src1 << 16) | ((d.src2 | (d.is_const << 7)) << 24);
 }
 
-// Micro-op of the direct-threaded interpreter (one PTX block per
-// instruction): table indices precomputed here.
-//   [0,5)   ia   src1 register, or NR for unary ops (skip)
-//   [5,10)  ib   src2 register, or NR for a constant src2
-//   [10,17) io   op*16 + dest (op/dest table)
-//   [17,21) constant index
-//   21      slow: DIV or unary, finished by the C++ arm
-constexpr int kUopFormatBytes = 0;
-constexpr int kUopFormatThreaded = 1;
-
-__host__ __device__ __forceinline__ uint32_t encode_uop_threaded(const Decoded& d, int nr) {
-    const uint32_t ia = d.unary ? (uint32_t)nr : d.src1;
-    const uint32_t ib = d.is_const ? (uint32_t)nr : d.src2;
-    const uint32_t io = d.op * 16u + d.dest;
-    const uint32_t slow = (d.unary || d.op == kDiv) ? 1u : 0u;
-    return ia | (ib << 5) | (io << 10) | ((d.src2 & 15u) << 17) | (slow << 21);
-}
-
 __device__ __forceinline__ uint32_t uop_op(uint32_t u) { return u & 7u; }
 __device__ __forceinline__ uint32_t uop_dest(uint32_t u) { return (u >> 8) & 0xffu; }
 __device__ __forceinline__ uint32_t uop_src1(uint32_t u) { return (u >> 16) & 0xffu; }

@@ -179,7 +179,7 @@ __global__ void scan_apply_kernel(const int32_t* __restrict__ in, int64_t n,
 // Write micro-ops of the interpreted instructions of program i at eff_off[i].
 // raw_out (optional) receives the raw words of the same instructions.
 template <class Src>
-__global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int strip, int format,
+__global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int strip,
                                        const int64_t* __restrict__ eff_off,
                                        uint32_t* __restrict__ uops,
                                        uint32_t* __restrict__ raw_out) {
@@ -191,9 +191,7 @@ __global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int st
     if (!strip) {
         for (int64_t pc = 0; pc < raw; ++pc) {
             const uint32_t w = __ldg(src.words + s + pc);
-            const Decoded d = decode_raw(isa, w);
-            uops[o + pc] = format == kUopFormatThreaded ? encode_uop_threaded(d, isa.num_registers)
-                                                        : encode_uop(d);
+            uops[o + pc] = encode_uop(decode_raw(isa, w));
             if (raw_out) raw_out[o + pc] = w;
         }
         return;
@@ -205,7 +203,7 @@ __global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int st
         const Decoded d = decode_raw(isa, w);
         if (!((live >> d.dest) & 1u)) continue;
         --pos;
-        uops[pos] = format == kUopFormatThreaded ? encode_uop_threaded(d, isa.num_registers) : encode_uop(d);
+        uops[pos] = encode_uop(d);
         if (raw_out) raw_out[pos] = w;
         live &= ~(1u << d.dest);
         if (!d.unary) live |= 1u << d.src1;

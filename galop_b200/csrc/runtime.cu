@@ -114,7 +114,7 @@ namespace {
 int pick_k(const galop_ctx* ctx) {
     const int k = ctx->opt.cases_per_lane;
     if (k == 1 || k == 2 || k == 4 || k == 8) return k;
-    return ctx->isa.num_registers >= 16 ? 2 : 4;
+    return 4;
 }
 
 int pick_wpb(const galop_ctx* ctx) {
@@ -124,7 +124,7 @@ int pick_wpb(const galop_ctx* ctx) {
 
 const void* kernel_for(const galop_ctx* ctx, int k, int mode) {
     const int reduce = ctx->opt.reduce;
-    const int dispatch = (ctx->opt.dispatch >= 0 && ctx->opt.dispatch <= 4) ? ctx->opt.dispatch : 1;
+    const int dispatch = (ctx->opt.dispatch >= 0 && ctx->opt.dispatch <= 2) ? ctx->opt.dispatch : 2;
     if (ctx->isa.num_registers == 8) return interp_kernel_nr8(k, dispatch, ctx->isa.profile, reduce, mode);
     if (ctx->isa.num_registers == 16) return interp_kernel_nr16(k, dispatch, ctx->isa.profile, reduce, mode);
     return nullptr;
@@ -165,8 +165,7 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
     // Device buffer for micro-ops sized by the raw total (an upper bound).
     GALOP_CK(ctx->uops.ensure((size_t)std::max<int64_t>(raw_words_total, 1)), "alloc uops");
     if (n > 0) {
-        const int format = ctx->opt.dispatch == 3 ? kUopFormatThreaded : kUopFormatBytes;
-        prepass_compact_kernel<Src><<<blocks, tpb, 0, s>>>(src, n, ctx->isa, strip ? 1 : 0, format,
+        prepass_compact_kernel<Src><<<blocks, tpb, 0, s>>>(src, n, ctx->isa, strip ? 1 : 0,
                                                            ctx->eff_off.p, ctx->uops.p, raw_out);
         ctx->launches += 1;
     }
@@ -195,9 +194,14 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     if (!fn) return ctx->fail(GALOP_E_INVALID, "no interpreter kernel for NR=%d K=%d",
                               ctx->isa.num_registers, k);
     // Shared-memory register file (dispatch 4): NR*K floats per lane.
-    const size_t smem = ctx->opt.dispatch == 4 ? (size_t)threads * ctx->isa.num_registers * k * sizeof(float) : 0;
-    if (smem > 48 * 1024)
+    // plus one block-shared copy of the constant pool laid out the same way.
+    const size_t smem = ctx->opt.dispatch == 2
+                            ? (size_t)(threads + 32) * ctx->isa.num_registers * k * sizeof(float) : 0;
+    if (smem) {
         GALOP_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        GALOP_CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared), "smem carveout");
+    }
     int per_sm = 0;
     GALOP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem), "occupancy");
     if (per_sm < 1) per_sm = 1;
@@ -364,7 +368,7 @@ int galop_options_init(galop_options* opt) {
     opt->intron_prepass = 1;
     opt->cases_per_lane = 0;
     opt->warps_per_block = 0;
-    opt->dispatch = 1;
+    opt->dispatch = 2;
     return GALOP_OK;
 }
 

@@ -80,9 +80,10 @@ typedef struct {
                                  (src/Introns.h:28-57); outputs unchanged       */
     int32_t cases_per_lane;   /* 0 = tuned default; else 1, 2, 4 or 8          */
     int32_t warps_per_block;  /* 0 = tuned default; else 1..8                  */
-    int32_t dispatch;         /* interpreter register access: 1 = PTX jump
-                                 tables, cheap ops fused with their dest
-                                 (default); 0 = plain C++ switches          */
+    int32_t dispatch;         /* LGP register file: 2 = shared memory,
+                                 register index = address (default);
+                                 1 = lane registers behind PTX jump tables;
+                                 0 = lane registers behind C++ switches     */
     int32_t reserved[3];
 } galop_options;
 
