@@ -324,9 +324,9 @@ def run_b200(args, dist: Dist):
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         try:
             from oracle.oracle import Oracle, RefCuda
-            m = min(n, 32768)
+            m = min(n, 4096)
             sub = wl.subsample(np.arange(m))
-            _, kms = RefCuda().evaluate_packed(sub.words, sub.offsets, wl.X, wl.y, reps=2)
+            _, kms = RefCuda().evaluate_packed(sub.words, sub.offsets, wl.X, wl.y, reps=1)
             eff = float(Oracle(0, 16).effective_lengths(sub.words, sub.offsets).sum())
             ref_gpu = {"value": eff * wl.n_cases / (kms / 1e3) / 1e9, "unit": UNIT,
                        "raw_gpops": float(sub.offsets[-1]) * wl.n_cases / (kms / 1e3) / 1e9,

@@ -444,10 +444,10 @@ __device__ __forceinline__ void slow_op(uint32_t op, const float (&a)[K], const 
     }
 }
 
-// 64 registers per thread (8 blocks of 128 threads per SM) hold every
+// 64 registers per thread (4 blocks of 256 threads per SM) hold every
 // instantiation without spills; residency is then bounded by shared memory.
 template <int NR, int K, int PROFILE, int REDUCE, int MODE>
-__global__ void __launch_bounds__(128, 8)
+__global__ void __launch_bounds__(256, 4)
 interp_smem_kernel(InterpArgs args) {
     // Shared memory: [constant pool: NR registers x 32 lanes x K][warp 0
     // registers][warp 1 registers]...  The pool is written once per block

@@ -98,6 +98,7 @@ struct galop_ctx {
         return code;
     }
     int cuda_fail(cudaError_t e, const char* what) {
+        cudaGetLastError();   // a non-sticky error must not resurface in a later call
         return fail(e == cudaErrorMemoryAllocation ? GALOP_E_NOMEM : GALOP_E_CUDA,
                     "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
     }
