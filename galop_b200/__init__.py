@@ -49,7 +49,7 @@ EXPORTED = (
     "galop_case_outputs_csr", "galop_trace_program", "galop_effective_csr", "galop_last_stats",
     "galop_synchronize", "galop_host_alloc", "galop_host_free", "galop_device_alloc",
     "galop_device_free", "galop_memcpy_h2d", "galop_memcpy_d2h", "galop_timer_record",
-    "galop_timer_elapsed",
+    "galop_timer_elapsed", "galop_evaluate_csr_noalloc",
 )
 
 
@@ -126,6 +126,8 @@ def load_library(path: Optional[Path] = None) -> C.CDLL:
         "galop_memcpy_d2h": (C.c_int, [_P, _P, _P, C.c_int64]),
         "galop_timer_record": (C.c_int, [_P, C.c_int32]),
         "galop_timer_elapsed": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+        "galop_evaluate_csr_noalloc": (C.c_int, [C.POINTER(_Options), _P, _P, C.c_int64, C.c_int64, _P, _P,
+                                                 C.c_int64, C.c_int64, C.c_int32, _P, _P, _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

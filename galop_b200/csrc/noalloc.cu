@@ -1,0 +1,203 @@
+// noalloc.cu -- population evaluation for callers that cannot allocate.
+//
+// Every other entry point keeps its working buffers (micro-ops, offsets,
+// evaluation order, work-queue counters, per-chunk partial sums) in device
+// memory it obtains with cudaMalloc and grows as populations grow.  Some
+// callers cannot let a library do that: cudaMalloc and cudaFree synchronise
+// the whole device and are not permitted while a stream is being captured,
+// and hosts that own a fixed device-memory budget (a framework's own pool,
+// a serving process that must never hit an out-of-memory error mid-run)
+// cannot have a library allocate behind their back.
+//
+// galop_evaluate_csr_noalloc runs the same pre-pass and interpreter kernels
+// as galop_evaluate_csr_device, but its working buffers live in one
+// file-scope __device__ array of fixed size (about 11 MiB) that every GPU
+// loading this library holds until the process exits.  It allocates nothing:
+// no cudaMalloc, no cudaFree, no allocating library routine.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <mutex>
+
+#include "../../include/galop_b200.h"
+#include "interp.cuh"
+#include "prepass.cuh"
+
+namespace galop {
+const void* interp_kernel_nr8(int k, int dispatch, int profile, int reduce, int mode);
+const void* interp_kernel_nr16(int k, int dispatch, int profile, int reduce, int mode);
+}  // namespace galop
+
+using namespace galop;
+
+namespace {
+
+constexpr int64_t kNaMaxPrograms = GALOP_NOALLOC_MAX_PROGRAMS;
+constexpr int64_t kNaMaxWords = GALOP_NOALLOC_MAX_WORDS;
+constexpr int64_t kNaMaxPartials = 4 * GALOP_NOALLOC_MAX_PROGRAMS;
+constexpr int64_t kNaMaxTiles = (kNaMaxPrograms + kScanTile - 1) / kScanTile;
+
+struct NoAllocScratch {
+    uint32_t uops[kNaMaxWords];
+    int64_t eff_off[kNaMaxPrograms + 1];
+    int64_t tiles[kNaMaxTiles + 1];
+    double partial[kNaMaxPartials];
+    int32_t eff_len[kNaMaxPrograms];
+    int32_t order[kNaMaxPrograms];
+    unsigned int hist[kOrderBins];
+    unsigned long long counters[4];   // [0] work-queue head, [1..2] length totals
+};
+
+// The scratch itself.  Host code must not pass `g_noalloc_scratch` to a
+// kernel: in host code the name is a host-side stand-in, not a device
+// address.  The device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+NoAllocScratch* g_scratch_addr[kMaxDevices] = {};
+
+// Once per device, with that device current: the scratch's device address.
+cudaError_t scratch_for_device(int device, NoAllocScratch** out) {
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_addr[device] = static_cast<NoAllocScratch*>(p);
+    }
+    *out = g_scratch_addr[device];
+    return cudaSuccess;
+}
+
+// Reference constant pools (src/LGPConfig.h:159-168).
+const float kPool8[8] = {0.0f, 1.0f, -1.0f, 3.14159f, 0.5f, 2.0f, 10.0f, 100.0f};
+const float kPool16[16] = {0.0f, 1.0f, -1.0f, 3.14159f, 0.5f, 2.0f, 10.0f, 100.0f,
+                           0.1f, -0.5f, 0.25f, 5.0f, 20.0f, -2.0f, 0.01f, 1000.0f};
+
+}  // namespace
+
+extern "C" int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32_t* d_words,
+                                          const int64_t* d_offsets, int64_t n_programs, int64_t total_words,
+                                          const float* d_inputs, const float* d_targets, int64_t n_cases,
+                                          int64_t padded_cases, int32_t num_inputs, float* d_fitness,
+                                          double* d_sse, void* stream) {
+    if (!opt || !d_offsets || n_programs < 0 || total_words < 0 || n_cases < 0) return GALOP_E_INVALID;
+    if (opt->num_registers != 8 && opt->num_registers != 16) return GALOP_E_INVALID;
+    if (opt->profile != GALOP_PROFILE_REF && opt->profile != GALOP_PROFILE_BJ) return GALOP_E_INVALID;
+    if (opt->reduce < GALOP_REDUCE_KAHAN32 || opt->reduce > GALOP_REDUCE_ORDERED) return GALOP_E_INVALID;
+    if (num_inputs < 0 || num_inputs > opt->num_registers) return GALOP_E_INVALID;
+    if (padded_cases < n_cases || padded_cases % 1024 != 0 || padded_cases == 0) return GALOP_E_INVALID;
+    if (n_programs > kNaMaxPrograms || total_words > kNaMaxWords) return GALOP_E_CAPACITY;
+    if (n_programs > 0 && (!d_words && total_words > 0)) return GALOP_E_INVALID;
+    if (n_programs > 0 && (!d_fitness || !d_targets || (num_inputs > 0 && !d_inputs))) return GALOP_E_INVALID;
+    if (n_programs == 0) return GALOP_OK;
+
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return GALOP_E_NO_DEVICE; }
+    NoAllocScratch* sc = nullptr;
+    if (scratch_for_device(device, &sc) != cudaSuccess) { cudaGetLastError(); return GALOP_E_CUDA; }
+    int sm_count = 0;
+    if (cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        return GALOP_E_CUDA;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    IsaParams isa{opt->profile, opt->num_registers, opt->input_protect ? 1 : 0,
+                  opt->input_protect ? opt->num_registers / 2 : 0};
+    ConstPool pool{};
+    const float* src_pool = opt->constants ? opt->constants : (opt->num_registers == 16 ? kPool16 : kPool8);
+    for (int i = 0; i < kMaxRegisters; ++i) pool.c[i] = i < opt->num_registers ? src_pool[i] : 0.0f;
+    const bool strip = opt->intron_prepass != 0;
+    const int k = (opt->cases_per_lane == 1 || opt->cases_per_lane == 2 || opt->cases_per_lane == 4 ||
+                   opt->cases_per_lane == 8) ? opt->cases_per_lane : 4;
+    const int wpb = (opt->warps_per_block >= 1 && opt->warps_per_block <= 8) ? opt->warps_per_block : 4;
+    const int dispatch = (opt->dispatch >= 0 && opt->dispatch <= 2) ? opt->dispatch : 2;
+
+    // The work-queue head, the length totals and the order histogram carry
+    // the previous call's values: clear them first.
+    cudaError_t e = cudaMemsetAsync(sc->counters, 0, sizeof(sc->counters), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(sc->hist, 0, sizeof(sc->hist), s);
+    if (e != cudaSuccess) { cudaGetLastError(); return GALOP_E_CUDA; }
+
+    // Intron pass, scan, compaction, longest-first order (prepass.cuh).
+    CsrSource src{d_words, d_offsets};
+    const int64_t n = n_programs;
+    const int tpb = 256;
+    const unsigned blocks = (unsigned)((n + tpb - 1) / tpb);
+    const int64_t n_tiles = (n + kScanTile - 1) / kScanTile;
+    prepass_count_kernel<CsrSource><<<blocks, tpb, 0, s>>>(src, n, isa, strip ? 1 : 0, sc->eff_len,
+                                                           sc->counters + 1);
+    scan_tile_sums_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(sc->eff_len, n, sc->tiles);
+    scan_tile_offsets_kernel<<<1, kScanThreads, 0, s>>>(sc->tiles, n_tiles);
+    scan_apply_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(sc->eff_len, n, sc->tiles, n_tiles, sc->eff_off);
+    prepass_compact_kernel<CsrSource><<<blocks, tpb, 0, s>>>(src, n, isa, strip ? 1 : 0, sc->eff_off, sc->uops,
+                                                             nullptr);
+    const bool sched = n > 1;
+    if (sched) {
+        order_hist_kernel<<<blocks, tpb, 0, s>>>(sc->eff_len, n, sc->hist);
+        order_scan_kernel<<<1, 1024, 0, s>>>(sc->hist);
+        order_scatter_kernel<<<blocks, tpb, 0, s>>>(sc->eff_len, n, sc->hist, sc->order);
+    }
+    if (cudaGetLastError() != cudaSuccess) return GALOP_E_CUDA;
+
+    // Interpreter: same kernel selection and case chunking as the other entry points.
+    const void* fn = opt->num_registers == 8 ? interp_kernel_nr8(k, dispatch, opt->profile, opt->reduce, kModeFitness)
+                                             : interp_kernel_nr16(k, dispatch, opt->profile, opt->reduce, kModeFitness);
+    if (!fn) return GALOP_E_INVALID;
+    const int threads = 32 * wpb;
+    const size_t smem = dispatch == 2 ? (size_t)(threads + 32) * opt->num_registers * k * sizeof(float) : 0;
+    if (smem) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) { cudaGetLastError(); return GALOP_E_CUDA; }
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return GALOP_E_CUDA;
+    }
+    per_sm = std::max(per_sm, 1);
+    const int64_t resident_warps = (int64_t)sm_count * per_sm * wpb;
+    const int64_t pass = 32LL * k;
+    const int64_t passes = std::max<int64_t>(1, (n_cases + pass - 1) / pass);
+    int64_t n_chunks = 1;
+    if (opt->reduce != GALOP_REDUCE_ORDERED && n < 4 * resident_warps)
+        n_chunks = std::min<int64_t>(passes, (4 * resident_warps + n - 1) / n);
+    n_chunks = std::min<int64_t>(n_chunks, kNaMaxPartials / n);
+    const int64_t chunk_cases = ((passes + n_chunks - 1) / n_chunks) * pass;
+    n_chunks = std::max<int64_t>(1, (std::max<int64_t>(n_cases, 1) + chunk_cases - 1) / chunk_cases);
+
+    InterpArgs a{};
+    a.uops = sc->uops;
+    a.eff_off = sc->eff_off;
+    a.order = sched ? sc->order : nullptr;
+    a.n_programs = n;
+    a.n_chunks = (int32_t)n_chunks;
+    a.chunk_cases = chunk_cases;
+    a.X = d_inputs;
+    a.y = d_targets;
+    a.N = n_cases;
+    a.Np = padded_cases;
+    a.num_inputs = num_inputs;
+    a.output_reg = isa.output_reg;
+    a.consts = pool;
+    a.counter = sc->counters;
+    a.fitness = d_fitness;
+    a.sse = d_sse;
+    a.partial = n_chunks > 1 ? sc->partial : nullptr;
+    const int64_t need = (n * n_chunks + wpb - 1) / wpb;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((int64_t)sm_count * per_sm, need));
+    void* params[] = {&a};
+    if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(threads), params, smem, s) != cudaSuccess) {
+        cudaGetLastError();
+        return GALOP_E_CUDA;
+    }
+    if (n_chunks > 1)
+        finalize_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(sc->partial, n, (int)n_chunks, n_cases,
+                                                                  d_fitness, d_sse);
+    if (cudaGetLastError() != cudaSuccess) return GALOP_E_CUDA;
+    return GALOP_OK;
+}

@@ -82,7 +82,7 @@ __global__ void prepass_count_kernel(Src src, int64_t n, IsaParams isa, int stri
 }
 
 // Phase 1: per-tile sums.
-__global__ void scan_tile_sums_kernel(const int32_t* __restrict__ in, int64_t n,
+static __global__ void scan_tile_sums_kernel(const int32_t* __restrict__ in, int64_t n,
                                       int64_t* __restrict__ tile_sums) {
     __shared__ int64_t warp_sums[kScanThreads / 32];
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
@@ -106,7 +106,7 @@ __global__ void scan_tile_sums_kernel(const int32_t* __restrict__ in, int64_t n,
 
 // Phase 2: exclusive scan of the tile sums in one block (serial over chunks
 // of kScanThreads), total written at tile_sums[n_tiles].
-__global__ void scan_tile_offsets_kernel(int64_t* __restrict__ tile_sums, int64_t n_tiles) {
+static __global__ void scan_tile_offsets_kernel(int64_t* __restrict__ tile_sums, int64_t n_tiles) {
     __shared__ int64_t buf[kScanThreads];
     __shared__ int64_t carry;
     if (threadIdx.x == 0) carry = 0;
@@ -133,7 +133,7 @@ __global__ void scan_tile_offsets_kernel(int64_t* __restrict__ tile_sums, int64_
 }
 
 // Phase 3: exclusive scan inside each tile plus the tile offset; out[n] = total.
-__global__ void scan_apply_kernel(const int32_t* __restrict__ in, int64_t n,
+static __global__ void scan_apply_kernel(const int32_t* __restrict__ in, int64_t n,
                                   const int64_t* __restrict__ tile_offsets, int64_t n_tiles,
                                   int64_t* __restrict__ out) {
     __shared__ int64_t warp_tot[kScanThreads / 32];
@@ -212,7 +212,7 @@ __global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int st
 }
 
 // Longest-first order: histogram of bins (bin 0 = longest), scan, scatter.
-__global__ void order_hist_kernel(const int32_t* __restrict__ len, int64_t n,
+static __global__ void order_hist_kernel(const int32_t* __restrict__ len, int64_t n,
                                   unsigned int* __restrict__ hist) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -221,7 +221,7 @@ __global__ void order_hist_kernel(const int32_t* __restrict__ len, int64_t n,
     atomicAdd(&hist[kOrderBins - 1 - l], 1u);
 }
 
-__global__ void order_scan_kernel(unsigned int* __restrict__ hist) {
+static __global__ void order_scan_kernel(unsigned int* __restrict__ hist) {
     // Single block of 1024 threads, 4 bins per thread, exclusive in place.
     __shared__ unsigned int buf[1024];
     const int t = threadIdx.x;
@@ -241,7 +241,7 @@ __global__ void order_scan_kernel(unsigned int* __restrict__ hist) {
     for (int j = 0; j < 4; ++j) { hist[t * 4 + j] = run; run += v[j]; }
 }
 
-__global__ void order_scatter_kernel(const int32_t* __restrict__ len, int64_t n,
+static __global__ void order_scatter_kernel(const int32_t* __restrict__ len, int64_t n,
                                      unsigned int* __restrict__ cursor,
                                      int32_t* __restrict__ order) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -253,7 +253,7 @@ __global__ void order_scatter_kernel(const int32_t* __restrict__ len, int64_t n,
 }
 
 // Case-major (AoS) dataset to feature-major (SoA) with zero padding to Np.
-__global__ void dataset_transpose_kernel(const float* __restrict__ aos, const float* __restrict__ y_in,
+static __global__ void dataset_transpose_kernel(const float* __restrict__ aos, const float* __restrict__ y_in,
                                          int64_t n, int k, int64_t np,
                                          float* __restrict__ X, float* __restrict__ y) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -264,7 +264,7 @@ __global__ void dataset_transpose_kernel(const float* __restrict__ aos, const fl
 }
 
 // Sum of chunk partials in chunk order, then fitness.
-__global__ void finalize_kernel(const double* __restrict__ partial, int64_t n_programs,
+static __global__ void finalize_kernel(const double* __restrict__ partial, int64_t n_programs,
                                 int n_chunks, int64_t n_cases, float* __restrict__ fitness,
                                 double* __restrict__ sse_out) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -202,6 +202,44 @@ GALOP_API int galop_device_free(galop_ctx* ctx, void* p);
 GALOP_API int galop_memcpy_h2d(galop_ctx* ctx, void* dst, const void* src, int64_t bytes);
 GALOP_API int galop_memcpy_d2h(galop_ctx* ctx, void* dst, const void* src, int64_t bytes);
 
+/* ---- evaluation without allocation --------------------------------------- */
+
+/* Limits of galop_evaluate_csr_noalloc: programs and total instructions per
+ * call.  Its working buffers are a fixed ~11 MiB __device__ array that every
+ * GPU loading this library holds until the process exits. */
+#define GALOP_NOALLOC_MAX_PROGRAMS 65536
+#define GALOP_NOALLOC_MAX_WORDS 2097152
+
+/* No counterpart in the reference.  For callers that cannot let a library
+ * call cudaMalloc: code that evaluates while a stream is being captured
+ * (cudaMalloc and cudaFree are not allowed there and would synchronise the
+ * device), and hosts that hand the library a fixed device-memory budget and
+ * cannot afford an out-of-memory failure in the middle of a run.  It needs no
+ * galop_ctx and allocates nothing -- no cudaMalloc, no cudaFree, no
+ * allocating library routine; its scratch is the static array above.
+ *
+ * Same evaluation as galop_evaluate_csr_device: device pointers, CSR programs
+ * (words, int64 offsets starting at 0, total_words = offsets[n_programs]), the
+ * dataset already feature-major on the device -- d_inputs[f*padded_cases + c],
+ * d_targets[c], padded_cases a multiple of 1024 and >= n_cases (padding values
+ * are never counted) -- opt as for galop_create (device ignored: the current
+ * device is used).  Work is queued on `stream` (NULL = default stream) and the
+ * call returns without waiting.
+ *
+ * Limits: n_programs <= GALOP_NOALLOC_MAX_PROGRAMS and total_words <=
+ * GALOP_NOALLOC_MAX_WORDS, else GALOP_E_CAPACITY with nothing queued.
+ * The first call on a device looks up the scratch's device address (and
+ * loads this library's code on that device); make that first call before any
+ * stream capture.  Every call uses the same scratch: calls whose work
+ * overlaps on the GPU (different streams, or different host threads, without
+ * ordering between them) race and corrupt each other's results. */
+GALOP_API int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32_t* d_words,
+                                         const int64_t* d_offsets, int64_t n_programs,
+                                         int64_t total_words, const float* d_inputs,
+                                         const float* d_targets, int64_t n_cases,
+                                         int64_t padded_cases, int32_t num_inputs,
+                                         float* d_fitness, double* d_sse, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
