@@ -49,7 +49,13 @@ EXPORTED = (
     "galop_case_outputs_csr", "galop_trace_program", "galop_effective_csr", "galop_last_stats",
     "galop_synchronize", "galop_host_alloc", "galop_host_free", "galop_device_alloc",
     "galop_device_free", "galop_memcpy_h2d", "galop_memcpy_d2h", "galop_timer_record",
-    "galop_timer_elapsed", "galop_evaluate_csr_noalloc",
+    "galop_timer_elapsed", "galop_evaluate_csr_noalloc", "galop_dataset_create", "galop_dataset_destroy",
+    "galop_dataset_device_bytes", "galop_batch_create", "galop_batch_destroy", "galop_batch_device_bytes",
+    "galop_batch_set_population", "galop_batch_evaluate", "galop_batch_synchronize", "galop_batch_get_fitness",
+    "galop_batch_last_stats", "galop_batch_stream", "galop_batch_create_pool", "galop_batch_clear",
+    "galop_batch_append", "galop_batch_population_work", "galop_server_options_init", "galop_server_create",
+    "galop_server_destroy", "galop_server_open_run", "galop_server_close_run", "galop_server_submit",
+    "galop_server_wait", "galop_server_stats",
 )
 
 
@@ -74,6 +80,25 @@ class Stats(C.Structure):
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
+class PopulationSpec(C.Structure):
+    _fields_ = [("dataset", C.c_void_p), ("max_programs", C.c_int64), ("max_words", C.c_int64)]
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("slots", C.c_int32), ("max_pops_per_batch", C.c_int32),
+                ("slot_programs", C.c_int64), ("slot_words", C.c_int64), ("slot_items", C.c_int64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("batch_requests", C.c_int32), ("eff_instructions", C.c_int64),
+                ("queued_ms", C.c_double), ("latency_ms", C.c_double), ("device_ms", C.c_double)]
+
+
+class ServerTotals(C.Structure):
+    _fields_ = [("completed", C.c_int64), ("batches", C.c_int64), ("pending", C.c_int64),
+                ("resident_bytes", C.c_int64), ("case_ops", C.c_int64), ("device_ms", C.c_double)]
 
 
 class GalopError(RuntimeError):
@@ -128,6 +153,30 @@ def load_library(path: Optional[Path] = None) -> C.CDLL:
         "galop_timer_elapsed": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
         "galop_evaluate_csr_noalloc": (C.c_int, [C.POINTER(_Options), _P, _P, C.c_int64, C.c_int64, _P, _P,
                                                  C.c_int64, C.c_int64, C.c_int32, _P, _P, _P]),
+        "galop_dataset_create": (C.c_int, [_P, _F32P, _F32P, C.c_int64, C.c_int32, C.POINTER(_P)]),
+        "galop_dataset_destroy": (C.c_int, [_P]),
+        "galop_dataset_device_bytes": (C.c_int64, [_P]),
+        "galop_batch_create": (C.c_int, [_P, C.POINTER(PopulationSpec), C.c_int32, C.POINTER(_P)]),
+        "galop_batch_destroy": (C.c_int, [_P]),
+        "galop_batch_device_bytes": (C.c_int64, [_P]),
+        "galop_batch_set_population": (C.c_int, [_P, C.c_int32, _U32P, _I64P, C.c_int64]),
+        "galop_batch_evaluate": (C.c_int, [_P, C.c_int32]),
+        "galop_batch_synchronize": (C.c_int, [_P]),
+        "galop_batch_get_fitness": (C.c_int, [_P, C.c_int32, _F32P, _F64P]),
+        "galop_batch_last_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+        "galop_batch_stream": (_P, [_P]),
+        "galop_batch_create_pool": (C.c_int, [_P, C.c_int32, C.c_int64, C.c_int64, C.c_int64, C.POINTER(_P)]),
+        "galop_batch_clear": (C.c_int, [_P]),
+        "galop_batch_append": (C.c_int, [_P, _P, _U32P, _I64P, C.c_int64, C.POINTER(C.c_int32)]),
+        "galop_batch_population_work": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int64)]),
+        "galop_server_options_init": (C.c_int, [C.POINTER(ServerOptions)]),
+        "galop_server_create": (C.c_int, [_P, C.POINTER(ServerOptions), C.POINTER(_P)]),
+        "galop_server_destroy": (C.c_int, [_P]),
+        "galop_server_open_run": (C.c_int, [_P, _F32P, _F32P, C.c_int64, C.c_int32, C.POINTER(C.c_int32)]),
+        "galop_server_close_run": (C.c_int, [_P, C.c_int32]),
+        "galop_server_submit": (C.c_int, [_P, C.c_int32, _U32P, _I64P, C.c_int64, _F32P, C.POINTER(C.c_int64)]),
+        "galop_server_wait": (C.c_int, [_P, C.c_int64, C.c_double, C.POINTER(RequestInfo)]),
+        "galop_server_stats": (C.c_int, [_P, C.POINTER(ServerTotals)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -404,3 +453,180 @@ def csr_from_dense(instructions: np.ndarray, lengths: np.ndarray, stride: int):
     idx = (np.repeat(np.arange(lengths.shape[0], dtype=np.int64) * stride, lengths)
            + (np.arange(offsets[-1], dtype=np.int64) - np.repeat(offsets[:-1], lengths)))
     return flat[idx], offsets
+
+
+class ResidentDataset:
+    """A dataset kept on the device (galop_dataset_create); usable by
+    several batches of the same evaluator."""
+
+    def __init__(self, evaluator: "Evaluator", dataset: Dataset):
+        self.evaluator = evaluator
+        self.dataset = dataset
+        self._h = C.c_void_p()
+        evaluator._check(evaluator._lib.galop_dataset_create(
+            evaluator.handle, _ptr(dataset.inputs, C.c_float), _ptr(dataset.targets, C.c_float), dataset.N,
+            dataset.num_inputs, C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.evaluator._lib.galop_dataset_device_bytes(self._h))
+
+    def close(self):
+        if self._h and self._h.value:
+            self.evaluator._lib.galop_dataset_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Several populations evaluated by one persistent launch per generation
+    (galop_batch_*).  ``specs``: (ResidentDataset, max_programs, max_words)."""
+
+    def __init__(self, evaluator: "Evaluator", specs):
+        self.evaluator = evaluator
+        self.specs = list(specs)
+        arr = (PopulationSpec * len(self.specs))()
+        for i, (ds, mp, mw) in enumerate(self.specs):
+            arr[i] = PopulationSpec(ds.handle.value, int(mp), int(mw))
+        self._h = C.c_void_p()
+        self._n = [0] * len(self.specs)
+        evaluator._check(evaluator._lib.galop_batch_create(evaluator.handle, arr, len(self.specs), C.byref(self._h)))
+
+    def _check(self, rc):
+        self.evaluator._check(rc)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.evaluator._lib.galop_batch_device_bytes(self._h))
+
+    def set_population(self, pop: int, words: np.ndarray, offsets: np.ndarray):
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        self._keep = getattr(self, "_keep", {})
+        self._keep[pop] = (words, offsets)      # host buffers must live until the copy is done
+        self._check(self.evaluator._lib.galop_batch_set_population(
+            self._h, pop, _ptr(words, C.c_uint32), _ptr(offsets, C.c_int64), offsets.shape[0] - 1))
+        self._n[pop] = offsets.shape[0] - 1
+
+    def evaluate(self, use_graph: bool = False):
+        self._check(self.evaluator._lib.galop_batch_evaluate(self._h, int(bool(use_graph))))
+
+    def synchronize(self):
+        self._check(self.evaluator._lib.galop_batch_synchronize(self._h))
+        self._keep = {}
+
+    def fitness(self, pop: int, with_sse: bool = False):
+        n = self._n[pop]
+        fit = np.empty(n, dtype=np.float32)
+        sse = np.empty(n, dtype=np.float64) if with_sse else None
+        self._check(self.evaluator._lib.galop_batch_get_fitness(self._h, pop, _ptr(fit, C.c_float),
+                                                                _ptr(sse, C.c_double)))
+        return (fit, sse) if with_sse else fit
+
+    @property
+    def stats(self) -> Stats:
+        s = Stats()
+        self._check(self.evaluator._lib.galop_batch_last_stats(self._h, C.byref(s)))
+        return s
+
+    def close(self):
+        if self._h and self._h.value:
+            self.evaluator._lib.galop_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching evaluation for many GP runs (galop_server_*).
+
+    ``open_run(dataset)`` registers a run; ``submit(run, words, offsets)``
+    queues one generation and returns a request id; ``wait(id)`` returns its
+    fitness and a RequestInfo (latency, batch size, ...)."""
+
+    def __init__(self, evaluator: "Evaluator", **options):
+        self.evaluator = evaluator
+        lib = evaluator._lib
+        o = ServerOptions()
+        lib.galop_server_options_init(C.byref(o))
+        for k, v in options.items():
+            setattr(o, k, v)
+        self.options = o
+        self._h = C.c_void_p()
+        evaluator._check(lib.galop_server_create(evaluator.handle, C.byref(o), C.byref(self._h)))
+        self._out = {}
+
+    def open_run(self, dataset: Dataset) -> int:
+        rid = C.c_int32()
+        self.evaluator._check(self.evaluator._lib.galop_server_open_run(
+            self._h, _ptr(dataset.inputs, C.c_float), _ptr(dataset.targets, C.c_float), dataset.N,
+            dataset.num_inputs, C.byref(rid)))
+        return rid.value
+
+    def close_run(self, run_id: int):
+        self.evaluator._check(self.evaluator._lib.galop_server_close_run(self._h, run_id))
+
+    def submit(self, run_id: int, words: np.ndarray, offsets: np.ndarray) -> int:
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        out = np.empty(offsets.shape[0] - 1, dtype=np.float32)
+        rq = C.c_int64()
+        rc = self.evaluator._lib.galop_server_submit(self._h, run_id, _ptr(words, C.c_uint32),
+                                                     _ptr(offsets, C.c_int64), offsets.shape[0] - 1,
+                                                     _ptr(out, C.c_float), C.byref(rq))
+        if rc != OK:
+            raise GalopError(rc, "galop_server_submit failed")
+        self._out[rq.value] = out
+        return rq.value
+
+    def wait(self, request_id: int, timeout: float = 0.0):
+        info = RequestInfo()
+        rc = self.evaluator._lib.galop_server_wait(self._h, request_id, timeout, C.byref(info))
+        if rc == E_TIMEOUT:
+            raise GalopError(rc, "timed out")
+        if rc != OK:
+            self._out.pop(request_id, None)
+            raise GalopError(rc, "request failed")
+        return self._out.pop(request_id), info
+
+    @property
+    def totals(self) -> ServerTotals:
+        t = ServerTotals()
+        self.evaluator._check(self.evaluator._lib.galop_server_stats(self._h, C.byref(t)))
+        return t
+
+    def close(self):
+        if self._h and self._h.value:
+            self.evaluator._lib.galop_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

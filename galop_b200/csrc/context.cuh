@@ -1,0 +1,109 @@
+// context.cuh -- the evaluator context shared by the C ABI's source files.
+#pragma once
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/galop_b200.h"
+#include "interp.cuh"
+
+namespace galop {
+
+// Reference constant pools (src/LGPConfig.h:159-168).
+inline const float kRefPool8[8] = {0.0f, 1.0f, -1.0f, 3.14159f, 0.5f, 2.0f, 10.0f, 100.0f};
+inline const float kRefPool16[16] = {0.0f, 1.0f, -1.0f, 3.14159f, 0.5f, 2.0f, 10.0f, 100.0f,
+                              0.1f, -0.5f, 0.25f, 5.0f, 20.0f, -2.0f, 0.01f, 1000.0f};
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t cap = 0;  // elements
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        size_t want = std::max<size_t>(n, cap + cap / 4);
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        if (e != cudaSuccess) { p = nullptr; return e; }
+        cap = want;
+        return cudaSuccess;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+enum Ev { kEvStart = 0, kEvH2D, kEvPrepass, kEvInterp, kEvFinalize, kEvD2H, kEvCount };
+
+}  // namespace galop
+
+using galop::DevBuf;
+using galop::kEvCount;
+using galop::ConstPool;
+using galop::IsaParams;
+
+struct galop_ctx {
+    galop_options opt{};
+    IsaParams isa{};
+    ConstPool pool{};
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[kEvCount] = {};
+    cudaEvent_t timers[8] = {};
+    std::string err;
+
+    // resident dataset (feature-major, padded)
+    DevBuf<float> X, y;
+    DevBuf<float> stage_aos, stage_y;
+    int64_t N = -1, Np = 0;
+    int num_inputs = 0;
+
+    // population buffers (high-water)
+    DevBuf<uint32_t> raw_words, uops, eff_raw;
+    DevBuf<uint8_t> raw_lens8;
+    DevBuf<int64_t> raw_off, eff_off, tiles;
+    DevBuf<int32_t> eff_len, order;
+    DevBuf<float> fitness, outputs, trace;
+    DevBuf<double> sse, partial;
+    DevBuf<unsigned long long> counters;   // [0] queue head, [1..2] totals
+    DevBuf<unsigned int> hist;
+    std::vector<int64_t> host_tmp;
+
+    galop_stats stats{};
+    int launches = 0;
+    bool stats_pending = false;   // device-path call whose timings are not read yet
+
+    int fail(int code, const char* fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        err = buf;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* what) {
+        cudaGetLastError();   // a non-sticky error must not resurface in a later call
+        return fail(e == cudaErrorMemoryAllocation ? GALOP_E_NOMEM : GALOP_E_CUDA,
+                    "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+    }
+};
+
+#define GALOP_CK(call, what)                                   \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return ctx->cuda_fail(_e, what); \
+    } while (0)
+
+
+namespace galop {
+// Interpreter configuration shared by the single-population and batched paths.
+int pick_k(const galop_ctx* ctx);
+int pick_wpb(const galop_ctx* ctx);
+const void* kernel_for(const galop_ctx* ctx, int k, int mode);
+const void* interp_kernel_nr8(int k, int dispatch, int profile, int reduce, int mode);
+const void* interp_kernel_nr16(int k, int dispatch, int profile, int reduce, int mode);
+}  // namespace galop

@@ -30,6 +30,22 @@ namespace galop {
 enum Reduce : int { kReduceKahan32 = 0, kReduceFp64 = 1, kReduceOrdered = 2 };
 enum Mode : int { kModeFitness = 0, kModeOutputs = 1, kModeTrace = 2 };
 
+// One population of a batched evaluation (galop_batch_*): its resident
+// dataset, case chunking and outputs.  Programs of all populations are
+// numbered globally; prog_base is this population's first.
+struct PopDesc {
+    const float* X;                // [num_inputs][Np]
+    const float* y;                // [Np]
+    int64_t N;
+    int64_t Np;
+    float* fitness;                // [n_programs of the population]
+    double* sse;                   // or null
+    int64_t prog_base;
+    int64_t chunk_cases;           // cases per work item (multiple of 1024)
+    int32_t n_chunks;              // work items per program
+    int32_t num_inputs;
+};
+
 struct InterpArgs {
     const uint32_t* uops;          // micro-ops, CSR by eff_off
     const int64_t* eff_off;        // [n_programs + 1]
@@ -50,6 +66,13 @@ struct InterpArgs {
     double* partial;               // [n_programs * n_chunks] (n_chunks > 1)
     float* outputs;                // kModeOutputs: [n_programs * N]
     float* trace;                  // kModeTrace: [(L+1) * NR][n_traced]
+    // Batched mode (pops != null, fitness mode, shared-memory kernel only):
+    // work item i is items[i] = global program << 20 | chunk, longest work
+    // first; partial sums of chunked programs go to partial[i].
+    const PopDesc* pops;
+    const int32_t* prog_pop;       // global program -> population
+    const unsigned long long* items;
+    int64_t n_items;
 };
 
 #define GALOP_CASES16(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) \
@@ -463,7 +486,8 @@ interp_smem_kernel(InterpArgs args) {
     for (int i = threadIdx.x; i < NR * RS; i += blockDim.x)
         reinterpret_cast<float*>(galop_smem4)[i] = args.consts.c[i / RS];
     __syncthreads();
-    const int64_t total_items = args.n_programs * (int64_t)args.n_chunks;
+    const bool batched = args.pops != nullptr;
+    const int64_t total_items = batched ? args.n_items : args.n_programs * (int64_t)args.n_chunks;
     constexpr int kPass = 32 * K;
 
     for (;;) {
@@ -472,15 +496,49 @@ interp_smem_kernel(InterpArgs args) {
         item = __shfl_sync(0xffffffffu, item, 0);
         if ((int64_t)item >= total_items) break;
 
-        const int64_t slot = (int64_t)item / args.n_chunks;
-        const int chunk = (int)((int64_t)item % args.n_chunks);
-        const int64_t prog = args.order ? (int64_t)args.order[slot] : slot;
+        // Resolve the work item: program, case range, dataset, output slot.
+        int64_t prog, cbeg, cend, N, Np, out_index, partial_index = -1;
+        int chunk, num_inputs;
+        const float* __restrict__ Xd;
+        const float* __restrict__ yd;
+        float* out_fitness;
+        double* out_sse;
+        if (batched) {
+            const unsigned long long it = args.items[item];
+            prog = (int64_t)(it >> 20);
+            chunk = (int)(it & 0xFFFFFull);
+            const PopDesc* d = args.pops + args.prog_pop[prog];
+            Xd = d->X;
+            yd = d->y;
+            N = d->N;
+            Np = d->Np;
+            num_inputs = d->num_inputs;
+            cbeg = (int64_t)chunk * d->chunk_cases;
+            cend = cbeg + d->chunk_cases;
+            out_fitness = d->fitness;
+            out_sse = d->sse;
+            out_index = prog - d->prog_base;
+            if (d->n_chunks > 1) partial_index = (int64_t)item;
+        } else {
+            const int64_t slot = (int64_t)item / args.n_chunks;
+            chunk = (int)((int64_t)item % args.n_chunks);
+            prog = args.order ? (int64_t)args.order[slot] : slot;
+            Xd = args.X;
+            yd = args.y;
+            N = args.N;
+            Np = args.Np;
+            num_inputs = args.num_inputs;
+            cbeg = (int64_t)chunk * args.chunk_cases;
+            cend = cbeg + args.chunk_cases;
+            out_fitness = args.fitness;
+            out_sse = args.sse;
+            out_index = prog;
+            if (args.n_chunks > 1) partial_index = prog * args.n_chunks + chunk;
+        }
+        if (cend > N) cend = N;
         const int64_t p0 = args.eff_off[prog];
         const int64_t L = args.eff_off[prog + 1] - p0;
         const uint32_t* __restrict__ pw = args.uops + p0;
-        const int64_t cbeg = (int64_t)chunk * args.chunk_cases;
-        int64_t cend = cbeg + args.chunk_cases;
-        if (cend > args.N) cend = args.N;
 
         float ks = 0.0f, kc = 0.0f;
         double acc = 0.0;
@@ -493,11 +551,11 @@ interp_smem_kernel(InterpArgs args) {
 #pragma unroll
             for (int f = 0; f < NR; ++f) {
                 float v[K];
-                if (f < args.num_inputs) {
+                if (f < num_inputs) {
 #pragma unroll
                     for (int q = 0; q < K / V; ++q) {
                         float w[V];
-                        load_cases<V>(args.X + (int64_t)f * args.Np + c0 + q * 32 * V, w);
+                        load_cases<V>(Xd + (int64_t)f * Np + c0 + q * 32 * V, w);
 #pragma unroll
                         for (int e = 0; e < V; ++e) v[q * V + e] = w[e];
                     }
@@ -553,14 +611,14 @@ interp_smem_kernel(InterpArgs args) {
 #pragma unroll
                     for (int e = 0; e < V; ++e) {
                         const int64_t c = base + (int64_t)(q * 32 + lane) * V + e;
-                        if (c < cend) args.outputs[prog * args.N + c] = o[q * V + e];
+                        if (c < cend) args.outputs[prog * N + c] = o[q * V + e];
                     }
             } else if constexpr (MODE == kModeFitness) {
                 float t[K];
 #pragma unroll
                 for (int q = 0; q < K / V; ++q) {
                     float w[V];
-                    load_cases<V>(args.y + c0 + q * 32 * V, w);
+                    load_cases<V>(yd + c0 + q * 32 * V, w);
 #pragma unroll
                     for (int e = 0; e < V; ++e) t[q * V + e] = w[e];
                 }
@@ -611,11 +669,11 @@ interp_smem_kernel(InterpArgs args) {
             else if constexpr (REDUCE == kReduceFp64) sse = warp_sum_f64(acc);
             else sse = acc;
             if (lane == 0) {
-                if (args.n_chunks == 1) {
-                    args.fitness[prog] = fitness_from_sse(sse, args.N);
-                    if (args.sse) args.sse[prog] = sse;
+                if (partial_index < 0) {
+                    out_fitness[out_index] = fitness_from_sse(sse, N);
+                    if (out_sse) out_sse[out_index] = sse;
                 } else {
-                    args.partial[prog * args.n_chunks + chunk] = sse;
+                    args.partial[partial_index] = sse;
                 }
             }
         }

@@ -202,6 +202,121 @@ GALOP_API int galop_device_free(galop_ctx* ctx, void* p);
 GALOP_API int galop_memcpy_h2d(galop_ctx* ctx, void* dst, const void* src, int64_t bytes);
 GALOP_API int galop_memcpy_d2h(galop_ctx* ctx, void* dst, const void* src, int64_t bytes);
 
+/* ---- resident datasets and batched populations ---------------------------- */
+
+/* A dataset uploaded once and kept on the device (feature-major, padded). */
+typedef struct galop_dataset galop_dataset;
+GALOP_API int galop_dataset_create(galop_ctx* ctx, const float* inputs, const float* targets,
+                                   int64_t n_cases, int32_t num_inputs, galop_dataset** out);
+GALOP_API int galop_dataset_destroy(galop_dataset* ds);
+GALOP_API int64_t galop_dataset_device_bytes(const galop_dataset* ds);
+
+/* A fixed set of populations evaluated together, one generation per
+ * galop_batch_evaluate: one persistent interpreter launch pulls (program,
+ * case chunk) items of every population from a device queue, largest work
+ * (effective length x cases) first.  Each population has its own dataset and
+ * capacities (programs, total instructions); all device memory is allocated
+ * at creation.  Case chunking depends only on a population's own case count,
+ * so its fitness does not depend on which batch it is evaluated in.  Each
+ * batch has its own stream; different batches run concurrently.
+ * Generalises CudaEvaluator::evaluate_population (src/EvaluatorCuda.cu:298-469)
+ * from one population to many; no single reference counterpart. */
+typedef struct galop_batch galop_batch;
+typedef struct {
+    const galop_dataset* dataset;
+    int64_t max_programs;
+    int64_t max_words;
+} galop_population_spec;
+
+GALOP_API int galop_batch_create(galop_ctx* ctx, const galop_population_spec* pops, int32_t n_pops,
+                                 galop_batch** out);
+GALOP_API int galop_batch_destroy(galop_batch* b);
+GALOP_API int64_t galop_batch_device_bytes(const galop_batch* b);
+/* Host CSR programs of population `pop` for the next evaluation (H2D on the
+ * batch's stream; pinned host memory makes it asynchronous). */
+GALOP_API int galop_batch_set_population(galop_batch* b, int32_t pop, const uint32_t* words,
+                                         const int64_t* offsets, int64_t n_programs);
+/* Queue one generation on the batch's stream.  use_graph != 0: the device
+ * work is captured as a CUDA graph the first time (and again whenever a
+ * population's program count changes) and replayed afterwards. */
+GALOP_API int galop_batch_evaluate(galop_batch* b, int32_t use_graph);
+GALOP_API int galop_batch_synchronize(galop_batch* b);
+/* D2H of one population's fitness (and SSE, may be NULL); waits. */
+GALOP_API int galop_batch_get_fitness(galop_batch* b, int32_t pop, float* fitness_out, double* sse_out);
+GALOP_API int galop_batch_last_stats(galop_batch* b, galop_stats* out);
+/* The batch's cudaStream_t. */
+GALOP_API void* galop_batch_stream(galop_batch* b);
+
+/* Pooled batch: capacities are totals shared by whatever populations are
+ * appended for the next evaluation (up to max_pops populations, max_programs
+ * programs, max_words instructions, max_items work items -- a program has
+ * ceil(cases / 16384) items, 1 in ORDERED mode).  All memory is allocated
+ * here; galop_batch_clear + galop_batch_append recompose it every
+ * generation without allocating.  append returns GALOP_E_CAPACITY when the
+ * population does not fit. */
+GALOP_API int galop_batch_create_pool(galop_ctx* ctx, int32_t max_pops, int64_t max_programs,
+                                      int64_t max_words, int64_t max_items, galop_batch** out);
+GALOP_API int galop_batch_clear(galop_batch* b);
+GALOP_API int galop_batch_append(galop_batch* b, const galop_dataset* ds, const uint32_t* words,
+                                 const int64_t* offsets, int64_t n_programs, int32_t* pop_out);
+/* Interpreted (effective) instructions of population `pop` in the last
+ * evaluation, summed over its programs; waits. */
+GALOP_API int galop_batch_population_work(galop_batch* b, int32_t pop, int64_t* eff_instructions);
+
+/* ---- serving: continuous batching for many independent GP runs ------------ */
+
+/* A server owns a worker thread that admits submitted generations by HBM
+ * footprint, packs them into pooled batches (one persistent launch each,
+ * several batches in flight on their own streams) and completes them into
+ * the callers' fitness buffers.  A run's dataset is uploaded when its first
+ * request is admitted and stays resident while the run has work; datasets
+ * of idle runs are evicted when the budget is needed.  A request's fitness
+ * does not depend on what it was batched with. */
+typedef struct galop_server galop_server;
+typedef struct {
+    int64_t hbm_budget_bytes;     /* resident datasets + slot buffers (default 150e9) */
+    int32_t slots;                /* batches in flight (default 2) */
+    int32_t max_pops_per_batch;   /* requests per batch (default 64) */
+    int64_t slot_programs;        /* per-batch capacities (defaults 2^20, 2^27, 2^23) */
+    int64_t slot_words;
+    int64_t slot_items;
+} galop_server_options;
+
+typedef struct {
+    int32_t status;               /* GALOP_OK, or the error that ended the request */
+    int32_t batch_requests;       /* requests in its batch */
+    int64_t eff_instructions;     /* interpreted instructions of its programs */
+    double queued_ms;             /* submit -> launch */
+    double latency_ms;            /* submit -> fitness in the caller's buffer */
+    double device_ms;             /* device time of its batch */
+} galop_request_info;
+
+typedef struct {
+    int64_t completed, batches, pending;
+    int64_t resident_bytes;       /* datasets + slot buffers on the device */
+    int64_t case_ops;             /* sum over completed requests: eff. instructions x cases */
+    double device_ms;
+} galop_server_totals;
+
+GALOP_API int galop_server_options_init(galop_server_options* opt);
+GALOP_API int galop_server_create(galop_ctx* ctx, const galop_server_options* opt, galop_server** out);
+/* Finishes queued work, then stops the worker and frees everything. */
+GALOP_API int galop_server_destroy(galop_server* sv);
+/* Registers a GP run; the dataset is copied (host) at this call. */
+GALOP_API int galop_server_open_run(galop_server* sv, const float* inputs, const float* targets,
+                                    int64_t n_cases, int32_t num_inputs, int32_t* run_id);
+GALOP_API int galop_server_close_run(galop_server* sv, int32_t run_id);
+/* One generation of a run: programs are copied at this call; fitness_out
+ * (n_programs floats) must stay valid until galop_server_wait returns. */
+GALOP_API int galop_server_submit(galop_server* sv, int32_t run_id, const uint32_t* words,
+                                  const int64_t* offsets, int64_t n_programs, float* fitness_out,
+                                  int64_t* request_id);
+/* Waits for a request (timeout_s <= 0: no limit); GALOP_E_TIMEOUT if it is
+ * not done in time (it stays queued and can be waited on again). */
+GALOP_API int galop_server_wait(galop_server* sv, int64_t request_id, double timeout_s,
+                                galop_request_info* info);
+GALOP_API int galop_server_stats(galop_server* sv, galop_server_totals* out);
+
 /* ---- evaluation without allocation --------------------------------------- */
 
 /* Limits of galop_evaluate_csr_noalloc: programs and total instructions per

@@ -1,0 +1,105 @@
+"""Batched evaluation (galop_batch_*): many populations, each with its own
+resident dataset, in one persistent launch per generation."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import galop_b200 as g
+from galop_b200 import workloads as W
+from conftest import bits
+
+pytestmark = pytest.mark.gpu
+
+
+def _populations(seed, specs, nr=16):
+    """specs: list of (n_programs, n_cases, n_features, len_lo, len_hi)."""
+    rng = np.random.default_rng(seed)
+    isa = W.IsaSpec(g.PROFILE_REF, nr)
+    out = []
+    for n, N, k, lo, hi in specs:
+        X = rng.uniform(-2, 2, (N, k)).astype(np.float32)
+        y = rng.uniform(-1, 1, N).astype(np.float32)
+        words, off = W.structured_population(rng, W.uniform_lengths(rng, n, lo, hi), isa, 0.6)
+        out.append((g.Dataset(X, y), words, off))
+    return out
+
+
+SPECS = [(700, 1000, 3, 4, 60), (50, 40000, 5, 8, 120), (1500, 33, 1, 2, 30), (3, 70000, 2, 10, 40),
+         (0, 100, 1, 1, 1), (900, 4096, 8, 16, 200)]
+
+
+@pytest.mark.parametrize("reduce", [g.REDUCE_KAHAN32, g.REDUCE_ORDERED])
+def test_batch_matches_single_population_calls(native, reduce):
+    pops = _populations(1, SPECS)
+    with g.Evaluator(num_registers=16, reduce=reduce) as ev:
+        single = [ev.evaluate_csr(w, o, ds) if o.shape[0] > 1 else np.zeros(0, np.float32) for ds, w, o in pops]
+        rds = [g.ResidentDataset(ev, ds) for ds, _, _ in pops]
+        with g.Batch(ev, [(r, max(o.shape[0] - 1, 1), max(int(o[-1]), 1)) for r, (_, _, o) in zip(rds, pops)]) as b:
+            for p, (_, w, o) in enumerate(pops):
+                b.set_population(p, w, o)
+            b.evaluate()
+            b.synchronize()
+            got = [b.fitness(p) for p in range(len(pops))]
+            st = b.stats
+    assert st.eff_instructions < st.raw_instructions
+    for p, (a, want) in enumerate(zip(got, single)):
+        if reduce == g.REDUCE_ORDERED:
+            assert np.array_equal(bits(a), bits(want)), p
+        else:
+            rel = np.abs(a.astype(np.float64) - want) / np.maximum(np.abs(want.astype(np.float64)), 1e-30)
+            assert rel.size == 0 or rel.max() <= 1e-6, p
+
+
+def test_population_fitness_is_identical_alone_and_in_a_mix(native):
+    """Case chunking depends on a population's own case count only, so its
+    fitness does not depend on what else is batched with it."""
+    pops = _populations(2, SPECS)
+    with g.Evaluator(num_registers=16) as ev:
+        rds = [g.ResidentDataset(ev, ds) for ds, _, _ in pops]
+        caps = [(r, max(o.shape[0] - 1, 1), max(int(o[-1]), 1)) for r, (_, _, o) in zip(rds, pops)]
+        with g.Batch(ev, caps) as mix:
+            for p, (_, w, o) in enumerate(pops):
+                mix.set_population(p, w, o)
+            mix.evaluate()
+            mixed = [mix.fitness(p) for p in range(len(pops))]
+        for p, (_, w, o) in enumerate(pops):
+            with g.Batch(ev, [caps[p]]) as alone:
+                alone.set_population(0, w, o)
+                alone.evaluate()
+                assert np.array_equal(bits(alone.fitness(0)), bits(mixed[p])), p
+
+
+def test_graph_replay_across_generations(native):
+    """A captured generation replays with new program contents (same counts)
+    and gives the same fitness as an uncaptured evaluation."""
+    rng = np.random.default_rng(3)
+    pops = _populations(3, SPECS[:3])
+    isa = W.IsaSpec(g.PROFILE_REF, 16)
+    with g.Evaluator(num_registers=16) as ev:
+        rds = [g.ResidentDataset(ev, ds) for ds, _, _ in pops]
+        caps = [(r, o.shape[0] - 1, 2 * int(o[-1]) + 1000) for r, (_, _, o) in zip(rds, pops)]
+        with g.Batch(ev, caps) as bg, g.Batch(ev, caps) as bp:
+            for gen in range(3):
+                gens = []
+                for p, (_, _, o) in enumerate(pops):
+                    n = o.shape[0] - 1
+                    lens = W.uniform_lengths(rng, n, 1, 2 * int(o[-1]) // max(n, 1))
+                    w, off = W.structured_population(rng, lens, isa, 0.5)
+                    bg.set_population(p, w, off)
+                    bp.set_population(p, w, off)
+                bg.evaluate(use_graph=True)
+                bp.evaluate(use_graph=False)
+                for p in range(len(pops)):
+                    assert np.array_equal(bits(bg.fitness(p)), bits(bp.fitness(p))), (gen, p)
+
+
+def test_batch_capacity_is_enforced(native):
+    pops = _populations(4, SPECS[:1])
+    ds, w, o = pops[0]
+    with g.Evaluator(num_registers=16) as ev:
+        r = g.ResidentDataset(ev, ds)
+        with g.Batch(ev, [(r, 10, 100)]) as b:
+            with pytest.raises(g.GalopError) as e:
+                b.set_population(0, w, o)
+            assert e.value.status == g.E_CAPACITY
