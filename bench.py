@@ -26,6 +26,7 @@ the same workload.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -60,6 +61,12 @@ def parse():
     ap.add_argument("--reduce", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "stream"],
+                    help="single: the headline single-generation workload; batch: many populations in one "
+                         "persistent launch per generation (graph replay) vs one plain launch per population; "
+                         "serve: continuous batching of Poisson-arriving GP runs; stream: 2^20-case dataset")
+    ap.add_argument("--scale", type=float, default=1.0 / 32,
+                    help="population-size scale of the batch/serve/stream workloads")
     return ap.parse_args()
 
 
@@ -379,12 +386,184 @@ def run_b200(args, dist: Dist):
     ev.close()
 
 
+def run_batch(args):
+    """Many populations of uneven sizes and lengths on one shared dataset,
+    one persistent launch per generation replayed from a CUDA graph; the
+    plain form (one launch per population, no intron pass) timed beside it,
+    and the compensated-FP32 fitness compared with the FP64 case-order sum."""
+    import galop_b200 as g
+    from galop_b200 import workloads as W
+    n_cases = args.cases if args.cases != 4096 else 1 << 16
+    lo, hi = max(8, int(1000 * args.scale)), max(64, int((1 << 20) * args.scale))
+    isa, X, y, pops = W.many_populations(n_cases=n_cases, size_lo=lo, size_hi=hi)
+    ds = g.Dataset(X, y)
+    ev = g.Evaluator(num_registers=16)
+    rd = g.ResidentDataset(ev, ds)
+    caps = [(rd, o.shape[0] - 1, int(o[-1])) for _, o in pops]
+    b = g.Batch(ev, caps)
+
+    def generation(use_graph):
+        for p_, (w, o) in enumerate(pops):
+            b.set_population(p_, w, o)
+        b.evaluate(use_graph=use_graph)
+        b.synchronize()
+        return b.stats
+
+    for _ in range(args.warmup):
+        generation(True)
+    dev_ms, wall = [], time.perf_counter()
+    for _ in range(args.steps):
+        dev_ms.append(generation(True).total_ms)
+    wall = (time.perf_counter() - wall) * 1e3 / args.steps
+    st = b.stats
+    eff_total = 0
+    for p_ in range(len(pops)):
+        e = ctypes.c_int64()
+        ev._check(ev._lib.galop_batch_population_work(b._h, p_, ctypes.byref(e)))
+        eff_total += e.value
+    ops = float(eff_total) * n_cases
+    batched = ops / (np.mean(dev_ms) / 1e3) / 1e9
+    fit_k = [b.fitness(p_) for p_ in range(len(pops))]
+    b.close()
+    # FP64 case-order reference of the same outputs
+    ev_o = g.Evaluator(num_registers=16, reduce=g.REDUCE_ORDERED)
+    rd_o = g.ResidentDataset(ev_o, ds)
+    bo = g.Batch(ev_o, [(rd_o, c[1], c[2]) for c in caps])
+    for p_, (w, o) in enumerate(pops):
+        bo.set_population(p_, w, o)
+    bo.evaluate()
+    bo.synchronize()
+    fit_o = [bo.fitness(p_) for p_ in range(len(pops))]
+    bo.close()
+    ev_o.close()
+    fk = np.concatenate(fit_k).astype(np.float64)
+    fo = np.concatenate(fit_o).astype(np.float64)
+    nz = fo > 0
+    rel = float(np.max(np.abs(fk[nz] - fo[nz]) / fo[nz])) if nz.any() else 0.0
+    # plain: one launch per population, raw programs (no intron pass), per generation
+    ev_p = g.Evaluator(num_registers=16, intron_prepass=False)
+    ev_p.set_dataset(ds)
+    plain_ms = 0.0
+    for w, o in pops:
+        ev_p.evaluate_csr(w, o)
+        plain_ms += ev_p.stats.prepass_ms + ev_p.stats.interp_ms + ev_p.stats.finalize_ms
+    ev_p.close()
+    plain = ops / (plain_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": batched, "unit": UNIT, "workload": "batch", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(dev_ms)),
+        "wall_ms_per_generation": wall, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"{len(pops)} populations, sizes log-uniform [{lo},{hi}] (x{args.scale:g} of "
+                               f"[1000, 2^20]), lengths log-uniform [8,2048], one shared dataset of {n_cases} cases "
+                               "x 4 features N(0,10^2), targets ~1e4 + N(0,1); generations replayed from a CUDA graph",
+                   "programs": int(sum(c[1] for c in caps)), "raw_instructions": int(sum(c[2] for c in caps)),
+                   "effective_instructions": int(eff_total)},
+        "plain_per_population_gpops": plain, "speedup_vs_plain": batched / plain,
+        "fitness_rel_err_kahan32_vs_fp64_case_order": rel,
+        "kernels_per_generation": st.kernels_launched,
+    }
+    rd.close()
+    ev.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """256 independent GP runs arriving as a Poisson process (mean 2 ms),
+    each with its own dataset; every run submits its generations one after
+    the other through the continuous-batching server."""
+    import threading
+    import galop_b200 as g
+    from galop_b200 import workloads as W
+    cases_hi = max(1024, int((1 << 20) * args.scale * 2))
+    pop_hi = max(1024, int((1 << 18) * args.scale * 2))
+    isa, runs = W.serving_runs(n_runs=256, cases_hi=cases_hi, pop_hi=pop_hi, generations=3)
+    ev = g.Evaluator(num_registers=16)
+    sv = g.Server(ev, hbm_budget_bytes=int(150e9), slots=2, slot_programs=1 << 20, slot_words=1 << 27,
+                  slot_items=1 << 23)
+    rng = np.random.default_rng(9)
+    arrivals = np.cumsum(rng.exponential(2e-3, size=len(runs)))
+    lat, queued, sizes = [], [], []
+    lock = threading.Lock()
+    t0 = time.perf_counter()
+
+    def client(i):
+        X, y, gens = runs[i]
+        delay = t0 + arrivals[i] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        rid = sv.open_run(g.Dataset(X, y))
+        for w, o in gens:
+            rq = sv.submit(rid, w, o)
+            _, info = sv.wait(rq)
+            with lock:
+                lat.append(info.latency_ms)
+                queued.append(info.queued_ms)
+                sizes.append(info.batch_requests)
+        sv.close_run(rid)
+
+    threads = [threading.Thread(target=client, args=(i,)) for i in range(len(runs))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    wall = time.perf_counter() - t0
+    tot = sv.totals
+    sv.close()
+    ev.close()
+    line = {
+        "metric": METRIC, "value": tot.case_ops / wall / 1e9, "unit": UNIT, "workload": "serve",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "mean": float(np.mean(lat))},
+        "queued_ms": {"p50": float(np.percentile(queued, 50)), "p99": float(np.percentile(queued, 99))},
+        "requests": len(lat), "batches": int(tot.batches), "mean_batch_requests": float(np.mean(sizes)),
+        "device_busy_frac": tot.device_ms / 1e3 / wall, "wall_s": wall,
+        "config": {"workload": f"256 GP runs, Poisson arrivals (mean 2 ms), 3 generations each; cases "
+                               f"log-uniform [256,{cases_hi}], 1-8 features; populations log-uniform "
+                               f"[1000,{pop_hi}], lengths U[8,512]; HBM admission cap 150 GB; 2 batches in flight"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_stream(args):
+    """2^20 fitness cases x 8 features (32 MiB + 4 MiB resident), programs
+    log-uniform [32,1024], the intron pre-pass on; a sample of the 2^22
+    programs."""
+    import galop_b200 as g
+    from galop_b200 import workloads as W
+    n = max(1024, int((1 << 22) * args.scale / 8))
+    wl = W.hbm_streaming(n_programs=n, n_cases=1 << 20)
+    ev = g.Evaluator(num_registers=16)
+    ev.set_dataset(g.Dataset(wl.X, wl.y))
+    for _ in range(args.warmup):
+        ev.evaluate_csr(wl.words, wl.offsets)
+    ms = []
+    for _ in range(args.steps):
+        ev.evaluate_csr(wl.words, wl.offsets)
+        ms.append(ev.stats.interp_ms + ev.stats.prepass_ms + ev.stats.finalize_ms)
+    st = ev.stats
+    ev.close()
+    ops = float(st.eff_instructions) * wl.n_cases
+    line = {"metric": METRIC, "value": ops / (np.mean(ms) / 1e3) / 1e9, "unit": UNIT, "workload": "stream",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(ms)),
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": wl.description, "programs": n, "raw_instructions": st.raw_instructions,
+                       "effective_instructions": st.eff_instructions, "case_chunks": st.case_chunks}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     dist = Dist()
     try:
         if args.impl == "reference":
             run_reference(args, dist)
+        elif args.workload == "batch":
+            run_batch(args)
+        elif args.workload == "serve":
+            run_serve(args)
+        elif args.workload == "stream":
+            run_stream(args)
         else:
             run_b200(args, dist)
     finally:

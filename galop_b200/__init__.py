@@ -20,6 +20,7 @@ library must be present: there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass, field
 from pathlib import Path
 from typing import Optional, Sequence
@@ -268,10 +269,19 @@ class Evaluator:
             raise GalopError(rc, f"galop_create failed: {status_string(rc)}")
         self._dataset_key = None
         self.dataset: Optional[Dataset] = None
+        self._children = weakref.WeakSet()
 
     # -- lifetime -------------------------------------------------------------
+    def _adopt(self, child):
+        self._children.add(child)
+
     def close(self):
         if getattr(self, "_ctx", None) and self._ctx.value:
+            # servers first (their workers use batches and datasets), then batches, then datasets
+            for kind in (Server, Batch, ResidentDataset):
+                for child in list(self._children):
+                    if isinstance(child, kind):
+                        child.close()
             self._lib.galop_destroy(self._ctx)
             self._ctx = C.c_void_p()
 
@@ -463,6 +473,7 @@ class ResidentDataset:
         self.evaluator = evaluator
         self.dataset = dataset
         self._h = C.c_void_p()
+        evaluator._adopt(self)
         evaluator._check(evaluator._lib.galop_dataset_create(
             evaluator.handle, _ptr(dataset.inputs, C.c_float), _ptr(dataset.targets, C.c_float), dataset.N,
             dataset.num_inputs, C.byref(self._h)))
@@ -498,6 +509,7 @@ class Batch:
         for i, (ds, mp, mw) in enumerate(self.specs):
             arr[i] = PopulationSpec(ds.handle.value, int(mp), int(mw))
         self._h = C.c_void_p()
+        evaluator._adopt(self)
         self._n = [0] * len(self.specs)
         evaluator._check(evaluator._lib.galop_batch_create(evaluator.handle, arr, len(self.specs), C.byref(self._h)))
 
@@ -572,6 +584,7 @@ class Server:
             setattr(o, k, v)
         self.options = o
         self._h = C.c_void_p()
+        evaluator._adopt(self)
         evaluator._check(lib.galop_server_create(evaluator.handle, C.byref(o), C.byref(self._h)))
         self._out = {}
 

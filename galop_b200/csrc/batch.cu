@@ -40,6 +40,7 @@ int64_t chunks_for(int64_t n_cases) {
 
 struct galop_dataset {
     galop_ctx* ctx = nullptr;
+    int device = 0;                 // kept so destruction never reads the context
     DevBuf<float> X, y;
     int64_t N = 0, Np = 0;
     int32_t k = 0;
@@ -55,6 +56,7 @@ struct BatchPop {
 
 struct galop_batch {
     galop_ctx* ctx = nullptr;
+    int device = 0;                 // kept so destruction never reads the context
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     std::vector<BatchPop> pops;
@@ -226,8 +228,10 @@ int galop_dataset_create(galop_ctx* ctx, const float* inputs, const float* targe
     if (n_cases > 0 && (!targets || (num_inputs > 0 && !inputs)))
         return ctx->fail(GALOP_E_INVALID, "null dataset pointer");
     GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    cudaGetLastError();   // a stale error of an earlier call must not be reported as ours
     galop_dataset* ds = new galop_dataset();
     ds->ctx = ctx;
+    ds->device = ctx->device;
     ds->N = n_cases;
     ds->k = num_inputs;
     ds->Np = std::max<int64_t>(1024, (n_cases + 1023) / 1024 * 1024);
@@ -261,7 +265,7 @@ int galop_dataset_create(galop_ctx* ctx, const float* inputs, const float* targe
 
 int galop_dataset_destroy(galop_dataset* ds) {
     if (!ds) return GALOP_OK;
-    cudaSetDevice(ds->ctx->device);
+    cudaSetDevice(ds->device);
     ds->X.release();
     ds->y.release();
     delete ds;
@@ -342,6 +346,7 @@ int galop_batch_create(galop_ctx* ctx, const galop_population_spec* specs, int32
     GALOP_CK(cudaSetDevice(ctx->device), "set device");
     galop_batch* b = new galop_batch();
     b->ctx = ctx;
+    b->device = ctx->device;
     b->pops.resize(n_pops);
     int64_t words = 0, offs = 0, progs = 0, items = 0;
     for (int p = 0; p < n_pops; ++p) {
@@ -374,6 +379,7 @@ int galop_batch_create_pool(galop_ctx* ctx, int32_t max_pops, int64_t max_progra
     GALOP_CK(cudaSetDevice(ctx->device), "set device");
     galop_batch* b = new galop_batch();
     b->ctx = ctx;
+    b->device = ctx->device;
     b->pooled = true;
     b->max_pops = max_pops;
     if (int rc = allocate(b, max_words, max_programs + max_pops, max_programs, max_items, max_pops)) {
@@ -428,7 +434,7 @@ int galop_batch_append(galop_batch* b, const galop_dataset* ds, const uint32_t* 
 
 int galop_batch_destroy(galop_batch* b) {
     if (!b) return GALOP_OK;
-    cudaSetDevice(b->ctx->device);
+    cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graph(b);
     b->arena.release(); b->uops.release(); b->local_off.release(); b->starts.release();
@@ -484,6 +490,7 @@ int galop_batch_evaluate(galop_batch* b, int32_t use_graph) {
     if (!b) return GALOP_E_INVALID;
     galop_ctx* ctx = b->ctx;
     GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    cudaGetLastError();   // a stale error of an earlier call must not be reported as ours
     bool same = b->planned_n.size() == b->pops.size();
     for (size_t p = 0; same && p < b->pops.size(); ++p) same = b->planned_n[p] == b->pops[p].n;
     if (!same) {

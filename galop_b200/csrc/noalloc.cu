@@ -95,6 +95,7 @@ extern "C" int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32
 
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return GALOP_E_NO_DEVICE; }
+    cudaGetLastError();   // a stale error of an earlier call must not be reported as ours
     NoAllocScratch* sc = nullptr;
     if (scratch_for_device(device, &sc) != cudaSuccess) { cudaGetLastError(); return GALOP_E_CUDA; }
     int sm_count = 0;

@@ -202,6 +202,7 @@ int check_ready(galop_ctx* ctx) {
 }
 
 void begin_call(galop_ctx* ctx, int64_t n) {
+    cudaGetLastError();   // a stale error of an earlier call must not be reported as ours
     ctx->stats_pending = false;
     ctx->stats = galop_stats{};
     ctx->stats.n_programs = n;
@@ -439,6 +440,7 @@ int galop_memcpy_d2h(galop_ctx* ctx, void* dst, const void* src, int64_t bytes) 
 
 static int set_dataset_common(galop_ctx* ctx, const float* src_aos, const float* src_y,
                               int64_t n_cases, int32_t num_inputs) {
+    cudaGetLastError();   // a stale error of an earlier call must not be reported as ours
     const int64_t np = std::max<int64_t>(1024, (n_cases + 1023) / 1024 * 1024);
     GALOP_CK(ctx->X.ensure((size_t)(np * std::max(num_inputs, 1))), "alloc dataset X");
     GALOP_CK(ctx->y.ensure((size_t)np), "alloc dataset y");

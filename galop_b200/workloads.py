@@ -255,7 +255,7 @@ def regression_target(rng, X: np.ndarray, isa: IsaSpec, n_eff: int, noise_sigma:
             break
     y = y.astype(np.float64)
     if scale != 1.0:
-        y = y / max(float(np.std(y)), 1e-12) * scale
+        y = (y - float(np.mean(y))) / max(float(np.std(y)), 1e-12) * scale
     if noise_sigma:
         y = y + rng.normal(0.0, noise_sigma, size=y.shape)
     return y.astype(np.float32), prog
@@ -338,3 +338,45 @@ def plain_cpu(seed: int = 0, n_programs: int = 1000, n_cases: int = 64) -> Workl
     lens = uniform_lengths(rng, n_programs, 8, 64)
     words, off = structured_population(rng, lens, isa, 0.5, reg_limit=9, const_limit=4)
     return Workload("plain_cpu", isa, words, off, X, y, tp, "1000 programs, L~U[8,64], 64 cases, BJ ops")
+
+
+def many_populations(seed: int = 4, n_pops: int = 64, size_lo: int = 1000, size_hi: int = 1 << 20,
+                     len_lo: int = 8, len_hi: int = 2048, n_cases: int = 1 << 22, num_inputs: int = 4,
+                     x_sigma: float = 10.0, target_scale: float = 1e4, noise: float = 1.0, target_eff: int = 16):
+    """Batched populations on one shared dataset: population sizes and program
+    lengths log-uniform, 4 features N(0, x_sigma^2) (sigma 10 reads "N(0,100)"
+    as a variance), targets a random program rescaled to ~1e4 plus N(0, 1)
+    noise.  Returns (isa, X, y, [(words, offsets)] per population)."""
+    rng = np.random.default_rng(seed)
+    isa = IsaSpec(PROFILE_REF, 16)
+    X = (rng.standard_normal((n_cases, num_inputs)) * x_sigma).astype(np.float32)
+    y, _ = regression_target(rng, X, isa, target_eff, noise, scale=target_scale)
+    pops = []
+    for _ in range(n_pops):
+        n = int(log_uniform_lengths(rng, 1, size_lo, size_hi)[0])
+        lens = log_uniform_lengths(rng, n, len_lo, len_hi)
+        pops.append(random_population(rng, lens, isa.num_registers))
+    return isa, X, y, pops
+
+
+def serving_runs(seed: int = 5, n_runs: int = 256, cases_lo: int = 256, cases_hi: int = 1 << 20,
+                 pop_lo: int = 1000, pop_hi: int = 1 << 18, len_lo: int = 8, len_hi: int = 512,
+                 generations: int = 1):
+    """Independent GP runs for the serving loop: each has its own seeded
+    dataset (cases log-uniform, 1-8 features U[-1,1], target a random
+    program) and `generations` populations (size log-uniform, lengths
+    U[len_lo, len_hi], uniform random words)."""
+    rng = np.random.default_rng(seed)
+    isa = IsaSpec(PROFILE_REF, 16)
+    runs = []
+    for _ in range(n_runs):
+        N = int(log_uniform_lengths(rng, 1, cases_lo, cases_hi)[0])
+        k = int(rng.integers(1, 9))
+        X = rng.uniform(-1.0, 1.0, (N, k)).astype(np.float32)
+        y, _ = regression_target(rng, X, isa, 12)
+        gens = []
+        for _g in range(generations):
+            n = int(log_uniform_lengths(rng, 1, pop_lo, pop_hi)[0])
+            gens.append(random_population(rng, uniform_lengths(rng, n, len_lo, len_hi), isa.num_registers))
+        runs.append((X, y, gens))
+    return isa, runs

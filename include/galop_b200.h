@@ -204,7 +204,8 @@ GALOP_API int galop_memcpy_d2h(galop_ctx* ctx, void* dst, const void* src, int64
 
 /* ---- resident datasets and batched populations ---------------------------- */
 
-/* A dataset uploaded once and kept on the device (feature-major, padded). */
+/* A dataset uploaded once and kept on the device (feature-major, padded).
+ * Destroy datasets, batches and servers before the context they came from. */
 typedef struct galop_dataset galop_dataset;
 GALOP_API int galop_dataset_create(galop_ctx* ctx, const float* inputs, const float* targets,
                                    int64_t n_cases, int32_t num_inputs, galop_dataset** out);
