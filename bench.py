@@ -440,6 +440,7 @@ def run_batch(args):
     fo = np.concatenate(fit_o).astype(np.float64)
     nz = fo > 0
     rel = float(np.max(np.abs(fk[nz] - fo[nz]) / fo[nz])) if nz.any() else 0.0
+    zero_mismatch = int(np.sum((fo > 0) != (fk > 0)))
     # plain: one launch per population, raw programs (no intron pass), per generation
     ev_p = g.Evaluator(num_registers=16, intron_prepass=False)
     ev_p.set_dataset(ds)
@@ -460,6 +461,7 @@ def run_batch(args):
                    "effective_instructions": int(eff_total)},
         "plain_per_population_gpops": plain, "speedup_vs_plain": batched / plain,
         "fitness_rel_err_kahan32_vs_fp64_case_order": rel,
+        "fitness_zero_mismatches": zero_mismatch,
         "kernels_per_generation": st.kernels_launched,
     }
     rd.close()

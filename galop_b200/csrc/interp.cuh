@@ -249,6 +249,12 @@ __device__ __forceinline__ void step_brx(float (&r)[NR][K], uint32_t u, const Co
     }
 }
 
+// KAHAN32 keeps squared errors in FP32 only while |error| <= 2^52: a square
+// is then <= 2^104 and a lane's compensated sum of up to 2^20 of them stays
+// finite.  Larger (or non-finite) errors are squared and summed in FP64, so
+// the FP32 path never overflows where the CPU's double sum would not.
+constexpr float kKahanMaxError = 4503599627370496.0f;   // 2^52
+
 __device__ __forceinline__ double warp_sum_f64(double v) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -287,6 +293,7 @@ interp_kernel(InterpArgs args) {
         if (cend > args.N) cend = args.N;
 
         float ks = 0.0f, kc = 0.0f;   // Kahan sum / compensation (KAHAN32)
+        double big = 0.0;             // KAHAN32: squares of errors beyond kKahanMaxError
         double acc = 0.0;             // FP64 / ORDERED accumulator
 
         for (int64_t base = cbeg; base < cend; base += kPass) {
@@ -342,7 +349,10 @@ interp_kernel(InterpArgs args) {
 #pragma unroll
                     for (int k = 0; k < K; ++k) {
                         const float e = __fsub_rn(o[k], t[k]);
-                        const float q = (c0 + k < cend) ? __fmul_rn(e, e) : 0.0f;
+                        const bool valid = c0 + k < cend;
+                        const bool huge = !(fabsf(e) <= kKahanMaxError);
+                        const float q = (valid && !huge) ? __fmul_rn(e, e) : 0.0f;
+                        if (valid && huge) big = __dadd_rn(big, __dmul_rn((double)e, (double)e));
                         const float yk = __fsub_rn(q, kc);
                         const float tt = __fadd_rn(ks, yk);
                         kc = __fsub_rn(__fsub_rn(tt, ks), yk);
@@ -377,7 +387,7 @@ interp_kernel(InterpArgs args) {
         if constexpr (MODE == kModeFitness) {
             double sse;
             if constexpr (REDUCE == kReduceKahan32) {
-                sse = warp_sum_f64((double)ks - (double)kc);
+                sse = warp_sum_f64((double)ks - (double)kc + big);
             } else if constexpr (REDUCE == kReduceFp64) {
                 sse = warp_sum_f64(acc);
             } else {
@@ -541,6 +551,7 @@ interp_smem_kernel(InterpArgs args) {
         const uint32_t* __restrict__ pw = args.uops + p0;
 
         float ks = 0.0f, kc = 0.0f;
+        double big = 0.0;
         double acc = 0.0;
 
         for (int64_t base = cbeg; base < cend; base += kPass) {
@@ -627,7 +638,10 @@ interp_smem_kernel(InterpArgs args) {
                     for (int k = 0; k < K; ++k) {
                         const int64_t c = base + (int64_t)((k / V) * 32 + lane) * V + (k % V);
                         const float e = __fsub_rn(o[k], t[k]);
-                        const float qv = (c < cend) ? __fmul_rn(e, e) : 0.0f;
+                        const bool valid = c < cend;
+                        const bool huge = !(fabsf(e) <= kKahanMaxError);
+                        const float qv = (valid && !huge) ? __fmul_rn(e, e) : 0.0f;
+                        if (valid && huge) big = __dadd_rn(big, __dmul_rn((double)e, (double)e));
                         const float yk = __fsub_rn(qv, kc);
                         const float tt = __fadd_rn(ks, yk);
                         kc = __fsub_rn(__fsub_rn(tt, ks), yk);
@@ -665,7 +679,7 @@ interp_smem_kernel(InterpArgs args) {
 
         if constexpr (MODE == kModeFitness) {
             double sse;
-            if constexpr (REDUCE == kReduceKahan32) sse = warp_sum_f64((double)ks - (double)kc);
+            if constexpr (REDUCE == kReduceKahan32) sse = warp_sum_f64((double)ks - (double)kc + big);
             else if constexpr (REDUCE == kReduceFp64) sse = warp_sum_f64(acc);
             else sse = acc;
             if (lane == 0) {

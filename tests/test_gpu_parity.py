@@ -338,3 +338,27 @@ def test_single_generation_subsample_against_cpu(native, orc):
         ref = o.case_outputs(p, wl.X)
         if ieee[i]:
             assert same_or_nan(outs[i], ref).all(), i
+
+
+def test_kahan32_survives_errors_beyond_float_square_range(native):
+    """Errors up to ~1e28 (their squares overflow FP32): the compensated FP32
+    mode must still match the FP64 case-order sum to 1e-6 relative."""
+    rng = np.random.default_rng(12)
+    N = 5000
+    X = (10.0 ** rng.uniform(2, 7, (N, 1))).astype(np.float32)
+    y = rng.uniform(-1, 1, N).astype(np.float32)
+    MUL = 2
+    progs = [[], [(MUL, 0, 0, 0, 0)], [(MUL, 0, 0, 0, 0), (MUL, 0, 0, 0, 0)],
+             [(MUL, 1, 0, 0, 0), (MUL, 0, 1, 1, 0)], [(MUL, 0, 0, 6, 1), (MUL, 0, 0, 0, 0)]]
+    words = [W.encode([p[0] for p in pr], [p[1] for p in pr], [p[2] for p in pr], [p[3] for p in pr],
+                      [p[4] for p in pr]) if pr else np.zeros(0, np.uint32) for pr in progs]
+    off = W.csr_offsets([w.size for w in words])
+    words = np.concatenate(words).astype(np.uint32)
+    ds = g.Dataset(X, y)
+    with g.Evaluator(num_registers=8, reduce=g.REDUCE_ORDERED) as eo, g.Evaluator(num_registers=8) as ek:
+        fo, so = eo.evaluate_csr(words, off, ds, with_sse=True)
+        fk, sk = ek.evaluate_csr(words, off, ds, with_sse=True)
+    fin = np.isfinite(so)
+    assert fin.sum() >= 4 and (so[fin] > 3.4e38).any()
+    assert np.all(np.abs(sk[fin] - so[fin]) <= 1e-6 * so[fin])
+    assert np.all(np.abs(fk.astype(np.float64) - fo) <= 1e-6 * np.maximum(fo, 1e-45))
