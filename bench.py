@@ -480,7 +480,7 @@ def run_serve(args):
     pop_hi = max(1024, int((1 << 18) * args.scale * 2))
     isa, runs = W.serving_runs(n_runs=256, cases_hi=cases_hi, pop_hi=pop_hi, generations=3)
     ev = g.Evaluator(num_registers=16)
-    sv = g.Server(ev, hbm_budget_bytes=int(150e9), slots=2, slot_programs=1 << 20, slot_words=1 << 27,
+    sv = g.Server(ev, hbm_budget_bytes=int(150e9), slots=4, slot_programs=1 << 20, slot_words=1 << 27,
                   slot_items=1 << 23)
     rng = np.random.default_rng(9)
     arrivals = np.cumsum(rng.exponential(2e-3, size=len(runs)))
@@ -522,7 +522,7 @@ def run_serve(args):
         "device_busy_frac": tot.device_ms / 1e3 / wall, "wall_s": wall,
         "config": {"workload": f"256 GP runs, Poisson arrivals (mean 2 ms), 3 generations each; cases "
                                f"log-uniform [256,{cases_hi}], 1-8 features; populations log-uniform "
-                               f"[1000,{pop_hi}], lengths U[8,512]; HBM admission cap 150 GB; 2 batches in flight"},
+                               f"[1000,{pop_hi}], lengths U[8,512]; HBM admission cap 150 GB; 4 batches in flight"},
     }
     print(json.dumps(line), flush=True)
 

@@ -54,6 +54,7 @@ EXPORTED = (
     "galop_dataset_device_bytes", "galop_batch_create", "galop_batch_destroy", "galop_batch_device_bytes",
     "galop_batch_set_population", "galop_batch_evaluate", "galop_batch_synchronize", "galop_batch_get_fitness",
     "galop_batch_last_stats", "galop_batch_stream", "galop_batch_create_pool", "galop_batch_clear",
+    "galop_batch_get_fitness_all",
     "galop_batch_append", "galop_batch_population_work", "galop_server_options_init", "galop_server_create",
     "galop_server_destroy", "galop_server_open_run", "galop_server_close_run", "galop_server_submit",
     "galop_server_wait", "galop_server_stats",
@@ -89,7 +90,8 @@ class PopulationSpec(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_int64), ("slots", C.c_int32), ("max_pops_per_batch", C.c_int32),
-                ("slot_programs", C.c_int64), ("slot_words", C.c_int64), ("slot_items", C.c_int64)]
+                ("slot_programs", C.c_int64), ("slot_words", C.c_int64), ("slot_items", C.c_int64),
+                ("pinned_bytes", C.c_int64)]
 
 
 class RequestInfo(C.Structure):
@@ -170,6 +172,7 @@ def load_library(path: Optional[Path] = None) -> C.CDLL:
         "galop_batch_clear": (C.c_int, [_P]),
         "galop_batch_append": (C.c_int, [_P, _P, _U32P, _I64P, C.c_int64, C.POINTER(C.c_int32)]),
         "galop_batch_population_work": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int64)]),
+        "galop_batch_get_fitness_all": (C.c_int, [_P, _F32P, C.POINTER(C.c_int64)]),
         "galop_server_options_init": (C.c_int, [C.POINTER(ServerOptions)]),
         "galop_server_create": (C.c_int, [_P, C.POINTER(ServerOptions), C.POINTER(_P)]),
         "galop_server_destroy": (C.c_int, [_P]),

@@ -38,10 +38,12 @@ int64_t chunks_for(int64_t n_cases) {
 
 }  // namespace
 
+// Dataset buffers come from the stream-ordered allocator (cudaMallocAsync):
+// admitting a new dataset while batches run does not synchronise the device.
 struct galop_dataset {
     galop_ctx* ctx = nullptr;
     int device = 0;                 // kept so destruction never reads the context
-    DevBuf<float> X, y;
+    struct Buf { float* p = nullptr; size_t cap = 0; } X, y;
     int64_t N = 0, Np = 0;
     int32_t k = 0;
 };
@@ -235,27 +237,32 @@ int galop_dataset_create(galop_ctx* ctx, const float* inputs, const float* targe
     ds->N = n_cases;
     ds->k = num_inputs;
     ds->Np = std::max<int64_t>(1024, (n_cases + 1023) / 1024 * 1024);
-    DevBuf<float> aos, yin;
-    cudaError_t e = ds->X.ensure((size_t)ds->Np * std::max(num_inputs, 1));
-    if (e == cudaSuccess) e = ds->y.ensure((size_t)ds->Np);
-    if (e == cudaSuccess) e = aos.ensure(std::max<size_t>((size_t)n_cases * num_inputs, 1));
-    if (e == cudaSuccess) e = yin.ensure(std::max<size_t>((size_t)n_cases, 1));
+    ds->X.cap = (size_t)ds->Np * std::max(num_inputs, 1);
+    ds->y.cap = (size_t)ds->Np;
+    cudaStream_t s = ctx->stream;
+    float* aos = nullptr;
+    float* yin = nullptr;
+    const size_t nx = std::max<size_t>((size_t)n_cases * num_inputs, 1);
+    const size_t ny = std::max<size_t>((size_t)n_cases, 1);
+    cudaError_t e = cudaMallocAsync(&ds->X.p, ds->X.cap * sizeof(float), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&ds->y.p, ds->y.cap * sizeof(float), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&aos, nx * sizeof(float), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&yin, ny * sizeof(float), s);
     if (e == cudaSuccess && n_cases * num_inputs > 0)
-        e = cudaMemcpyAsync(aos.p, inputs, (size_t)n_cases * num_inputs * sizeof(float), cudaMemcpyHostToDevice,
-                            ctx->stream);
+        e = cudaMemcpyAsync(aos, inputs, (size_t)n_cases * num_inputs * sizeof(float), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && n_cases > 0)
-        e = cudaMemcpyAsync(yin.p, targets, (size_t)n_cases * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+        e = cudaMemcpyAsync(yin, targets, (size_t)n_cases * sizeof(float), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
-        dataset_transpose_kernel<<<(unsigned)((ds->Np + 255) / 256), 256, 0, ctx->stream>>>(
-            aos.p, yin.p, n_cases, num_inputs, ds->Np, ds->X.p, ds->y.p);
+        dataset_transpose_kernel<<<(unsigned)((ds->Np + 255) / 256), 256, 0, s>>>(aos, yin, n_cases, num_inputs,
+                                                                                ds->Np, ds->X.p, ds->y.p);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    aos.release();
-    yin.release();
+    if (aos) cudaFreeAsync(aos, s);
+    if (yin) cudaFreeAsync(yin, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // this stream only, not the device
     if (e != cudaSuccess) {
-        ds->X.release();
-        ds->y.release();
+        if (ds->X.p) cudaFreeAsync(ds->X.p, s);
+        if (ds->y.p) cudaFreeAsync(ds->y.p, s);
         delete ds;
         return ctx->cuda_fail(e, "dataset upload");
     }
@@ -266,8 +273,9 @@ int galop_dataset_create(galop_ctx* ctx, const float* inputs, const float* targe
 int galop_dataset_destroy(galop_dataset* ds) {
     if (!ds) return GALOP_OK;
     cudaSetDevice(ds->device);
-    ds->X.release();
-    ds->y.release();
+    // stream-ordered release; no kernel may still be reading the dataset
+    if (ds->X.p) cudaFreeAsync(ds->X.p, 0);
+    if (ds->y.p) cudaFreeAsync(ds->y.p, 0);
     delete ds;
     return GALOP_OK;
 }
@@ -564,6 +572,35 @@ int galop_batch_last_stats(galop_batch* b, galop_stats* out) {
 }
 
 void* galop_batch_stream(galop_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+int galop_batch_get_fitness_all(galop_batch* b, float* fitness_out, int64_t* eff_per_pop) {
+    if (!b) return GALOP_E_INVALID;
+    galop_ctx* ctx = b->ctx;
+    GALOP_CK(cudaSetDevice(ctx->device), "set device");
+    // Populations occupy consecutive output slots in pooled batches; fixed
+    // batches have per-population regions, copied one by one.
+    int64_t base = 0;
+    std::vector<int64_t> gb(b->pops.size());
+    for (size_t p = 0; p < b->pops.size(); ++p) { gb[p] = base; base += b->pops[p].n; }
+    std::vector<int64_t> eo;
+    if (eff_per_pop) {
+        eo.resize((size_t)base + 1);
+        B_CK(cudaMemcpyAsync(eo.data(), b->eff_off.p, eo.size() * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                             b->stream), "D2H effective offsets");
+    }
+    int64_t o = 0;
+    for (size_t p = 0; p < b->pops.size(); ++p) {
+        const BatchPop& P = b->pops[p];
+        if (P.n && fitness_out)
+            B_CK(cudaMemcpyAsync(fitness_out + o, b->fitness.p + P.out_base, (size_t)P.n * sizeof(float),
+                                 cudaMemcpyDeviceToHost, b->stream), "D2H fitness");
+        o += P.n;
+    }
+    if (int rc = galop_batch_synchronize(b)) return rc;
+    if (eff_per_pop)
+        for (size_t p = 0; p < b->pops.size(); ++p) eff_per_pop[p] = eo[gb[p] + b->pops[p].n] - eo[gb[p]];
+    return GALOP_OK;
+}
 
 int galop_batch_population_work(galop_batch* b, int32_t pop, int64_t* eff_instructions) {
     if (!b || !eff_instructions) return GALOP_E_INVALID;

@@ -12,7 +12,11 @@
 //   - overlap: with several slots, a batch is composed and copied while
 //     earlier batches still run, and its kernels start as SMs free up;
 //   - completion: a finished slot's fitness vectors are copied to the
-//     callers' buffers and waiters are woken.
+//     callers' buffers (one device-to-host copy per batch) and waiters are
+//     woken.
+// Programs are copied at submission, on the caller's thread, into a pinned
+// ring buffer, so a batch's host-to-device copies run asynchronously; a
+// request that does not fit the ring keeps a pageable copy instead.
 // Case chunking depends only on a run's own dataset, so a request's fitness
 // is the same alone and in any mix.
 #include <cuda_runtime.h>
@@ -50,11 +54,60 @@ struct Run {
     Clock::time_point last_use;
 };
 
+// Page-locked staging for submitted programs.  Blocks are reserved in
+// submission order and released as batches complete (roughly FIFO); space is
+// reclaimed from the oldest block once it and everything before it is free.
+class PinnedRing {
+public:
+    ~PinnedRing() { if (base_) cudaFreeHost(base_); }
+    bool init(size_t bytes) {
+        if (bytes == 0) return true;
+        if (cudaMallocHost(&base_, bytes) != cudaSuccess) { cudaGetLastError(); base_ = nullptr; return false; }
+        cap_ = bytes;
+        return true;
+    }
+    // Reserve n bytes (256-aligned); null when full.
+    char* alloc(size_t n) {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!base_) return nullptr;
+        n = (n + 255) & ~(size_t)255;
+        if (live_.empty()) front_ = head_ = 0;
+        size_t off;
+        if (live_.empty() || head_ > front_ || (head_ == front_ && live_.empty())) {
+            if (head_ + n <= cap_) off = head_;
+            else if (n <= front_) off = 0;
+            else return nullptr;
+        } else {
+            if (head_ + n <= front_) off = head_;
+            else return nullptr;
+        }
+        live_.push_back({off, n, false});
+        head_ = off + n;
+        return base_ + off;
+    }
+    void release(const char* p) {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (auto& b : live_)
+            if (base_ + b.off == p) { b.freed = true; break; }
+        while (!live_.empty() && live_.front().freed) live_.pop_front();
+        front_ = live_.empty() ? head_ : live_.front().off;
+    }
+private:
+    struct Block { size_t off, size; bool freed; };
+    std::mutex mu_;
+    char* base_ = nullptr;
+    size_t cap_ = 0, front_ = 0, head_ = 0;
+    std::deque<Block> live_;
+};
+
 struct Request {
     int64_t id = 0;
     int32_t run = 0;
-    std::vector<uint32_t> words;
+    std::vector<uint32_t> words;          // pageable copy when the ring is full
     std::vector<int64_t> offsets;
+    char* pinned = nullptr;               // ring block: offsets then words
+    const uint32_t* w = nullptr;
+    const int64_t* o = nullptr;
     int64_t n = 0;
     float* out = nullptr;
     int32_t status = 1;                   // 1 = pending, 0 = done, < 0 = error
@@ -69,6 +122,8 @@ struct Slot {
     galop_batch* batch = nullptr;
     std::vector<std::shared_ptr<Request>> reqs;
     std::vector<int32_t> pops;
+    std::vector<float> fitness;           // whole-batch fitness, host side
+    std::vector<int64_t> eff;             // interpreted instructions per population
     bool busy = false;
 };
 
@@ -87,6 +142,7 @@ struct galop_server {
     std::deque<std::shared_ptr<Request>> pending;
     std::map<int64_t, std::shared_ptr<Request>> by_id;
     std::vector<Slot> slots;
+    PinnedRing ring;
     int64_t slot_bytes = 0;
     int64_t resident_bytes = 0;          // datasets on the device
     int64_t completed = 0, batches = 0, case_ops = 0;
@@ -130,6 +186,8 @@ void galop_server::compose(Slot& s) {
                 GALOP_OK) {
                 q->status = GALOP_E_NOMEM;
                 q->done = Clock::now();
+                if (q->pinned) ring.release(q->pinned);
+                q->pinned = nullptr;
                 --r->outstanding;
                 it = pending.erase(it);
                 cv_done.notify_all();
@@ -139,11 +197,13 @@ void galop_server::compose(Slot& s) {
             resident_bytes += r->ds_bytes;
         }
         int32_t pop = -1;
-        const int rc = galop_batch_append(s.batch, r->ds, q->words.data(), q->offsets.data(), q->n, &pop);
+        const int rc = galop_batch_append(s.batch, r->ds, q->w, q->o, q->n, &pop);
         if (rc == GALOP_E_CAPACITY) {
             if (s.reqs.empty()) {                         // can never fit a slot
                 q->status = GALOP_E_CAPACITY;
                 q->done = Clock::now();
+                if (q->pinned) ring.release(q->pinned);
+                q->pinned = nullptr;
                 --r->outstanding;
                 it = pending.erase(it);
                 cv_done.notify_all();
@@ -154,6 +214,8 @@ void galop_server::compose(Slot& s) {
         if (rc != GALOP_OK) {
             q->status = rc;
             q->done = Clock::now();
+            if (q->pinned) ring.release(q->pinned);
+            q->pinned = nullptr;
             --r->outstanding;
             it = pending.erase(it);
             cv_done.notify_all();
@@ -174,6 +236,8 @@ void galop_server::compose(Slot& s) {
         for (auto& q : s.reqs) {
             q->status = GALOP_E_CUDA;
             q->done = Clock::now();
+            if (q->pinned) ring.release(q->pinned);
+            q->pinned = nullptr;
             --runs[q->run]->outstanding;
         }
         s.reqs.clear();
@@ -188,17 +252,29 @@ void galop_server::complete(Slot& s) {
     galop_stats st{};
     galop_batch_last_stats(s.batch, &st);
     device_ms_total += st.total_ms;
+    int64_t total = 0;
+    for (auto& q : s.reqs) total += q->n;
+    s.fitness.resize((size_t)std::max<int64_t>(total, 1));
+    s.eff.resize(s.reqs.size());
+    const int rc = galop_batch_get_fitness_all(s.batch, s.fitness.data(), s.eff.data());
+    int64_t o = 0;
+    const auto now = Clock::now();
     for (size_t i = 0; i < s.reqs.size(); ++i) {
         Request& q = *s.reqs[i];
-        int rc = galop_batch_get_fitness(s.batch, s.pops[i], q.out, nullptr);
-        if (rc == GALOP_OK) rc = galop_batch_population_work(s.batch, s.pops[i], &q.eff);
-        if (rc == GALOP_OK) case_ops += q.eff * runs[q.run]->n_cases;
+        Run* r = runs[q.run].get();
+        if (rc == GALOP_OK) {
+            if (q.n) std::memcpy(q.out, s.fitness.data() + o, (size_t)q.n * sizeof(float));
+            q.eff = s.eff[i];
+            case_ops += q.eff * r->n_cases;
+        }
+        o += q.n;
+        if (q.pinned) ring.release(q.pinned);
+        q.pinned = nullptr;
         q.status = rc;
         q.device_ms = st.total_ms;
-        q.done = Clock::now();
-        Run* r = runs[q.run].get();
+        q.done = now;
         --r->outstanding;
-        r->last_use = q.done;
+        r->last_use = now;
         ++completed;
     }
     s.reqs.clear();
@@ -260,7 +336,8 @@ int galop_server_options_init(galop_server_options* o) {
     if (!o) return GALOP_E_INVALID;
     std::memset(o, 0, sizeof *o);
     o->hbm_budget_bytes = 150LL * 1000 * 1000 * 1000;
-    o->slots = 2;
+    o->slots = 4;
+    o->pinned_bytes = 1LL << 30;
     o->max_pops_per_batch = 64;
     o->slot_programs = 1 << 20;
     o->slot_words = 1LL << 27;
@@ -279,6 +356,7 @@ int galop_server_create(galop_ctx* ctx, const galop_server_options* opt, galop_s
     auto* sv = new galop_server();
     sv->ctx = ctx;
     sv->opt = o;
+    sv->ring.init((size_t)std::max<int64_t>(o.pinned_bytes, 0));   // without it, pageable copies
     sv->slots.resize(o.slots);
     for (Slot& s : sv->slots) {
         const int rc = galop_batch_create_pool(ctx, o.max_pops_per_batch, o.slot_programs, o.slot_words,
@@ -350,15 +428,32 @@ int galop_server_submit(galop_server* sv, int32_t run_id, const uint32_t* words,
     for (int64_t i = 0; i < n_programs; ++i)
         if (offsets[i + 1] < offsets[i]) return GALOP_E_INVALID;
     auto q = std::make_shared<Request>();
-    q->words.assign(words, words + offsets[n_programs]);
-    q->offsets.assign(offsets, offsets + n_programs + 1);
+    const int64_t total = offsets[n_programs];
+    const size_t ob = (size_t)(n_programs + 1) * sizeof(int64_t);
+    const size_t bytes = ((ob + 255) & ~(size_t)255) + (size_t)total * sizeof(uint32_t);
+    q->pinned = sv->ring.alloc(bytes);
+    if (q->pinned) {
+        std::memcpy(q->pinned, offsets, ob);
+        q->o = reinterpret_cast<const int64_t*>(q->pinned);
+        uint32_t* wdst = reinterpret_cast<uint32_t*>(q->pinned + ((ob + 255) & ~(size_t)255));
+        if (total) std::memcpy(wdst, words, (size_t)total * sizeof(uint32_t));
+        q->w = wdst;
+    } else {
+        q->words.assign(words, words + total);
+        q->offsets.assign(offsets, offsets + n_programs + 1);
+        q->w = q->words.data();
+        q->o = q->offsets.data();
+    }
     q->n = n_programs;
     q->out = fitness_out;
     q->run = run_id;
     q->submitted = Clock::now();
     std::lock_guard<std::mutex> lk(sv->mu);
     auto it = sv->runs.find(run_id);
-    if (it == sv->runs.end() || it->second->closed) return GALOP_E_INVALID;
+    if (it == sv->runs.end() || it->second->closed) {
+        if (q->pinned) sv->ring.release(q->pinned);
+        return GALOP_E_INVALID;
+    }
     q->id = sv->next_req++;
     *request_id = q->id;
     ++it->second->outstanding;

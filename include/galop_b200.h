@@ -205,7 +205,8 @@ GALOP_API int galop_memcpy_d2h(galop_ctx* ctx, void* dst, const void* src, int64
 /* ---- resident datasets and batched populations ---------------------------- */
 
 /* A dataset uploaded once and kept on the device (feature-major, padded).
- * Destroy datasets, batches and servers before the context they came from. */
+ * Destroy datasets, batches and servers before the context they came from,
+ * and a dataset only when no evaluation using it is still running. */
 typedef struct galop_dataset galop_dataset;
 GALOP_API int galop_dataset_create(galop_ctx* ctx, const float* inputs, const float* targets,
                                    int64_t n_cases, int32_t num_inputs, galop_dataset** out);
@@ -260,6 +261,9 @@ GALOP_API int galop_batch_create_pool(galop_ctx* ctx, int32_t max_pops, int64_t 
 GALOP_API int galop_batch_clear(galop_batch* b);
 GALOP_API int galop_batch_append(galop_batch* b, const galop_dataset* ds, const uint32_t* words,
                                  const int64_t* offsets, int64_t n_programs, int32_t* pop_out);
+/* Fitness of every population, concatenated in population order, and the
+ * interpreted instructions of each (eff_per_pop[n_pops], may be NULL); waits. */
+GALOP_API int galop_batch_get_fitness_all(galop_batch* b, float* fitness_out, int64_t* eff_per_pop);
 /* Interpreted (effective) instructions of population `pop` in the last
  * evaluation, summed over its programs; waits. */
 GALOP_API int galop_batch_population_work(galop_batch* b, int32_t pop, int64_t* eff_instructions);
@@ -276,11 +280,12 @@ GALOP_API int galop_batch_population_work(galop_batch* b, int32_t pop, int64_t* 
 typedef struct galop_server galop_server;
 typedef struct {
     int64_t hbm_budget_bytes;     /* resident datasets + slot buffers (default 150e9) */
-    int32_t slots;                /* batches in flight (default 2) */
+    int32_t slots;                /* batches in flight (default 4) */
     int32_t max_pops_per_batch;   /* requests per batch (default 64) */
     int64_t slot_programs;        /* per-batch capacities (defaults 2^20, 2^27, 2^23) */
     int64_t slot_words;
     int64_t slot_items;
+    int64_t pinned_bytes;         /* page-locked staging for submitted programs (1 GiB) */
 } galop_server_options;
 
 typedef struct {
