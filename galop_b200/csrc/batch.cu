@@ -19,6 +19,7 @@
 #include "batch.cuh"
 #include "context.cuh"
 #include "prepass.cuh"
+#include "interp_wide.cuh"
 
 using namespace galop;
 
@@ -84,6 +85,7 @@ struct galop_batch {
     const void* interp_fn = nullptr;
     int threads = 0, grid = 0;
     size_t smem = 0;
+    UopFormat fmt{};                  // micro-op form of the chosen interpreter
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     galop_stats stats{};
@@ -136,10 +138,14 @@ int plan(galop_batch* b) {
     const int k = pick_k(ctx);
     const int wpb = pick_wpb(ctx);
     b->threads = 32 * wpb;
-    b->interp_fn = ctx->isa.num_registers == 8 ? interp_kernel_nr8(k, 2, ctx->isa.profile, ctx->opt.reduce, kModeFitness)
-                                                : interp_kernel_nr16(k, 2, ctx->isa.profile, ctx->opt.reduce, kModeFitness);
+    // Batched work items need a shared-memory interpreter (2 or 3).
+    const int dispatch = pick_dispatch(ctx) == 3 ? 3 : 2;
+    b->interp_fn = ctx->isa.num_registers == 8
+                       ? interp_kernel_nr8(k, dispatch, ctx->isa.profile, ctx->opt.reduce, kModeFitness)
+                       : interp_kernel_nr16(k, dispatch, ctx->isa.profile, ctx->opt.reduce, kModeFitness);
     if (!b->interp_fn) return ctx->fail(GALOP_E_INVALID, "no batched interpreter for this configuration");
-    b->smem = (size_t)(b->threads + 32) * ctx->isa.num_registers * k * sizeof(float);
+    b->smem = dispatch == 3 ? wide_smem_bytes(ctx->isa.num_registers, k, wpb)
+                            : (size_t)(b->threads + 32) * ctx->isa.num_registers * k * sizeof(float);
     B_CK(cudaFuncSetAttribute(b->interp_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem), "smem attr");
     B_CK(cudaFuncSetAttribute(b->interp_fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                               cudaSharedmemCarveoutMaxShared), "carveout");
@@ -180,7 +186,7 @@ int enqueue(galop_batch* b) {
     scan_tile_offsets_kernel<<<1, kScanThreads, 0, s>>>(b->tiles.p, n_tiles);
     scan_apply_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(b->eff_len.p, G, b->tiles.p, n_tiles, b->eff_off.p);
     prepass_compact_kernel<SpanSource><<<blocks, tpb, 0, s>>>(src, G, ctx->isa, strip ? 1 : 0, b->eff_off.p,
-                                                              b->uops.p, nullptr);
+                                                              b->uops.p, nullptr, b->fmt);
     batch_key_kernel<<<blocks, tpb, 0, s>>>(b->layout.p, b->prog_pop.p, b->eff_len.p, G, b->key.p);
     order_hist_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p);
     order_scan_kernel<<<1, 1024, 0, s>>>(b->hist.p);
@@ -315,7 +321,8 @@ int allocate(galop_batch* b, int64_t words, int64_t offs, int64_t progs, int64_t
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev2);
     if (e == cudaSuccess) e = b->arena.ensure(W1);
-    if (e == cudaSuccess) e = b->uops.ensure(W1);
+    b->fmt = uop_format(ctx);
+    if (e == cudaSuccess) e = b->uops.ensure(W1 * (b->fmt.wide ? 4 : 1));
     if (e == cudaSuccess) e = b->local_off.ensure((size_t)std::max<int64_t>(offs, 1));
     if (e == cudaSuccess) e = b->starts.ensure(G1);
     if (e == cudaSuccess) e = b->lens.ensure(G1);

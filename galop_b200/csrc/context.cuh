@@ -104,6 +104,9 @@ namespace galop {
 int pick_k(const galop_ctx* ctx);
 int pick_wpb(const galop_ctx* ctx);
 const void* kernel_for(const galop_ctx* ctx, int k, int mode);
+int pick_dispatch(const galop_ctx* ctx);
+UopFormat uop_format(const galop_ctx* ctx);
+size_t interp_smem_bytes(const galop_ctx* ctx, int k, int wpb);
 const void* interp_kernel_nr8(int k, int dispatch, int profile, int reduce, int mode);
 const void* interp_kernel_nr16(int k, int dispatch, int profile, int reduce, int mode);
 }  // namespace galop

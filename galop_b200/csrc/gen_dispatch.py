@@ -15,6 +15,12 @@ Emitted for NR in {8, 16} and K in {1, 2, 4, 8}:
   scatter  r[idx][k] = v[k]
   od_vec   r[d][k] = OP(a[k], b[k])   table index op*NR + d
   od_sca   r[d][k] = OP(a[k], c)      (constant src2, one scalar)
+  wide     one whole binary instruction of the 16-byte micro-op kernel:
+           load a (and b) from the shared-memory register file, compute,
+           store t -- the table index is op | constant-src2 << 3, and
+           protected DIV is one of the arms
+  wide loop  the same arms as one PTX loop over consecutive binary
+           instructions (returns at the first unary op or window end)
 where OP is one of the single-instruction ops: ADD, SUB, MUL (add/sub/mul
 with explicit .rn rounding, which ptxas never contracts into FMA) and, for
 the REF profile, LT, GT (set.lt/set.gt .f32.f32: 1.0 if the ordered
@@ -118,6 +124,124 @@ def cheap_table(k: int, profile: int) -> str:
             f"const float (&b)[{k}], float (&t)[{k}]) {{\n" + asm_block(L, outs, ins) + "    }\n")
 
 
+def _vec(regs: list[str]) -> str:
+    return regs[0] if len(regs) == 1 else "{" + ", ".join(regs) + "}"
+
+
+def wide_ops(k: int, profile: int) -> str:
+    """One binary instruction of the 16-byte micro-op kernel, start to end.
+
+    Inputs: %0 table index (op | const << 3), %1/%2/%3 shared-memory byte
+    addresses of the lane's src1 / src2 / dest register (V floats per vector,
+    vectors 32*V floats apart), %4 the constant's bits (const arms).  src1 is
+    loaded before the branch so its latency overlaps the dispatch; src2 only
+    in the register arms (its address is meaningless for a constant).  DIV is
+    b != 0 ? a / b (div.rn.f32) : 1.0, as src/ISA.h:224; setp.neu treats a
+    NaN divisor as nonzero, like C's b != 0.0f."""
+    v = min(k, 4)
+    nq = k // v
+    ops = tuple(sorted(PROFILES[profile] + (3,)))
+    vs = "" if v == 1 else f".v{v}"
+
+    def ld(dst: str, addr: str) -> list[str]:
+        return [f"ld.shared{vs}.f32 {_vec([f'{dst}{q * v + e}' for e in range(v)])}, [{addr}+{q * 128 * v}];"
+                for q in range(nq)]
+
+    def st(addr: str) -> list[str]:
+        return [f"st.shared{vs}.f32 [{addr}+{q * 128 * v}], {_vec([f't{q * v + e}' for e in range(v)])};"
+                for q in range(nq)]
+
+    def body(op: int, const: bool) -> list[str]:
+        out = []
+        for q in range(k):
+            bq = "c" if const else f"b{q}"
+            if op == 3:
+                pq = "p0" if const else f"p{q}"
+                if q == 0 or not const:
+                    out.append(f"setp.neu.f32 {pq}, {bq}, 0f00000000;")
+                out.append(f"mov.f32 t{q}, 0f3F800000; @{pq} div.rn.f32 t{q}, a{q}, {bq};")
+            else:
+                out.append(f"{CHEAP[op]} t{q}, a{q}, {bq};")
+        return out
+
+    regs = ", ".join(f"{n}<{k}>" for n in "abt")
+    L = [f".reg .f32 {regs}, c;", f".reg .pred p<{k}>;", "mov.b32 c, %4;"]
+    L += ld("a", "%1")
+    targets = [f"R{op}_%=" if op in ops else "E%=" for op in range(8)] + \
+              [f"C{op}_%=" if op in ops else "E%=" for op in range(8)]
+    L += ["T%=: .branchtargets " + ", ".join(targets) + ";", "brx.idx.uni %0, T%=;"]
+    for op in ops:
+        L.append(f"R{op}_%=: " + " ".join(ld("b", "%2") + body(op, False) + st("%3")) + " bra.uni E%=;")
+        L.append(f"C{op}_%=: " + " ".join(body(op, True) + st("%3")) + " bra.uni E%=;")
+    L.append("E%=:")
+    text = "\\n\\t".join(L)
+    return ("    static __device__ __forceinline__ void run(uint32_t idx, uint32_t pa, uint32_t pb, uint32_t pt, "
+            "uint32_t cbits) {\n"
+            f'    asm volatile("{{\\n\\t{text}\\n\\t}}"\n'
+            '        :\n        : "r"(idx), "r"(pa), "r"(pb), "r"(pt), "r"(cbits)\n        : "memory");\n    }\n')
+
+
+def wide_loop(k: int, profile: int) -> str:
+    """The fast path of the 16-byte micro-op kernel as one PTX loop: execute
+    binary instructions from the staged micro-op at byte address %0 on,
+    until a micro-op whose word w is negative (a unary op or the window's end
+    marker); return with %0 pointing at it.
+
+    Two copies of the loop body alternate between two micro-op register sets
+    (u, v): each body prefetches the next micro-op into the other set, so no
+    micro-op is ever copied between registers.  %1 is the lane's register-file
+    base address.  The arms are those of wide_ops."""
+    v = min(k, 4)
+    nq = k // v
+    ops = tuple(sorted(PROFILES[profile] + (3,)))
+    vs = "" if v == 1 else f".v{v}"
+
+    def ld(dst: str, addr: str) -> list[str]:
+        return [f"ld.shared{vs}.f32 {_vec([f'{dst}{q * v + e}' for e in range(v)])}, [{addr}+{q * 128 * v}];"
+                for q in range(nq)]
+
+    def st(addr: str) -> list[str]:
+        return [f"st.shared{vs}.f32 [{addr}+{q * 128 * v}], {_vec([f't{q * v + e}' for e in range(v)])};"
+                for q in range(nq)]
+
+    def body(op: int, const: bool) -> list[str]:
+        out = []
+        for q in range(k):
+            bq = "c" if const else f"b{q}"
+            if op == 3:
+                pq = "p0" if const else f"p{q}"
+                if q == 0 or not const:
+                    out.append(f"setp.neu.f32 {pq}, {bq}, 0f00000000;")
+                out.append(f"mov.f32 t{q}, 0f3F800000; @{pq} div.rn.f32 t{q}, a{q}, {bq};")
+            else:
+                out.append(f"{CHEAP[op]} t{q}, a{q}, {bq};")
+        return out
+
+    regs = ", ".join(f"{n}<{k}>" for n in "abt")
+    L = [f".reg .f32 {regs}, c;", f".reg .pred p<{k}>, q;",
+         ".reg .u32 ux, uy, uz, uw, vx, vy, vz, vw, pa, pb, pt;",
+         "ld.shared.v4.u32 {ux, uy, uz, uw}, [%0];"]
+    for cur, nxt, here, there in (("u", "v", "A", "B"), ("v", "u", "B", "A")):
+        x, y, z, w = (f"{cur}{f}" for f in "xyzw")
+        L += [f"L{here}%=: setp.lt.s32 q, {w}, 0;", "@q bra.uni D%=;",
+              f"ld.shared.v4.u32 {{{nxt}x, {nxt}y, {nxt}z, {nxt}w}}, [%0+16];",
+              "add.u32 %0, %0, 16;",
+              f"add.u32 pa, %1, {x};", f"add.u32 pb, %1, {y};", f"add.u32 pt, %1, {z};", f"mov.b32 c, {y};"]
+        L += ld("a", "pa")
+        targets = [f"R{here}{op}_%=" if op in ops else f"D%=" for op in range(8)] + \
+                  [f"C{here}{op}_%=" if op in ops else f"D%=" for op in range(8)]
+        L += [f"T{here}%=: .branchtargets " + ", ".join(targets) + ";", f"brx.idx.uni {w}, T{here}%=;"]
+        for op in ops:
+            L.append(f"R{here}{op}_%=: " + " ".join(ld("b", "pb") + body(op, False) + st("pt"))
+                     + f" bra.uni L{there}%=;")
+            L.append(f"C{here}{op}_%=: " + " ".join(body(op, True) + st("pt")) + f" bra.uni L{there}%=;")
+    L.append("D%=:")
+    text = "\\n\\t".join(L)
+    return ("    static __device__ __forceinline__ void run(uint32_t& sp, uint32_t base) {\n"
+            f'    asm volatile("{{\\n\\t{text}\\n\\t}}"\n'
+            '        : "+r"(sp)\n        : "r"(base)\n        : "memory");\n    }\n')
+
+
 def main() -> None:
     out = ["// dispatch_gen.cuh -- GENERATED by gen_dispatch.py; do not edit by hand.",
            "// Jump-table (PTX brx.idx) register access for the LGP interpreter; see",
@@ -138,6 +262,18 @@ def main() -> None:
         for prof in PROFILES:
             out.append(f"template <>\nstruct CheapOps<{k}, {prof}> {{")
             out.append(cheap_table(k, prof))
+            out.append("};\n")
+    out.append("template <int K, int PROFILE>\nstruct WideOps;\n")
+    for k in KS:
+        for prof in PROFILES:
+            out.append(f"template <>\nstruct WideOps<{k}, {prof}> {{")
+            out.append(wide_ops(k, prof))
+            out.append("};\n")
+    out.append("template <int K, int PROFILE>\nstruct WideLoop;\n")
+    for k in KS:
+        for prof in PROFILES:
+            out.append(f"template <>\nstruct WideLoop<{k}, {prof}> {{")
+            out.append(wide_loop(k, prof))
             out.append("};\n")
     out.append("}  // namespace galop\n")
     path = Path(__file__).resolve().parent / "dispatch_gen.cuh"

@@ -1,5 +1,6 @@
 // Instantiations of the interpreter for 16-register ISAs.
 #include "interp.cuh"
+#include "interp_wide.cuh"
 
 
 namespace galop {
@@ -12,6 +13,18 @@ static const void* pick_mode(int reduce, int mode) {
         case kReduceKahan32: return (const void*)&interp_kernel<16, K, P, kReduceKahan32, kModeFitness, D>;
         case kReduceFp64: return (const void*)&interp_kernel<16, K, P, kReduceFp64, kModeFitness, D>;
         case kReduceOrdered: return (const void*)&interp_kernel<16, K, P, kReduceOrdered, kModeFitness, D>;
+        default: return nullptr;
+    }
+}
+
+template <int K, int P>
+static const void* pick_wide_mode(int reduce, int mode) {
+    if (mode == kModeOutputs) return (const void*)&interp_wide_kernel<16, K, P, kReduceFp64, kModeOutputs>;
+    if (mode == kModeTrace) return (const void*)&interp_wide_kernel<16, K, P, kReduceFp64, kModeTrace>;
+    switch (reduce) {
+        case kReduceKahan32: return (const void*)&interp_wide_kernel<16, K, P, kReduceKahan32, kModeFitness>;
+        case kReduceFp64: return (const void*)&interp_wide_kernel<16, K, P, kReduceFp64, kModeFitness>;
+        case kReduceOrdered: return (const void*)&interp_wide_kernel<16, K, P, kReduceOrdered, kModeFitness>;
         default: return nullptr;
     }
 }
@@ -37,6 +50,11 @@ static const void* pick_profile(int profile, int reduce, int mode) {
 
 template <int K>
 static const void* pick_dispatch(int dispatch, int profile, int reduce, int mode) {
+    if (dispatch == 3) {
+        if (profile == kProfileRef) return pick_wide_mode<K, kProfileRef>(reduce, mode);
+        if (profile == kProfileBj) return pick_wide_mode<K, kProfileBj>(reduce, mode);
+        return nullptr;
+    }
     if (dispatch == 2) {
         if (profile == kProfileRef) return pick_smem_mode<K, kProfileRef>(reduce, mode);
         if (profile == kProfileBj) return pick_smem_mode<K, kProfileBj>(reduce, mode);

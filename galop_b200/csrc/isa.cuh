@@ -63,6 +63,33 @@ __host__ __device__ __forceinline__ uint32_t encode_uop(const Decoded& d) {
     return (d.op | (d.unary << 6)) | (d.dest << 8) | (d.src1 << 16) | ((d.src2 | (d.is_const << 7)) << 24);
 }
 
+// Wide micro-op (16 bytes, interp_wide_kernel): the operand fields are
+// already byte offsets into the warp's shared-memory register file and a
+// constant operand carries its value, so the interpreter decodes nothing.
+//   x = src1 * stride            (0 for unary ops)
+//   y = src2 * stride, or the constant's bits when src2 is a constant
+//   z = dest * stride
+//   w = op | const << 3 | unary << 31   (kWideEnd ends a window)
+// stride = bytes per register per warp (32 lanes x K cases x 4 bytes).
+constexpr uint32_t kWideSpecial = 0x80000000u;
+constexpr uint32_t kWideEnd = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint4 encode_wide(const Decoded& d, uint32_t stride, const ConstPool& cp) {
+    uint4 u;
+    u.x = d.unary ? 0u : d.src1 * stride;
+    u.y = d.is_const ? __float_as_uint(cp.c[d.src2]) : d.src2 * stride;
+    u.z = d.dest * stride;
+    u.w = d.op | (d.is_const << 3) | (d.unary ? kWideSpecial : 0u);
+    return u;
+}
+
+// Which micro-op form the pre-pass writes.
+struct UopFormat {
+    int wide;              // 0: 32-bit micro-ops, 1: 16-byte wide micro-ops
+    uint32_t stride;       // wide: bytes per register per warp
+    ConstPool consts;      // wide: constant values folded into the micro-ops
+};
+
 __device__ __forceinline__ uint32_t uop_op(uint32_t u) { return u & 7u; }
 __device__ __forceinline__ uint32_t uop_dest(uint32_t u) { return (u >> 8) & 0xffu; }
 __device__ __forceinline__ uint32_t uop_src1(uint32_t u) { return (u >> 16) & 0xffu; }

@@ -114,6 +114,8 @@ extern "C" int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32
     const int k = (opt->cases_per_lane == 1 || opt->cases_per_lane == 2 || opt->cases_per_lane == 4 ||
                    opt->cases_per_lane == 8) ? opt->cases_per_lane : 4;
     const int wpb = (opt->warps_per_block >= 1 && opt->warps_per_block <= 8) ? opt->warps_per_block : 4;
+    // 32-bit micro-ops only (the static scratch holds one word per
+    // instruction): the wide interpreter (3) maps to the shared-memory one.
     const int dispatch = (opt->dispatch >= 0 && opt->dispatch <= 2) ? opt->dispatch : 2;
 
     // The work-queue head, the length totals and the order histogram carry
@@ -134,7 +136,7 @@ extern "C" int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32
     scan_tile_offsets_kernel<<<1, kScanThreads, 0, s>>>(sc->tiles, n_tiles);
     scan_apply_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(sc->eff_len, n, sc->tiles, n_tiles, sc->eff_off);
     prepass_compact_kernel<CsrSource><<<blocks, tpb, 0, s>>>(src, n, isa, strip ? 1 : 0, sc->eff_off, sc->uops,
-                                                             nullptr);
+                                                             nullptr, UopFormat{});
     const bool sched = n > 1;
     if (sched) {
         order_hist_kernel<<<blocks, tpb, 0, s>>>(sc->eff_len, n, sc->hist);

@@ -176,13 +176,20 @@ static __global__ void scan_apply_kernel(const int32_t* __restrict__ in, int64_t
     if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tile_offsets[n_tiles];
 }
 
-// Write micro-ops of the interpreted instructions of program i at eff_off[i].
-// raw_out (optional) receives the raw words of the same instructions.
+__device__ __forceinline__ void put_uop(uint32_t* __restrict__ uops, int64_t pos, const Decoded& d,
+                                        const UopFormat& fmt) {
+    if (fmt.wide) reinterpret_cast<uint4*>(uops)[pos] = encode_wide(d, fmt.stride, fmt.consts);
+    else uops[pos] = encode_uop(d);
+}
+
+// Write micro-ops of the interpreted instructions of program i at eff_off[i]
+// (one word each, or four in the wide format).  raw_out (optional) receives
+// the raw words of the same instructions.
 template <class Src>
 __global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int strip,
                                        const int64_t* __restrict__ eff_off,
                                        uint32_t* __restrict__ uops,
-                                       uint32_t* __restrict__ raw_out) {
+                                       uint32_t* __restrict__ raw_out, UopFormat fmt) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int64_t s = src.start(i);
@@ -191,7 +198,7 @@ __global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int st
     if (!strip) {
         for (int64_t pc = 0; pc < raw; ++pc) {
             const uint32_t w = __ldg(src.words + s + pc);
-            uops[o + pc] = encode_uop(decode_raw(isa, w));
+            put_uop(uops, o + pc, decode_raw(isa, w), fmt);
             if (raw_out) raw_out[o + pc] = w;
         }
         return;
@@ -203,7 +210,7 @@ __global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int st
         const Decoded d = decode_raw(isa, w);
         if (!((live >> d.dest) & 1u)) continue;
         --pos;
-        uops[pos] = encode_uop(d);
+        put_uop(uops, pos, d, fmt);
         if (raw_out) raw_out[pos] = w;
         live &= ~(1u << d.dest);
         if (!d.unary) live |= 1u << d.src1;

@@ -19,6 +19,7 @@
 #include "../../include/galop_b200.h"
 #include "interp.cuh"
 #include "prepass.cuh"
+#include "interp_wide.cuh"
 
 namespace galop {
 const void* interp_kernel_nr8(int k, int dispatch, int profile, int reduce, int mode);
@@ -42,9 +43,33 @@ int pick_wpb(const galop_ctx* ctx) {
     return (w >= 1 && w <= 8) ? w : 4;
 }
 
+int pick_dispatch(const galop_ctx* ctx) {
+    const int d = ctx->opt.dispatch;
+    return (d >= 0 && d <= 3) ? d : 3;
+}
+
+// Micro-op form the pre-pass writes for the chosen interpreter.
+UopFormat uop_format(const galop_ctx* ctx) {
+    UopFormat f{};
+    f.wide = pick_dispatch(ctx) == 3 ? 1 : 0;
+    f.stride = 128u * (uint32_t)pick_k(ctx);
+    f.consts = ctx->pool;
+    return f;
+}
+
+// Dynamic shared memory of one interpreter block.
+size_t interp_smem_bytes(const galop_ctx* ctx, int k, int wpb) {
+    const int d = pick_dispatch(ctx);
+    if (d == 3) return wide_smem_bytes(ctx->isa.num_registers, k, wpb);
+    // Register file of every lane plus one block-shared copy of the constant
+    // pool laid out the same way.
+    if (d == 2) return (size_t)(32 * wpb + 32) * ctx->isa.num_registers * k * sizeof(float);
+    return 0;
+}
+
 const void* kernel_for(const galop_ctx* ctx, int k, int mode) {
     const int reduce = ctx->opt.reduce;
-    const int dispatch = (ctx->opt.dispatch >= 0 && ctx->opt.dispatch <= 2) ? ctx->opt.dispatch : 2;
+    const int dispatch = pick_dispatch(ctx);
     if (ctx->isa.num_registers == 8) return interp_kernel_nr8(k, dispatch, ctx->isa.profile, reduce, mode);
     if (ctx->isa.num_registers == 16) return interp_kernel_nr16(k, dispatch, ctx->isa.profile, reduce, mode);
     return nullptr;
@@ -87,10 +112,11 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
     }
     GALOP_CK(cudaGetLastError(), "pre-pass count/scan launch");
     // Device buffer for micro-ops sized by the raw total (an upper bound).
-    GALOP_CK(ctx->uops.ensure((size_t)std::max<int64_t>(raw_words_total, 1)), "alloc uops");
+    const UopFormat fmt = uop_format(ctx);
+    GALOP_CK(ctx->uops.ensure((size_t)std::max<int64_t>(raw_words_total, 1) * (fmt.wide ? 4 : 1)), "alloc uops");
     if (n > 0) {
         prepass_compact_kernel<Src><<<blocks, tpb, 0, s>>>(src, n, ctx->isa, strip ? 1 : 0,
-                                                           ctx->eff_off.p, ctx->uops.p, raw_out);
+                                                           ctx->eff_off.p, ctx->uops.p, raw_out, fmt);
         ctx->launches += 1;
     }
     GALOP_CK(cudaGetLastError(), "pre-pass compact launch");
@@ -117,10 +143,7 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     const void* fn = kernel_for(ctx, k, mode);
     if (!fn) return ctx->fail(GALOP_E_INVALID, "no interpreter kernel for NR=%d K=%d",
                               ctx->isa.num_registers, k);
-    // Shared-memory register file (dispatch 4): NR*K floats per lane.
-    // plus one block-shared copy of the constant pool laid out the same way.
-    const size_t smem = ctx->opt.dispatch == 2
-                            ? (size_t)(threads + 32) * ctx->isa.num_registers * k * sizeof(float) : 0;
+    const size_t smem = interp_smem_bytes(ctx, k, wpb);
     if (smem) {
         GALOP_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
         GALOP_CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -293,7 +316,7 @@ int galop_options_init(galop_options* opt) {
     opt->intron_prepass = 1;
     opt->cases_per_lane = 0;
     opt->warps_per_block = 0;
-    opt->dispatch = 2;
+    opt->dispatch = 3;
     return GALOP_OK;
 }
 

@@ -24,7 +24,7 @@ def main():
     ap.add_argument("--workload", default="single_generation", choices=["single_generation", "opset"])
     ap.add_argument("--programs", type=int, default=16384)
     ap.add_argument("--cases", type=int, default=4096)
-    ap.add_argument("--dispatch", type=int, default=2)
+    ap.add_argument("--dispatch", type=int, default=3)
     ap.add_argument("--k", type=int, default=4)
     ap.add_argument("--wpb", type=int, default=4)
     ap.add_argument("--registers", type=int, default=16)

@@ -80,10 +80,12 @@ typedef struct {
                                  (src/Introns.h:28-57); outputs unchanged       */
     int32_t cases_per_lane;   /* 0 = tuned default; else 1, 2, 4 or 8          */
     int32_t warps_per_block;  /* 0 = tuned default; else 1..8                  */
-    int32_t dispatch;         /* LGP register file: 2 = shared memory,
-                                 register index = address (default);
-                                 1 = lane registers behind PTX jump tables;
-                                 0 = lane registers behind C++ switches     */
+    int32_t dispatch;         /* interpreter: 3 = shared-memory register file,
+                                 16-byte pre-decoded micro-ops (default);
+                                 2 = shared-memory register file, 32-bit
+                                 micro-ops; 1 = lane registers behind PTX
+                                 jump tables; 0 = lane registers behind C++
+                                 switches.  All give identical results.     */
     int32_t reserved[3];
 } galop_options;
 

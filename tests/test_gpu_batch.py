@@ -29,10 +29,11 @@ SPECS = [(700, 1000, 3, 4, 60), (50, 40000, 5, 8, 120), (1500, 33, 1, 2, 30), (3
          (0, 100, 1, 1, 1), (900, 4096, 8, 16, 200)]
 
 
+@pytest.mark.parametrize("dispatch", [2, 3])
 @pytest.mark.parametrize("reduce", [g.REDUCE_KAHAN32, g.REDUCE_ORDERED])
-def test_batch_matches_single_population_calls(native, reduce):
+def test_batch_matches_single_population_calls(native, reduce, dispatch):
     pops = _populations(1, SPECS)
-    with g.Evaluator(num_registers=16, reduce=reduce) as ev:
+    with g.Evaluator(num_registers=16, reduce=reduce, dispatch=dispatch) as ev:
         single = [ev.evaluate_csr(w, o, ds) if o.shape[0] > 1 else np.zeros(0, np.float32) for ds, w, o in pops]
         rds = [g.ResidentDataset(ev, ds) for ds, _, _ in pops]
         with g.Batch(ev, [(r, max(o.shape[0] - 1, 1), max(int(o[-1]), 1)) for r, (_, _, o) in zip(rds, pops)]) as b:
@@ -51,11 +52,12 @@ def test_batch_matches_single_population_calls(native, reduce):
             assert rel.size == 0 or rel.max() <= 1e-6, p
 
 
-def test_population_fitness_is_identical_alone_and_in_a_mix(native):
+@pytest.mark.parametrize("dispatch", [2, 3])
+def test_population_fitness_is_identical_alone_and_in_a_mix(native, dispatch):
     """Case chunking depends on a population's own case count only, so its
     fitness does not depend on what else is batched with it."""
     pops = _populations(2, SPECS)
-    with g.Evaluator(num_registers=16) as ev:
+    with g.Evaluator(num_registers=16, dispatch=dispatch) as ev:
         rds = [g.ResidentDataset(ev, ds) for ds, _, _ in pops]
         caps = [(r, max(o.shape[0] - 1, 1), max(int(o[-1]), 1)) for r, (_, _, o) in zip(rds, pops)]
         with g.Batch(ev, caps) as mix:
@@ -70,13 +72,14 @@ def test_population_fitness_is_identical_alone_and_in_a_mix(native):
                 assert np.array_equal(bits(alone.fitness(0)), bits(mixed[p])), p
 
 
-def test_graph_replay_across_generations(native):
+@pytest.mark.parametrize("dispatch", [2, 3])
+def test_graph_replay_across_generations(native, dispatch):
     """A captured generation replays with new program contents (same counts)
     and gives the same fitness as an uncaptured evaluation."""
     rng = np.random.default_rng(3)
     pops = _populations(3, SPECS[:3])
     isa = W.IsaSpec(g.PROFILE_REF, 16)
-    with g.Evaluator(num_registers=16) as ev:
+    with g.Evaluator(num_registers=16, dispatch=dispatch) as ev:
         rds = [g.ResidentDataset(ev, ds) for ds, _, _ in pops]
         caps = [(r, o.shape[0] - 1, 2 * int(o[-1]) + 1000) for r, (_, _, o) in zip(rds, pops)]
         with g.Batch(ev, caps) as bg, g.Batch(ev, caps) as bp:

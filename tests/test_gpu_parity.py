@@ -26,6 +26,9 @@ pytestmark = pytest.mark.gpu
 VARIANTS = {"nr8": (8, False), "nr16": (16, False), "ip16": (16, True)}
 IEEE_REF = {0, 1, 2, 3, 6, 7}
 IEEE_BJ = {0, 1, 2, 3}
+# Shared-memory register file with 32-bit micro-ops (2) and with 16-byte
+# pre-decoded micro-ops (3).
+DISPATCHES = [2, 3]
 
 
 def ordered(x: np.ndarray) -> np.ndarray:
@@ -61,15 +64,16 @@ def program_is_ieee(o, prog, profile) -> bool:
 
 # --- single instructions ----------------------------------------------------------
 
+@pytest.mark.parametrize("dispatch", DISPATCHES)
 @pytest.mark.parametrize("k", [1, 4])
-def test_apply_op_against_reference_vectors(native, k):
+def test_apply_op_against_reference_vectors(native, k, dispatch):
     """Every opcode on special and random operands (golden values recorded
     from the reference's ISA::apply_op)."""
     with np.load(GOLDEN / "ops_ref.npz") as z:
         a, b, out = z["a"], z["b"], z["out"]
     X = np.stack([a, b], axis=1)
     ds = g.Dataset(X, np.zeros(a.size, np.float32))
-    with g.Evaluator(num_registers=8, cases_per_lane=k, intron_prepass=False) as ev:
+    with g.Evaluator(num_registers=8, cases_per_lane=k, intron_prepass=False, dispatch=dispatch) as ev:
         ev.set_dataset(ds)
         for op in range(8):
             prog = W.encode([op], [0], [0], [1], [0])
@@ -82,14 +86,15 @@ def test_apply_op_against_reference_vectors(native, k):
                 assert ok.all(), (op, a[~ok][:5], b[~ok][:5], got[~ok][:5], out[op][~ok][:5])
 
 
-def test_bj_exp_log_within_2ulp(native, orc):
+@pytest.mark.parametrize("dispatch", DISPATCHES)
+def test_bj_exp_log_within_2ulp(native, orc, dispatch):
     rng = np.random.default_rng(5)
     x = np.concatenate([rng.uniform(-100, 100, 20000), rng.standard_normal(20000) * 1e3,
                         np.array([0.0, -0.0, 1e-40, -1e-40, np.inf, -np.inf, np.nan, 88.72, 88.73, -103.9])
                         ]).astype(np.float32)
     o = orc.Oracle(orc.PROFILE_BJ, 8)
     ds = g.Dataset(x.reshape(-1, 1), np.zeros_like(x))
-    with g.Evaluator(profile=g.PROFILE_BJ, num_registers=8) as ev:
+    with g.Evaluator(profile=g.PROFILE_BJ, num_registers=8, dispatch=dispatch) as ev:
         ev.set_dataset(ds)
         for op in (6, 7):
             prog = W.encode([op], [0], [3], [0], [0])
@@ -100,9 +105,10 @@ def test_bj_exp_log_within_2ulp(native, orc):
 
 # --- golden vectors recorded from the reference ---------------------------------
 
+@pytest.mark.parametrize("dispatch", DISPATCHES)
 @pytest.mark.parametrize("variant", list(VARIANTS))
 @pytest.mark.parametrize("k", [2, 8])
-def test_golden_vectors_outputs_and_fitness(native, orc, variant, k):
+def test_golden_vectors_outputs_and_fitness(native, orc, variant, k, dispatch):
     v = load_vectors(variant)
     nr, ip = VARIANTS[variant]
     o = orc.Oracle(orc.PROFILE_REF, nr, ip)
@@ -110,8 +116,10 @@ def test_golden_vectors_outputs_and_fitness(native, orc, variant, k):
     n = len(off) - 1
     ieee = np.array([program_is_ieee(o, words[off[i]:off[i + 1]], g.PROFILE_REF) for i in range(n)])
     assert ieee.sum() > 50
-    with g.Evaluator(num_registers=nr, input_protect=ip, reduce=g.REDUCE_ORDERED, cases_per_lane=k) as ev, \
-            g.Evaluator(num_registers=nr, input_protect=ip, reduce=g.REDUCE_KAHAN32, cases_per_lane=k) as ek:
+    with g.Evaluator(num_registers=nr, input_protect=ip, reduce=g.REDUCE_ORDERED, cases_per_lane=k,
+                     dispatch=dispatch) as ev, \
+            g.Evaluator(num_registers=nr, input_protect=ip, reduce=g.REDUCE_KAHAN32, cases_per_lane=k,
+                        dispatch=dispatch) as ek:
         for d in ("d1", "d2", "d3", "d4"):
             ds = g.Dataset(v[f"{d}_X"], v[f"{d}_y"])
             outs = ev.case_outputs(words, off, ds)
@@ -156,16 +164,17 @@ def test_dense_layout_matches_csr_bitwise(native, variant):
 
 # --- instruction-level replay -------------------------------------------------------
 
+@pytest.mark.parametrize("dispatch", DISPATCHES)
 @pytest.mark.parametrize("profile,nr", [(g.PROFILE_REF, 8), (g.PROFILE_REF, 16), (g.PROFILE_BJ, 8),
                                         (g.PROFILE_BJ, 16)])
-def test_trace_replay_every_instruction(native, orc, profile, nr):
+def test_trace_replay_every_instruction(native, orc, profile, nr, dispatch):
     """Each GPU instruction, fed the GPU's own register file, reproduces the
     CPU's apply_op: bit-exact for IEEE ops, <= 2 ulp for SIN/COS/EXP/LOG."""
     rng = np.random.default_rng(7 + nr + profile)
     o = orc.Oracle(profile, nr)
     X = rng.uniform(-4, 4, size=(256, min(5, nr))).astype(np.float32)
     ds = g.Dataset(X, np.zeros(256, np.float32))
-    with g.Evaluator(profile=profile, num_registers=nr, cases_per_lane=4) as ev:
+    with g.Evaluator(profile=profile, num_registers=nr, cases_per_lane=4, dispatch=dispatch) as ev:
         ev.set_dataset(ds)
         for _ in range(12):
             prog = W.random_words(rng, int(rng.integers(1, 120)), nr)
@@ -214,7 +223,7 @@ def test_prepass_on_off_and_tile_shapes_bitwise(native):
     for pre in (True, False):
         for k in (1, 2, 4, 8):
             for wpb in (1, 4, 8):
-                for disp in (0, 1, 2):
+                for disp in (0, 1, 2, 3):
                     with g.Evaluator(num_registers=16, intron_prepass=pre, cases_per_lane=k, warps_per_block=wpb,
                                      reduce=g.REDUCE_ORDERED, dispatch=disp) as ev:
                         outs = ev.case_outputs(wl.words, wl.offsets, ds)
@@ -261,11 +270,12 @@ def test_reduction_modes_against_fp64_sum_of_gpu_outputs(native):
 
 # --- edge cases ------------------------------------------------------------------------
 
-def test_edge_cases(native, orc):
+@pytest.mark.parametrize("dispatch", DISPATCHES)
+def test_edge_cases(native, orc, dispatch):
     o = orc.Oracle(orc.PROFILE_REF, 8)
     rng = np.random.default_rng(4)
     words, off = W.random_population(rng, np.array([0, 1, 5, 0, 50]), 8)
-    with g.Evaluator(num_registers=8, reduce=g.REDUCE_ORDERED) as ev:
+    with g.Evaluator(num_registers=8, reduce=g.REDUCE_ORDERED, dispatch=dispatch) as ev:
         with pytest.raises(g.GalopError) as e:
             ev.evaluate_csr(words, off)
         assert e.value.status == g.E_NO_DATASET
@@ -293,7 +303,8 @@ def test_edge_cases(native, orc):
         assert e.value.status == g.E_INVALID
 
 
-def test_case_chunking_large_n_few_programs(native, orc):
+@pytest.mark.parametrize("dispatch", DISPATCHES)
+def test_case_chunking_large_n_few_programs(native, orc, dispatch):
     """Few programs over many cases split each program into case chunks
     whose partial sums are combined in chunk order."""
     rng = np.random.default_rng(8)
@@ -304,7 +315,7 @@ def test_case_chunking_large_n_few_programs(native, orc):
     words, off = W.structured_population(rng, W.uniform_lengths(rng, 8, 5, 40), isa, 0.8)
     o = orc.Oracle(orc.PROFILE_REF, 8)
     want, sse = o.evaluate_csr(words, off, X, y, with_sse=True)
-    with g.Evaluator(num_registers=8, reduce=g.REDUCE_FP64) as ev:
+    with g.Evaluator(num_registers=8, reduce=g.REDUCE_FP64, dispatch=dispatch) as ev:
         fit, gsse = ev.evaluate_csr(words, off, g.Dataset(X, y), with_sse=True)
         assert ev.stats.case_chunks > 1
     ieee = np.array([program_is_ieee(o, words[off[i]:off[i + 1]], 0) for i in range(len(off) - 1)])
