@@ -165,15 +165,20 @@ def measured_peaks() -> dict:
     return {}
 
 
-def profile_traffic():
-    """DRAM bytes per interpreter launch from the committed ncu summary."""
+def profile_summary() -> dict:
+    """Kernel name and DRAM bytes per interpreter launch from the committed
+    ncu summary."""
     p = ROOT / "profiles" / "interp_single_generation.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get("dram_bytes_per_launch_full")
+            return json.loads(p.read_text())
         except (ValueError, OSError):
-            return None
-    return None
+            return {}
+    return {}
+
+
+def profile_traffic():
+    return profile_summary().get("dram_bytes_per_launch_full")
 
 
 def cpu_reference_rate(wl, seconds: float, threads: int):
@@ -367,7 +372,7 @@ def run_b200(args, dist: Dist):
             "raw_gpops": value * raw_instr / max(eff_instr, 1),
             "roofline": {"bound": "fp32_issue", "achieved": achieved, "peak": peak_gops, "unit": UNIT,
                          "frac": achieved / peak_gops, "traffic": profile_traffic(),
-                         "kernel": "interp_kernel", "kernel_ms": interp_avg_ms,
+                         "kernel": profile_summary().get("kernel", "interp_wide_kernel"), "kernel_ms": interp_avg_ms,
                          "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {sm_max:.0f} MHz "
                                         f"(sm_max_mhz of MEASURED_PEAKS.json)"},
             "clocks": clock,
