@@ -403,6 +403,11 @@ def run_batch(args):
     isa, X, y, pops = W.many_populations(n_cases=n_cases, size_lo=lo, size_hi=hi)
     ds = g.Dataset(X, y)
     ev = g.Evaluator(num_registers=16)
+    # Tile from the autotuner, measured on a sample of all populations together.
+    all_words = np.concatenate([w for w, _ in pops])
+    all_off = np.concatenate([[0]] + [o[1:] + base for (_, o), base in
+                                      zip(pops, np.cumsum([0] + [int(o[-1]) for _, o in pops[:-1]]))])
+    tune = ev.autotune(all_words, all_off.astype(np.int64), ds, cache=os.environ.get("GALOP_TUNE_CACHE"))
     rd = g.ResidentDataset(ev, ds)
     caps = [(rd, o.shape[0] - 1, int(o[-1])) for _, o in pops]
     b = g.Batch(ev, caps)
@@ -468,6 +473,7 @@ def run_batch(args):
         "fitness_rel_err_kahan32_vs_fp64_case_order": rel,
         "fitness_zero_mismatches": zero_mismatch,
         "kernels_per_generation": st.kernels_launched,
+        "autotune": {k: v for k, v in tune.as_dict().items() if k != "key"},
     }
     rd.close()
     ev.close()

@@ -57,7 +57,7 @@ EXPORTED = (
     "galop_batch_get_fitness_all",
     "galop_batch_append", "galop_batch_population_work", "galop_server_options_init", "galop_server_create",
     "galop_server_destroy", "galop_server_open_run", "galop_server_close_run", "galop_server_submit",
-    "galop_server_wait", "galop_server_stats",
+    "galop_server_wait", "galop_server_stats", "galop_autotune",
 )
 
 
@@ -68,6 +68,19 @@ class _Options(C.Structure):
         ("intron_prepass", C.c_int32), ("cases_per_lane", C.c_int32),
         ("warps_per_block", C.c_int32), ("dispatch", C.c_int32), ("reserved", C.c_int32 * 3),
     ]
+
+
+class TuneResult(C.Structure):
+    """galop_tune_result: the tile the autotuner chose."""
+    _fields_ = [("dispatch", C.c_int32), ("cases_per_lane", C.c_int32), ("warps_per_block", C.c_int32),
+                ("from_cache", C.c_int32), ("candidates", C.c_int32), ("reserved0", C.c_int32),
+                ("sample_programs", C.c_int64), ("gpops", C.c_double), ("default_gpops", C.c_double),
+                ("key", C.c_char * 320)]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
+        d["key"] = self.key.decode()
+        return d
 
 
 class Stats(C.Structure):
@@ -145,6 +158,8 @@ def load_library(path: Optional[Path] = None) -> C.CDLL:
         "galop_trace_program": (C.c_int, [_P, _U32P, C.c_int64, _F32P, _I64P]),
         "galop_effective_csr": (C.c_int, [_P, _U32P, _I64P, C.c_int64, _I64P, _U32P]),
         "galop_last_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+        "galop_autotune": (C.c_int, [_P, _U32P, _I64P, C.c_int64, C.c_int64, C.c_int32, C.c_char_p,
+                                     C.POINTER(TuneResult)]),
         "galop_synchronize": (C.c_int, [_P]),
         "galop_host_alloc": (C.c_int, [C.c_int64, C.POINTER(_P)]),
         "galop_host_free": (C.c_int, [_P]),
@@ -400,6 +415,20 @@ class Evaluator:
         s = Stats()
         self._check(self._lib.galop_last_stats(self._ctx, C.byref(s)))
         return s
+
+    def autotune(self, words: np.ndarray, offsets: np.ndarray, dataset: Optional[Dataset] = None,
+                 cache: Optional[str] = None, sample: int = 0, reps: int = 0) -> TuneResult:
+        """galop_autotune: time every tile on a sample of this population and
+        keep the fastest for this evaluator (cached in `cache`, a JSON-lines
+        file, when given)."""
+        self._ensure_dataset(dataset)
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        r = TuneResult()
+        self._check(self._lib.galop_autotune(self._ctx, _ptr(words, C.c_uint32), _ptr(offsets, C.c_int64),
+                                             offsets.shape[0] - 1, sample, reps,
+                                             cache.encode() if cache else None, C.byref(r)))
+        return r
 
     def synchronize(self):
         self._check(self._lib.galop_synchronize(self._ctx))

@@ -25,7 +25,7 @@ using namespace galop;
 
 namespace {
 
-constexpr int64_t kChunkCases = 16384;
+constexpr int64_t kChunkCases = kMaxItemCases;
 
 int64_t chunk_cases_for(int64_t n_cases) {
     const int64_t padded = std::max<int64_t>(1024, (n_cases + 1023) / 1024 * 1024);

@@ -44,6 +44,11 @@ using galop::kEvCount;
 using galop::ConstPool;
 using galop::IsaParams;
 
+// Most cases one work item of the persistent interpreter covers (a
+// multiple of every pass width 32*K): longer case ranges are split into
+// chunks whose partial sums are added in chunk order.
+constexpr int64_t kMaxItemCases = 16384;
+
 struct galop_ctx {
     galop_options opt{};
     IsaParams isa{};

@@ -154,13 +154,15 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     if (per_sm < 1) per_sm = 1;
     const int64_t resident_warps = (int64_t)ctx->sm_count * per_sm * wpb;
 
-    // Case chunking: enough work items to keep every resident warp busy.
+    // Case chunking: enough work items to keep every resident warp busy, and
+    // no item longer than kMaxItemCases cases, so that the longest programs
+    // of a population with uneven lengths do not leave a tail of one warp.
     const int64_t pass = 32LL * k;
     const int64_t passes = std::max<int64_t>(1, (ctx->N + pass - 1) / pass);
     int64_t n_chunks = 1;
-    if (mode == kModeFitness && ctx->opt.reduce != GALOP_REDUCE_ORDERED && n > 0 &&
-        n < 4 * resident_warps) {
-        n_chunks = std::min<int64_t>(passes, (4 * resident_warps + n - 1) / n);
+    if (mode == kModeFitness && ctx->opt.reduce != GALOP_REDUCE_ORDERED && n > 0) {
+        if (n < 4 * resident_warps) n_chunks = std::min<int64_t>(passes, (4 * resident_warps + n - 1) / n);
+        n_chunks = std::max<int64_t>(n_chunks, std::min<int64_t>(passes, (ctx->N + kMaxItemCases - 1) / kMaxItemCases));
     }
     if (mode != kModeFitness) n_chunks = 1;
     const int64_t chunk_passes = (passes + n_chunks - 1) / n_chunks;

@@ -126,6 +126,42 @@ GALOP_API const char* galop_last_error(const galop_ctx* ctx);
 GALOP_API const char* galop_status_string(int status);
 GALOP_API int galop_abi_version(void);
 
+/* ---- autotuner ----------------------------------------------------------- */
+
+/* No counterpart in the reference, whose kernel shape is fixed at compile
+ * time (src/EvaluatorCuda.cu:28-31).  Chooses the interpreter tile for this
+ * context and a population like `words`/`offsets` (CSR, host memory) on the
+ * resident dataset: every candidate of dispatch {3, 2} x cases per lane
+ * {1, 2, 4, 8} x warps per block {2, 4, 8} evaluates a sample of the
+ * population (every s-th program, at most sample_programs; 0 = 16,384), one
+ * warm-up and `reps` timed calls (0 = 2), and the shortest interpreter time
+ * wins.  The choice is written into the context's options, so later calls,
+ * and batches and servers created afterwards, use it.
+ *
+ * With cache_path non-NULL the choice is appended to that file as one JSON
+ * object per line under `key` = device name and SM count, ISA (registers,
+ * profile, input protection), reduction, intron pass, and the workload's
+ * size class (case count, mean raw program length and program count, each
+ * rounded to a power of two).  A later call whose key is in the file applies
+ * the file's last entry for it without measuring (from_cache = 1).
+ * Candidates run as ordinary evaluate calls on the context's stream. */
+typedef struct {
+    int32_t dispatch;
+    int32_t cases_per_lane;
+    int32_t warps_per_block;
+    int32_t from_cache;            /* 1: taken from the cache file            */
+    int32_t candidates;            /* tiles measured (0 when from the cache)  */
+    int32_t reserved0;
+    int64_t sample_programs;       /* programs in the timed sample            */
+    double gpops;                  /* effective GPop/s of the choice (sample) */
+    double default_gpops;          /* the default tile (3, 4, 4) on the sample */
+    char key[320];
+} galop_tune_result;
+
+GALOP_API int galop_autotune(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets,
+                             int64_t n_programs, int64_t sample_programs, int32_t reps,
+                             const char* cache_path, galop_tune_result* out);
+
 /* ---- dataset ------------------------------------------------------------- */
 
 /* Replaces CudaEvaluator::upload_dataset (src/EvaluatorCuda.cu:96-110).
