@@ -530,7 +530,9 @@ def run_serve(args):
                        "mean": float(np.mean(lat))},
         "queued_ms": {"p50": float(np.percentile(queued, 50)), "p99": float(np.percentile(queued, 99))},
         "requests": len(lat), "batches": int(tot.batches), "mean_batch_requests": float(np.mean(sizes)),
-        "device_busy_frac": tot.device_ms / 1e3 / wall, "wall_s": wall,
+        # sum of the batches' own device times over wall time: above 1 when
+        # batches in different slots overlap on the device
+        "batch_device_time_over_wall": tot.device_ms / 1e3 / wall, "wall_s": wall,
         "config": {"workload": f"256 GP runs, Poisson arrivals (mean 2 ms), 3 generations each; cases "
                                f"log-uniform [256,{cases_hi}], 1-8 features; populations log-uniform "
                                f"[1000,{pop_hi}], lengths U[8,512]; HBM admission cap 150 GB; 4 batches in flight"},
