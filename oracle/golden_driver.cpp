@@ -11,17 +11,46 @@
 //
 // usage: <bin> <train_csv> <test_csv> <target_name> <run_seed>
 //              <results_csv> <program_txt> <history_csv>
+//
+// Runs that are not golden cells may change the evaluation ISA (the engine
+// itself only moves instruction words, so it is unaffected):
+//   GALOP_DRIVER_PROFILE=bj          BJ op set: EXP and protected LOG in
+//                                    place of LT and GT (oracle and B200
+//                                    backends only)
+//   GALOP_DRIVER_CONSTANTS=<file>    NUM_REGISTERS whitespace-separated
+//                                    floats replacing LGPConfig::CONSTANTS
 #include <cstdio>
+#include <cstdlib>
 #include <fstream>
 #include <iostream>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "Dataset.h"
 #include "EvalBackend.h"
 #include "EvaluatorCpu.h"
 #include "LGPConfig.h"
 #include "LGPEngine.h"
+
+// 0 = REF, 1 = BJ.
+static int driver_profile() {
+    const char* p = std::getenv("GALOP_DRIVER_PROFILE");
+    return (p && std::string(p) == "bj") ? 1 : 0;
+}
+
+static std::vector<float> driver_constants() {
+    std::vector<float> c(LGPConfig::CONSTANTS.begin(), LGPConfig::CONSTANTS.end());
+    if (const char* path = std::getenv("GALOP_DRIVER_CONSTANTS")) {
+        std::ifstream f(path);
+        for (auto& v : c)
+            if (!(f >> v)) {
+                std::cerr << "GALOP_DRIVER_CONSTANTS: need " << c.size() << " floats in " << path << "\n";
+                std::exit(2);
+            }
+    }
+    return c;
+}
 
 #if defined(GOLDEN_BACKEND_B200)
 #include "galop_b200_backend.hpp"
@@ -38,10 +67,11 @@ void orc_evaluate_population_dense(const orc_isa_t* isa, const uint32_t* instruc
 }
 // EvalBackend over the C restatement, configured from this build's LGPConfig.
 struct OracleBackend : EvalBackend {
+    int profile = driver_profile();
+    std::vector<float> constants = driver_constants();
     void evaluate_population(const uint32_t* instructions, const uint8_t* lengths, float* fitness_out,
                              int n_programs, const Dataset& ds) override {
-        orc_isa_t isa{0, LGPConfig::NUM_REGISTERS, LGPConfig::INPUT_PROTECT ? 1 : 0, 0,
-                      LGPConfig::CONSTANTS.data()};
+        orc_isa_t isa{profile, LGPConfig::NUM_REGISTERS, LGPConfig::INPUT_PROTECT ? 1 : 0, 0, constants.data()};
         orc_evaluate_population_dense(&isa, instructions, lengths, LGPConfig::MAX_PROGRAM_SIZE, n_programs,
                                       ds.inputs.data(), ds.targets.data(), ds.num_inputs, ds.N, fitness_out);
     }
@@ -50,10 +80,18 @@ struct OracleBackend : EvalBackend {
 
 static std::unique_ptr<EvalBackend> make_backend() {
 #if defined(GOLDEN_BACKEND_B200)
-    return std::make_unique<galop::B200Evaluator>();
+    const std::vector<float> constants = driver_constants();
+    galop_options o = galop::B200Evaluator::options_from_config();
+    o.profile = driver_profile() ? GALOP_PROFILE_BJ : GALOP_PROFILE_REF;
+    o.constants = constants.data();                 // copied by galop_create
+    return std::make_unique<galop::B200Evaluator>(o);
 #elif defined(GOLDEN_BACKEND_ORACLE)
     return std::make_unique<OracleBackend>();
 #else
+    if (driver_profile() != 0 || std::getenv("GALOP_DRIVER_CONSTANTS")) {
+        std::cerr << "the reference CpuEvaluator evaluates the REF ISA with LGPConfig::CONSTANTS only\n";
+        std::exit(2);
+    }
     return std::make_unique<CpuEvaluator>();
 #endif
 }

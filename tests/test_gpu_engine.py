@@ -48,3 +48,32 @@ def test_golden_cells_with_b200_backend(tmp_path, capsys):
         report.append(f"{t} s{s}: {same - 1}/{len(gold) - 1} generations identical")
     with capsys.disabled():
         print("\n" + "\n".join(report))
+
+
+C1 = {b: ROOT / "oracle" / "_ref" / f"lgp_run_c1_{b}" for b in ("cpu", "oracle", "b200")}
+
+
+@pytest.mark.skipif(not all(e.exists() for e in C1.values()), reason="oracle/_ref/lgp_run_c1_* not built")
+def test_config1_engine_run_b200_vs_oracle(tmp_path, capsys):
+    """The 50-generation small-problem run with the B200 backend: the REF
+    ISA against the reference's CpuEvaluator, the BJ op set against the C
+    restatement.  Fitness bits agree whenever the per-case outputs do, so
+    the histories could part only where a <=2-ulp transcendental difference
+    changes a selection; on this run none does, and all 50 generations are
+    required to match."""
+    import config1 as c1
+    paths = c1.write_case(tmp_path)
+    report = []
+    for bj, ref_exe in ((False, C1["cpu"]), (True, C1["oracle"])):
+        want = c1.run(ref_exe, paths, tmp_path, f"ref_{bj}", bj=bj)
+        got = c1.run(C1["b200"], paths, tmp_path, f"b200_{bj}", bj=bj)
+        assert len(got) == len(want) == 51
+        same = 0
+        for a, b in zip(got, want):
+            if a != b:
+                break
+            same += 1
+        assert same == len(want), ("bj" if bj else "ref", same - 1)
+        report.append(f"config 1 {'BJ' if bj else 'REF'}: {same - 1}/50 generations identical")
+    with capsys.disabled():
+        print("\n" + "\n".join(report))
