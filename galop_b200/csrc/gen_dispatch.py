@@ -124,6 +124,44 @@ def cheap_table(k: int, profile: int) -> str:
             f"const float (&b)[{k}], float (&t)[{k}]) {{\n" + asm_block(L, outs, ins) + "    }\n")
 
 
+# Scratch registers of the wide arms (declared once per asm block).
+WIDE_TEMPS = ".reg .pred dp, dn, dz; .reg .f32 da, db, dq; .reg .b32 ds;"
+
+
+def wide_body(k: int, op: int, const: bool) -> list[str]:
+    """t[q] = OP(a[q], b[q]) (b = the scalar c for a constant src2).
+
+    DIV is b != 0 ? a / b : 1.0 (src/ISA.h:224) with IEEE round-to-nearest
+    (div.rn.f32), evaluated as:
+      dp = b != 0 or NaN (setp.neu: NaN counts as nonzero, like C's b != 0)
+      dz = a == +-0 and b is not NaN: the quotient is a zero whose sign is
+           sign(a) xor sign(b) (IEEE 754: 0/x = +-0 for every nonzero,
+           non-NaN x, infinities included), formed with one xor/and;
+      otherwise div.rn on (a, b), with a zero dividend or divisor replaced by
+      1.0 so the division only ever sees the operands whose quotient is used.
+    Zero dividends are common in LGP code (LT/GT results, x - x)."""
+    out = []
+    for q in range(k):
+        bq = "c" if const else f"b{q}"
+        if op != 3:
+            out.append(f"{CHEAP[op]} t{q}, a{q}, {bq};")
+            continue
+        out += [f"setp.neu.f32 dp, {bq}, 0f00000000;",
+                f"setp.num.f32 dn, {bq}, {bq};",
+                f"setp.eq.and.f32 dz, a{q}, 0f00000000, dn;",
+                f"selp.f32 da, 0f3F800000, a{q}, dz;",
+                f"selp.f32 db, {bq}, 0f3F800000, dp;",
+                "div.rn.f32 dq, da, db;",
+                f"mov.b32 ds, a{q};",
+                f"mov.b32 t{q}, {bq};",          # t as bit scratch until the select below
+                f"xor.b32 ds, ds, t{q};",
+                "and.b32 ds, ds, 0x80000000;",
+                f"selp.f32 t{q}, dq, 0f3F800000, dp;",
+                "and.pred dz, dz, dp;",
+                f"@dz mov.b32 t{q}, ds;"]
+    return out
+
+
 def _vec(regs: list[str]) -> str:
     return regs[0] if len(regs) == 1 else "{" + ", ".join(regs) + "}"
 
@@ -152,20 +190,10 @@ def wide_ops(k: int, profile: int) -> str:
                 for q in range(nq)]
 
     def body(op: int, const: bool) -> list[str]:
-        out = []
-        for q in range(k):
-            bq = "c" if const else f"b{q}"
-            if op == 3:
-                pq = "p0" if const else f"p{q}"
-                if q == 0 or not const:
-                    out.append(f"setp.neu.f32 {pq}, {bq}, 0f00000000;")
-                out.append(f"mov.f32 t{q}, 0f3F800000; @{pq} div.rn.f32 t{q}, a{q}, {bq};")
-            else:
-                out.append(f"{CHEAP[op]} t{q}, a{q}, {bq};")
-        return out
+        return wide_body(k, op, const)
 
     regs = ", ".join(f"{n}<{k}>" for n in "abt")
-    L = [f".reg .f32 {regs}, c;", f".reg .pred p<{k}>;", "mov.b32 c, %4;"]
+    L = [f".reg .f32 {regs}, c;", WIDE_TEMPS, "mov.b32 c, %4;"]
     L += ld("a", "%1")
     targets = [f"R{op}_%=" if op in ops else "E%=" for op in range(8)] + \
               [f"C{op}_%=" if op in ops else "E%=" for op in range(8)]
@@ -205,20 +233,10 @@ def wide_loop(k: int, profile: int) -> str:
                 for q in range(nq)]
 
     def body(op: int, const: bool) -> list[str]:
-        out = []
-        for q in range(k):
-            bq = "c" if const else f"b{q}"
-            if op == 3:
-                pq = "p0" if const else f"p{q}"
-                if q == 0 or not const:
-                    out.append(f"setp.neu.f32 {pq}, {bq}, 0f00000000;")
-                out.append(f"mov.f32 t{q}, 0f3F800000; @{pq} div.rn.f32 t{q}, a{q}, {bq};")
-            else:
-                out.append(f"{CHEAP[op]} t{q}, a{q}, {bq};")
-        return out
+        return wide_body(k, op, const)
 
     regs = ", ".join(f"{n}<{k}>" for n in "abt")
-    L = [f".reg .f32 {regs}, c;", f".reg .pred p<{k}>, q;",
+    L = [f".reg .f32 {regs}, c;", WIDE_TEMPS, ".reg .pred q;",
          ".reg .u32 ux, uy, uz, uw, vx, vy, vz, vw, pa, pb, pt;",
          "ld.shared.v4.u32 {ux, uy, uz, uw}, [%0];"]
     for cur, nxt, here, there in (("u", "v", "A", "B"), ("v", "u", "B", "A")):
