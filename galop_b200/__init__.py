@@ -32,6 +32,7 @@ LIB_PATH = _PKG / "libgalop_b200.so"
 
 PROFILE_REF, PROFILE_BJ = 0, 1
 REDUCE_KAHAN32, REDUCE_FP64, REDUCE_ORDERED = 0, 1, 2
+OBJECTIVE_MSE, OBJECTIVE_R2 = 0, 1
 
 OK = 0
 E_INVALID, E_CUDA, E_NOMEM, E_NO_DATASET, E_TIMEOUT, E_CAPACITY, E_NO_DEVICE, E_STATE = (
@@ -57,7 +58,7 @@ EXPORTED = (
     "galop_batch_get_fitness_all",
     "galop_batch_append", "galop_batch_population_work", "galop_server_options_init", "galop_server_create",
     "galop_server_destroy", "galop_server_open_run", "galop_server_close_run", "galop_server_submit",
-    "galop_server_wait", "galop_server_stats", "galop_autotune",
+    "galop_server_wait", "galop_server_stats", "galop_autotune", "galop_csv_read", "galop_csv_free",
 )
 
 
@@ -66,8 +67,14 @@ class _Options(C.Structure):
         ("profile", C.c_int32), ("num_registers", C.c_int32), ("input_protect", C.c_int32),
         ("reduce", C.c_int32), ("constants", C.POINTER(C.c_float)), ("device", C.c_int32),
         ("intron_prepass", C.c_int32), ("cases_per_lane", C.c_int32),
-        ("warps_per_block", C.c_int32), ("dispatch", C.c_int32), ("reserved", C.c_int32 * 3),
+        ("warps_per_block", C.c_int32), ("dispatch", C.c_int32), ("objective", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
+
+
+class _CsvDataset(C.Structure):
+    _fields_ = [("inputs", C.POINTER(C.c_float)), ("targets", C.POINTER(C.c_float)), ("n_cases", C.c_int64),
+                ("num_inputs", C.c_int32), ("reserved", C.c_int32), ("ss_tot", C.c_double)]
 
 
 class TuneResult(C.Structure):
@@ -158,6 +165,8 @@ def load_library(path: Optional[Path] = None) -> C.CDLL:
         "galop_trace_program": (C.c_int, [_P, _U32P, C.c_int64, _F32P, _I64P]),
         "galop_effective_csr": (C.c_int, [_P, _U32P, _I64P, C.c_int64, _I64P, _U32P]),
         "galop_last_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+        "galop_csv_read": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(_CsvDataset), C.c_char_p, C.c_int32]),
+        "galop_csv_free": (None, [C.POINTER(_CsvDataset)]),
         "galop_autotune": (C.c_int, [_P, _U32P, _I64P, C.c_int64, C.c_int64, C.c_int32, C.c_char_p,
                                      C.POINTER(TuneResult)]),
         "galop_synchronize": (C.c_int, [_P]),
@@ -235,11 +244,35 @@ class Dataset:
         self.targets = np.ascontiguousarray(self.targets, dtype=np.float32).reshape(-1)
         if self.inputs.shape[0] != self.targets.shape[0]:
             raise ValueError("inputs and targets disagree on the case count")
-        # Two-pass SS_tot over the valid targets (src/Dataset.cpp:35-47).
+        # Two-pass SS_tot over the valid targets, each pass a case-order
+        # double sum (cumsum accumulates sequentially) as src/Dataset.cpp:35-47.
         if self.N > 0:
             t = self.targets.astype(np.float64)
-            mean = float(np.sum(t)) / self.N
-            self.ss_tot = float(np.sum((t - mean) ** 2))
+            with np.errstate(all="ignore"):
+                mean = float(np.cumsum(t)[-1]) / self.N
+                d = t - mean
+                self.ss_tot = float(np.cumsum(d * d)[-1])
+
+    @classmethod
+    def from_csv(cls, path: str, multi: bool = False) -> "Dataset":
+        """load_csv_1d / load_csv_multi (src/Dataset.cpp:83-151) through
+        galop_csv_read: header line skipped, one case per non-empty line."""
+        lib = load_library()
+        d = _CsvDataset()
+        err = C.create_string_buffer(512)
+        rc = lib.galop_csv_read(str(path).encode(), int(bool(multi)), C.byref(d), err, len(err))
+        if rc != OK:
+            raise GalopError(rc, err.value.decode() or status_string(rc))
+        try:
+            n, k = int(d.n_cases), int(d.num_inputs)
+            X = np.ctypeslib.as_array(d.inputs, shape=(max(n * k, 1),))[: n * k].reshape(n, k).copy()
+            y = np.ctypeslib.as_array(d.targets, shape=(max(n, 1),))[:n].copy()
+            ss = float(d.ss_tot)
+        finally:
+            lib.galop_csv_free(C.byref(d))
+        ds = cls(X, y)
+        ds.ss_tot = ss
+        return ds
 
     @property
     def N(self) -> int:
@@ -257,7 +290,7 @@ class Evaluator:
     def __init__(self, profile: int = PROFILE_REF, num_registers: int = 8, input_protect: bool = False,
                  reduce: int = REDUCE_KAHAN32, constants: Optional[Sequence[float]] = None,
                  device: int = 0, intron_prepass: bool = True, cases_per_lane: int = 0,
-                 warps_per_block: int = 0, dispatch: Optional[int] = None):
+                 warps_per_block: int = 0, dispatch: Optional[int] = None, objective: int = OBJECTIVE_MSE):
         self._lib = load_library()
         opt = _Options()
         self._lib.galop_options_init(C.byref(opt))
@@ -271,6 +304,7 @@ class Evaluator:
         opt.warps_per_block = warps_per_block
         if dispatch is not None:
             opt.dispatch = dispatch
+        opt.objective = objective
         self.constants = None
         if constants is not None:
             self.constants = np.ascontiguousarray(constants, dtype=np.float32)

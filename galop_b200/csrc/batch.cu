@@ -47,6 +47,7 @@ struct galop_dataset {
     struct Buf { float* p = nullptr; size_t cap = 0; } X, y;
     int64_t N = 0, Np = 0;
     int32_t k = 0;
+    double ss_tot = 0.0;            // of the targets, for the R^2 objective
 };
 
 struct BatchPop {
@@ -120,7 +121,8 @@ int plan(galop_batch* b) {
         BatchPop& P = b->pops[p];
         lay[p] = PopLayout{base, P.n, P.word_base, P.off_base, P.ds->N};
         desc[p] = PopDesc{P.ds->X.p, P.ds->y.p, P.ds->N, P.ds->Np, b->fitness.p + P.out_base,
-                          b->sse.p + P.out_base, base, P.chunk_cases, (int32_t)P.n_chunks, P.ds->k};
+                          b->sse.p + P.out_base, base, P.chunk_cases, (int32_t)P.n_chunks, P.ds->k,
+                          objective_for(ctx, P.ds->ss_tot)};
         chunks[p] = (int32_t)P.n_chunks;
         base += P.n;
         items += P.n * P.n_chunks;
@@ -242,6 +244,7 @@ int galop_dataset_create(galop_ctx* ctx, const float* inputs, const float* targe
     ds->device = ctx->device;
     ds->N = n_cases;
     ds->k = num_inputs;
+    ds->ss_tot = targets_ss_tot(targets, n_cases);
     ds->Np = std::max<int64_t>(1024, (n_cases + 1023) / 1024 * 1024);
     ds->X.cap = (size_t)ds->Np * std::max(num_inputs, 1);
     ds->y.cap = (size_t)ds->Np;

@@ -104,8 +104,7 @@ static __global__ void batch_finalize_kernel(const PopDesc* __restrict__ descs, 
     const int64_t o = first_item[g];
     double s = 0.0;
     for (int c = 0; c < d.n_chunks; ++c) s += partial[o + c];
-    const float mse = (float)(s / (double)d.N);
-    d.fitness[g - d.prog_base] = isfinite(mse) ? __fdiv_rn(1.0f, __fadd_rn(1.0f, mse)) : 0.0f;
+    d.fitness[g - d.prog_base] = fitness_of(s, d.N, d.obj);
     if (d.sse) d.sse[g - d.prog_base] = s;
 }
 

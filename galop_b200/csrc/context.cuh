@@ -43,6 +43,23 @@ using galop::DevBuf;
 using galop::kEvCount;
 using galop::ConstPool;
 using galop::IsaParams;
+using galop::Objective;
+
+// Total sum of squares of the targets, two passes in double in case order
+// (the reference caches it per dataset: compute_ss_tot, src/Dataset.cpp:35-47).
+inline double targets_ss_tot(const float* y, int64_t n) {
+    if (n <= 0) return 0.0;
+    double mean = 0.0;
+    for (int64_t i = 0; i < n; ++i) mean += (double)y[i];
+    mean /= (double)n;
+    double ss = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double d = (double)y[i] - mean;
+        const double d2 = d * d;
+        ss += d2;
+    }
+    return ss;
+}
 
 // Most cases one work item of the persistent interpreter covers (a
 // multiple of every pass width 32*K): longer case ranges are split into
@@ -64,6 +81,7 @@ struct galop_ctx {
     DevBuf<float> X, y;
     DevBuf<float> stage_aos, stage_y;
     int64_t N = -1, Np = 0;
+    double ss_tot = 0.0;          // sum of squared target deviations (R^2)
     int num_inputs = 0;
 
     // population buffers (high-water)
@@ -115,3 +133,11 @@ size_t interp_smem_bytes(const galop_ctx* ctx, int k, int wpb);
 const void* interp_kernel_nr8(int k, int dispatch, int profile, int reduce, int mode);
 const void* interp_kernel_nr16(int k, int dispatch, int profile, int reduce, int mode);
 }  // namespace galop
+
+// The fitness definition of this context for a dataset with this ss_tot.
+inline Objective objective_for(const galop_ctx* ctx, double ss_tot) {
+    Objective o{};
+    o.kind = ctx->opt.objective == GALOP_OBJECTIVE_R2 ? galop::kObjectiveR2 : galop::kObjectiveMse;
+    o.ss_tot = ss_tot;
+    return o;
+}

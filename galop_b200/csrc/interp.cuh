@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 #include "isa.cuh"
 #include "dispatch_gen.cuh"
+#include "fitness.cuh"
 
 namespace galop {
 
@@ -44,6 +45,7 @@ struct PopDesc {
     int64_t chunk_cases;           // cases per work item (multiple of 1024)
     int32_t n_chunks;              // work items per program
     int32_t num_inputs;
+    Objective obj;                 // fitness from SSE for this population's dataset
 };
 
 struct InterpArgs {
@@ -60,6 +62,7 @@ struct InterpArgs {
     int32_t num_inputs;
     int32_t output_reg;
     ConstPool consts;
+    Objective obj;                 // fitness from SSE (single-population mode)
     unsigned long long* counter;   // work-queue head (zeroed before launch)
     float* fitness;                // [n_programs] (n_chunks == 1)
     double* sse;                   // [n_programs] or null (n_chunks == 1)
@@ -262,11 +265,6 @@ __device__ __forceinline__ double warp_sum_f64(double v) {
 }
 
 // src/Evaluator.cpp:44 then :88-91.
-__device__ __forceinline__ float fitness_from_sse(double sse, int64_t n_cases) {
-    const float mse = (float)(sse / (double)n_cases);
-    if (!isfinite(mse)) return 0.0f;
-    return __fdiv_rn(1.0f, __fadd_rn(1.0f, mse));
-}
 
 template <int NR, int K, int PROFILE, int REDUCE, int MODE, int DISPATCH>
 __global__ void __launch_bounds__(256, 1)
@@ -395,7 +393,7 @@ interp_kernel(InterpArgs args) {
             }
             if (lane == 0) {
                 if (args.n_chunks == 1) {
-                    args.fitness[prog] = fitness_from_sse(sse, args.N);
+                    args.fitness[prog] = fitness_of(sse, args.N, args.obj);
                     if (args.sse) args.sse[prog] = sse;
                 } else {
                     args.partial[prog * args.n_chunks + chunk] = sse;
@@ -513,6 +511,7 @@ interp_smem_kernel(InterpArgs args) {
         const float* __restrict__ yd;
         float* out_fitness;
         double* out_sse;
+        Objective obj;
         if (batched) {
             const unsigned long long it = args.items[item];
             prog = (int64_t)(it >> 20);
@@ -527,6 +526,7 @@ interp_smem_kernel(InterpArgs args) {
             cend = cbeg + d->chunk_cases;
             out_fitness = d->fitness;
             out_sse = d->sse;
+            obj = d->obj;
             out_index = prog - d->prog_base;
             if (d->n_chunks > 1) partial_index = (int64_t)item;
         } else {
@@ -542,6 +542,7 @@ interp_smem_kernel(InterpArgs args) {
             cend = cbeg + args.chunk_cases;
             out_fitness = args.fitness;
             out_sse = args.sse;
+            obj = args.obj;
             out_index = prog;
             if (args.n_chunks > 1) partial_index = prog * args.n_chunks + chunk;
         }
@@ -684,7 +685,7 @@ interp_smem_kernel(InterpArgs args) {
             else sse = acc;
             if (lane == 0) {
                 if (partial_index < 0) {
-                    out_fitness[out_index] = fitness_from_sse(sse, N);
+                    out_fitness[out_index] = fitness_of(sse, N, obj);
                     if (out_sse) out_sse[out_index] = sse;
                 } else {
                     args.partial[partial_index] = sse;

@@ -104,6 +104,7 @@ struct WideItem {
     const float* y;
     float* fitness;
     double* sse;
+    Objective obj;
 };
 
 __device__ __forceinline__ WideItem resolve_item(const InterpArgs& args, unsigned long long item) {
@@ -123,6 +124,7 @@ __device__ __forceinline__ WideItem resolve_item(const InterpArgs& args, unsigne
         w.cend = w.cbeg + d->chunk_cases;
         w.fitness = d->fitness;
         w.sse = d->sse;
+        w.obj = d->obj;
         w.out_index = w.prog - d->prog_base;
         if (d->n_chunks > 1) w.partial_index = (int64_t)item;
     } else {
@@ -138,6 +140,7 @@ __device__ __forceinline__ WideItem resolve_item(const InterpArgs& args, unsigne
         w.cend = w.cbeg + args.chunk_cases;
         w.fitness = args.fitness;
         w.sse = args.sse;
+        w.obj = args.obj;
         w.out_index = w.prog;
         if (args.n_chunks > 1) w.partial_index = w.prog * args.n_chunks + chunk;
     }
@@ -330,7 +333,7 @@ interp_wide_kernel(InterpArgs args) {
             else sse = acc;
             if (lane == 0) {
                 if (w.partial_index < 0) {
-                    w.fitness[w.out_index] = fitness_from_sse(sse, w.N);
+                    w.fitness[w.out_index] = fitness_of(sse, w.N, w.obj);
                     if (w.sse) w.sse[w.out_index] = sse;
                 } else {
                     args.partial[w.partial_index] = sse;

@@ -86,6 +86,7 @@ extern "C" int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32
     if (opt->num_registers != 8 && opt->num_registers != 16) return GALOP_E_INVALID;
     if (opt->profile != GALOP_PROFILE_REF && opt->profile != GALOP_PROFILE_BJ) return GALOP_E_INVALID;
     if (opt->reduce < GALOP_REDUCE_KAHAN32 || opt->reduce > GALOP_REDUCE_ORDERED) return GALOP_E_INVALID;
+    if (opt->objective != GALOP_OBJECTIVE_MSE) return GALOP_E_INVALID;   // R^2 needs the targets' ss_tot
     if (num_inputs < 0 || num_inputs > opt->num_registers) return GALOP_E_INVALID;
     if (padded_cases < n_cases || padded_cases % 1024 != 0 || padded_cases == 0) return GALOP_E_INVALID;
     if (n_programs > kNaMaxPrograms || total_words > kNaMaxWords) return GALOP_E_CAPACITY;
@@ -200,7 +201,7 @@ extern "C" int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32
     }
     if (n_chunks > 1)
         finalize_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(sc->partial, n, (int)n_chunks, n_cases,
-                                                                  d_fitness, d_sse);
+                                                                  Objective{}, d_fitness, d_sse);
     if (cudaGetLastError() != cudaSuccess) return GALOP_E_CUDA;
     return GALOP_OK;
 }

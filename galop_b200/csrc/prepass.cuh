@@ -18,6 +18,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "isa.cuh"
+#include "fitness.cuh"
 
 namespace galop {
 
@@ -272,14 +273,13 @@ static __global__ void dataset_transpose_kernel(const float* __restrict__ aos, c
 
 // Sum of chunk partials in chunk order, then fitness.
 static __global__ void finalize_kernel(const double* __restrict__ partial, int64_t n_programs,
-                                int n_chunks, int64_t n_cases, float* __restrict__ fitness,
+                                int n_chunks, int64_t n_cases, Objective obj, float* __restrict__ fitness,
                                 double* __restrict__ sse_out) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_programs) return;
     double s = 0.0;
     for (int c = 0; c < n_chunks; ++c) s += partial[i * n_chunks + c];
-    const float mse = (float)(s / (double)n_cases);
-    fitness[i] = isfinite(mse) ? __fdiv_rn(1.0f, __fadd_rn(1.0f, mse)) : 0.0f;
+    fitness[i] = fitness_of(s, n_cases, obj);
     if (sse_out) sse_out[i] = s;
 }
 

@@ -183,6 +183,7 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     a.num_inputs = ctx->num_inputs;
     a.output_reg = ctx->isa.output_reg;
     a.consts = ctx->pool;
+    a.obj = objective_for(ctx, ctx->ss_tot);
     a.counter = ctx->counters.p;
     a.fitness = d_fitness;
     a.sse = d_sse;
@@ -214,7 +215,7 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
 int finalize(galop_ctx* ctx, int64_t n, int32_t n_chunks, float* d_fitness, double* d_sse) {
     if (n_chunks <= 1 || n == 0) return GALOP_OK;
     finalize_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(
-        ctx->partial.p, n, n_chunks, ctx->N, d_fitness, d_sse);
+        ctx->partial.p, n, n_chunks, ctx->N, objective_for(ctx, ctx->ss_tot), d_fitness, d_sse);
     ctx->launches += 1;
     GALOP_CK(cudaGetLastError(), "finalize launch");
     return GALOP_OK;
@@ -328,6 +329,7 @@ int galop_create(const galop_options* opt, galop_ctx** out) {
     if (opt->num_registers != 8 && opt->num_registers != 16) return GALOP_E_INVALID;
     if (opt->profile != GALOP_PROFILE_REF && opt->profile != GALOP_PROFILE_BJ) return GALOP_E_INVALID;
     if (opt->reduce < GALOP_REDUCE_KAHAN32 || opt->reduce > GALOP_REDUCE_ORDERED) return GALOP_E_INVALID;
+    if (opt->objective != GALOP_OBJECTIVE_MSE && opt->objective != GALOP_OBJECTIVE_R2) return GALOP_E_INVALID;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -480,6 +482,18 @@ static int set_dataset_common(galop_ctx* ctx, const float* src_aos, const float*
     return GALOP_OK;
 }
 
+// ss_tot of targets already on the device (one copy to the host).
+static int device_ss_tot(galop_ctx* ctx, const float* d_targets, int64_t n_cases, double* out) {
+    *out = 0.0;
+    if (n_cases <= 0) return GALOP_OK;
+    std::vector<float> y((size_t)n_cases);
+    GALOP_CK(cudaMemcpyAsync(y.data(), d_targets, (size_t)n_cases * sizeof(float), cudaMemcpyDeviceToHost,
+                             ctx->stream), "D2H targets");
+    GALOP_CK(cudaStreamSynchronize(ctx->stream), "D2H targets");
+    *out = targets_ss_tot(y.data(), n_cases);
+    return GALOP_OK;
+}
+
 int galop_set_dataset(galop_ctx* ctx, const float* inputs, const float* targets, int64_t n_cases,
                       int32_t num_inputs) {
     if (!ctx) return GALOP_E_INVALID;
@@ -499,6 +513,7 @@ int galop_set_dataset(galop_ctx* ctx, const float* inputs, const float* targets,
     int rc = set_dataset_common(ctx, ctx->stage_aos.p, ctx->stage_y.p, n_cases, num_inputs);
     ctx->stage_aos.release();
     ctx->stage_y.release();
+    if (rc == GALOP_OK) ctx->ss_tot = targets_ss_tot(targets, n_cases);
     return rc;
 }
 
@@ -508,7 +523,12 @@ int galop_set_dataset_device(galop_ctx* ctx, const float* d_inputs, const float*
     if (n_cases < 0 || num_inputs < 0 || num_inputs > ctx->isa.num_registers)
         return ctx->fail(GALOP_E_INVALID, "bad dataset shape");
     GALOP_CK(cudaSetDevice(ctx->device), "set device");
-    return set_dataset_common(ctx, d_inputs, d_targets, n_cases, num_inputs);
+    double ss = 0.0;
+    if (ctx->opt.objective == GALOP_OBJECTIVE_R2)
+        if (int rc = device_ss_tot(ctx, d_targets, n_cases, &ss)) return rc;
+    if (int rc = set_dataset_common(ctx, d_inputs, d_targets, n_cases, num_inputs)) return rc;
+    ctx->ss_tot = ss;
+    return GALOP_OK;
 }
 
 }  // extern "C"

@@ -67,6 +67,16 @@ typedef enum {
     GALOP_REDUCE_ORDERED = 2
 } galop_reduce;
 
+/* Fitness of a program from its SSE over the N cases.
+ *   MSE : 1/(1 + mse), mse = float(sse/N), 0 if not finite
+ *         (src/Evaluator.cpp:44, Fitness::mse_to_fitness :88-91)
+ *   R2  : r2 = float(1 - sse/ss_tot), ss_tot = sum of (y - mean y)^2 over
+ *         the N cases in double, two passes in case order; 0 when
+ *         ss_tot <= 0 or sse is not finite (Evaluator::evaluate_sr_r2
+ *         src/Evaluator.cpp:49-85), then max(r2, 0), 0 if not finite
+ *         (Fitness::r2_to_fitness :93-97).                                  */
+typedef enum { GALOP_OBJECTIVE_MSE = 0, GALOP_OBJECTIVE_R2 = 1 } galop_objective;
+
 typedef struct {
     int32_t profile;          /* galop_profile                                  */
     int32_t num_registers;    /* 8 or 16 (src/LGPConfig.h:132-140)              */
@@ -86,7 +96,8 @@ typedef struct {
                                  micro-ops; 1 = lane registers behind PTX
                                  jump tables; 0 = lane registers behind C++
                                  switches.  All give identical results.     */
-    int32_t reserved[3];
+    int32_t objective;        /* galop_objective (default MSE)                  */
+    int32_t reserved[2];
 } galop_options;
 
 typedef struct galop_ctx galop_ctx;
@@ -125,6 +136,28 @@ GALOP_API void galop_destroy(galop_ctx* ctx);
 GALOP_API const char* galop_last_error(const galop_ctx* ctx);
 GALOP_API const char* galop_status_string(int status);
 GALOP_API int galop_abi_version(void);
+
+/* ---- CSV datasets ---------------------------------------------------------- */
+
+/* Replaces load_csv_1d (multi = 0) and load_csv_multi (multi = 1)
+ * (src/Dataset.cpp:83-151): reads a header line, then one case per
+ * non-empty line, into case-major inputs[c*num_inputs + i] and targets[c]
+ * (malloc'd; release with galop_csv_free), and the targets' total sum of
+ * squares (src/Dataset.cpp:35-47).  Numbers are read as std::stof reads
+ * them.  Returns GALOP_E_INVALID with a message in err (err_len bytes, may
+ * be NULL) for a missing file, a field that is not a float or is out of
+ * float range, or a ragged row.  Host only: no device is touched. */
+typedef struct {
+    float* inputs;
+    float* targets;
+    int64_t n_cases;
+    int32_t num_inputs;
+    int32_t reserved;
+    double ss_tot;
+} galop_csv_dataset;
+
+GALOP_API int galop_csv_read(const char* path, int32_t multi, galop_csv_dataset* out, char* err, int32_t err_len);
+GALOP_API void galop_csv_free(galop_csv_dataset* d);
 
 /* ---- autotuner ----------------------------------------------------------- */
 

@@ -233,6 +233,55 @@ float orc_mse_to_fitness(float mse) {
     return 1.0f / (1.0f + mse);
 }
 
+/* Two-pass total sum of squares of the targets, each pass a double sum in
+ * case order (compute_ss_tot, src/Dataset.cpp:35-47). */
+double orc_ss_tot(const float* targets, int64_t n) {
+    if (n <= 0) return 0.0;
+    double mean = 0.0;
+    for (int64_t i = 0; i < n; ++i) mean += (double)targets[i];
+    mean /= (double)n;
+    double ss = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double d = (double)targets[i] - mean;
+        ss += d * d;
+    }
+    return ss;
+}
+
+/* R^2 of one program (Evaluator::evaluate_sr_r2, src/Evaluator.cpp:49-85):
+ * 0 for a degenerate target (ss_tot <= 0) or a non-finite SSE, else
+ * float(1 - sse/ss_tot); the SSE is the same case-order sum as the MSE's. */
+float orc_evaluate_sr_r2(const orc_isa_t* isa, const uint32_t* prog, int64_t len,
+                         const float* inputs, const float* targets, int num_inputs,
+                         int64_t n_cases, double ss_tot) {
+    if (ss_tot <= 0.0) return 0.0f;
+    const double sse = orc_sse(isa, prog, len, inputs, targets, num_inputs, n_cases);
+    if (!isfinite(sse)) return 0.0f;
+    return (float)(1.0 - sse / ss_tot);
+}
+
+/* src/Evaluator.cpp:93-97. */
+float orc_r2_to_fitness(float r2) {
+    if (!isfinite(r2)) return 0.0f;
+    return r2 < 0.0f ? 0.0f : r2;
+}
+
+/* R^2 fitness of CSR programs, as orc_evaluate_population_csr. */
+void orc_evaluate_population_csr_r2(const orc_isa_t* isa, const uint32_t* words,
+                                    const int64_t* offsets, int64_t n_programs,
+                                    const float* inputs, const float* targets, int num_inputs,
+                                    int64_t n_cases, float* fitness_out, int threads) {
+    const double ss_tot = orc_ss_tot(targets, n_cases);
+#ifdef _OPENMP
+    if (threads < 1) threads = omp_get_max_threads();
+    #pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
+#endif
+    for (int64_t i = 0; i < n_programs; ++i)
+        fitness_out[i] = orc_r2_to_fitness(orc_evaluate_sr_r2(isa, words + offsets[i], offsets[i + 1] - offsets[i],
+                                                              inputs, targets, num_inputs, n_cases, ss_tot));
+    (void)threads;
+}
+
 /* Population evaluation over CSR programs: program i is
  * words[offsets[i] : offsets[i+1]].  The loop over programs follows
  * src/EvaluatorCpu.cpp:7-15; `threads` > 1 runs it as an OpenMP parallel for

@@ -83,6 +83,12 @@ class Oracle:
                 "orc_extract_effective": (_I64, [P(OrcIsa), P(_U32), _I64, P(_U32)]),
                 "orc_effective_lengths_csr": (None, [P(OrcIsa), P(_U32), P(_I64), _I64, P(_I64)]),
                 "orc_max_threads": (C.c_int, []),
+                "orc_ss_tot": (C.c_double, [P(_F32), _I64]),
+                "orc_evaluate_sr_r2": (C.c_float, [P(OrcIsa), P(_U32), _I64, P(_F32), P(_F32), C.c_int, _I64,
+                                                   C.c_double]),
+                "orc_r2_to_fitness": (C.c_float, [C.c_float]),
+                "orc_evaluate_population_csr_r2": (None, [P(OrcIsa), P(_U32), P(_I64), _I64, P(_F32), P(_F32),
+                                                          C.c_int, _I64, P(_F32), C.c_int]),
             }
             for name, (res, args) in sig.items():
                 fn = getattr(lib, name)
@@ -153,6 +159,24 @@ class Oracle:
                                                inputs.shape[0], _p(fit, _F32), _p(sse, _F64), threads)
         return (fit, sse) if with_sse else fit
 
+    def evaluate_csr_r2(self, words, offsets, inputs, targets, threads: int = 0):
+        """R^2 fitness (src/Evaluator.cpp:49-97) of CSR programs."""
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        inputs = np.ascontiguousarray(inputs, dtype=np.float32)
+        targets = np.ascontiguousarray(targets, dtype=np.float32)
+        n = offsets.shape[0] - 1
+        fit = np.empty(n, dtype=np.float32)
+        self.lib().orc_evaluate_population_csr_r2(C.byref(self.isa), _p(words, _U32), _p(offsets, _I64), n,
+                                                  _p(inputs, _F32), _p(targets, _F32), inputs.shape[1],
+                                                  inputs.shape[0], _p(fit, _F32), threads)
+        return fit
+
+    @staticmethod
+    def ss_tot(targets) -> float:
+        targets = np.ascontiguousarray(targets, dtype=np.float32)
+        return Oracle.lib().orc_ss_tot(_p(targets, _F32), targets.shape[0])
+
     def effective_lengths(self, words, offsets) -> np.ndarray:
         words = np.ascontiguousarray(words, dtype=np.uint32)
         offsets = np.ascontiguousarray(offsets, dtype=np.int64)
@@ -193,6 +217,10 @@ class RefLib:
                                         P(_F32), C.c_int]),
             "ref_effective_mask": (C.c_int, [P(_U32), C.c_int, C.c_char_p]),
             "ref_max_threads": (C.c_int, []),
+            "ref_evaluate_csr_r2": (None, [P(_U32), P(_I64), _I64, P(_F32), P(_F32), C.c_int, C.c_int, C.c_double,
+                                           P(_F32), P(_F32)]),
+            "ref_load_csv": (C.c_int, [C.c_char_p, C.c_int, P(_I64), P(C.c_int), P(_F32), P(_F32),
+                                       P(C.c_double)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -260,6 +288,31 @@ class RefLib:
         self.lib.ref_evaluate_csr(_p(words, _U32), _p(offsets, _I64), n, _p(inputs, _F32), _p(targets, _F32),
                                   inputs.shape[0], inputs.shape[1], _p(fit, _F32), _p(mse, _F32), threads)
         return (fit, mse) if with_mse else fit
+
+    def evaluate_csr_r2(self, words, offsets, inputs, targets, ss_tot: float, with_r2: bool = False):
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        inputs = np.ascontiguousarray(inputs, dtype=np.float32)
+        targets = np.ascontiguousarray(targets, dtype=np.float32)
+        n = offsets.shape[0] - 1
+        fit = np.empty(n, dtype=np.float32)
+        r2 = np.empty(n, dtype=np.float32)
+        self.lib.ref_evaluate_csr_r2(_p(words, _U32), _p(offsets, _I64), n, _p(inputs, _F32), _p(targets, _F32),
+                                     inputs.shape[0], inputs.shape[1], ss_tot, _p(fit, _F32), _p(r2, _F32))
+        return (fit, r2) if with_r2 else fit
+
+    def load_csv(self, path, multi: bool = False):
+        """The reference's load_csv_1d / load_csv_multi: (inputs (N, k),
+        targets (N,), ss_tot), or None when it throws."""
+        n, k, ss = _I64(0), C.c_int(0), C.c_double(0.0)
+        if self.lib.ref_load_csv(str(path).encode(), int(bool(multi)), C.byref(n), C.byref(k), None, None,
+                                 C.byref(ss)) != 0:
+            return None
+        X = np.empty((n.value, k.value), dtype=np.float32)
+        y = np.empty(n.value, dtype=np.float32)
+        self.lib.ref_load_csv(str(path).encode(), int(bool(multi)), C.byref(n), C.byref(k), _p(X, _F32),
+                              _p(y, _F32), C.byref(ss))
+        return X, y, ss.value
 
     def effective_mask(self, prog) -> np.ndarray:
         prog = np.ascontiguousarray(prog, dtype=np.uint32)

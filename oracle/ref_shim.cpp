@@ -115,6 +115,41 @@ void ref_evaluate_csr(const uint32_t* words, const int64_t* offsets, int64_t n, 
     (void)threads;
 }
 
+// Evaluator::evaluate_sr_r2 + Fitness::r2_to_fitness (src/Evaluator.cpp:49-97)
+// with the dataset's ss_tot given (as the reference's loaders compute it).
+void ref_evaluate_csr_r2(const uint32_t* words, const int64_t* offsets, int64_t n, const float* inputs,
+                         const float* targets, int n_cases, int num_inputs, double ss_tot, float* fitness,
+                         float* r2_out) {
+    Dataset d = make_dataset(inputs, targets, n_cases, num_inputs);
+    d.ss_tot = ss_tot;
+    for (int64_t i = 0; i < n; ++i) {
+        ProgramView pv{words + offsets[i], (int)(offsets[i + 1] - offsets[i])};
+        const float r2 = Evaluator::evaluate_sr_r2(pv, d);
+        if (r2_out) r2_out[i] = r2;
+        fitness[i] = Fitness::r2_to_fitness(r2);
+    }
+}
+
+// load_csv_1d / load_csv_multi (src/Dataset.cpp:83-151).  With inputs ==
+// NULL only the sizes and ss_tot are returned; call again with buffers of
+// n*k and n floats.  -1 when the reference's loader throws.
+int ref_load_csv(const char* path, int multi, int64_t* n, int* k, float* inputs, float* targets,
+                 double* ss_tot) {
+    try {
+        const Dataset d = multi ? load_csv_multi(path) : load_csv_1d(path);
+        *n = d.N;
+        *k = d.num_inputs;
+        *ss_tot = d.ss_tot;
+        if (inputs)
+            for (int64_t i = 0; i < (int64_t)d.N * d.num_inputs; ++i) inputs[i] = d.inputs[i];
+        if (targets)
+            for (int64_t i = 0; i < d.N; ++i) targets[i] = d.targets[i];
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
 // Introns::effective_mask (src/Introns.h:28-46).
 int ref_effective_mask(const uint32_t* prog, int len, char* mask) {
     return Introns::effective_mask(prog, len, mask);

@@ -106,3 +106,25 @@ def test_batch_capacity_is_enforced(native):
             with pytest.raises(g.GalopError) as e:
                 b.set_population(0, w, o)
             assert e.value.status == g.E_CAPACITY
+
+
+def test_batch_r2_objective_matches_single_population_calls(native):
+    """Each population's R^2 uses its own dataset's ss_tot.  Targets are
+    the first input plus noise, and every population starts with an empty
+    program (its output register is that input), so R^2 > 0 occurs."""
+    rng = np.random.default_rng(1)
+    pops = []
+    for ds, w, o in _populations(5, SPECS[:4]):
+        x0 = ds.inputs[:, 0].astype(np.float64)
+        y = (x0 + rng.normal(0, 0.1, x0.shape)).astype(np.float32)
+        pops.append((g.Dataset(ds.inputs, y), w, np.concatenate([[0], o]).astype(np.int64)))
+    with g.Evaluator(num_registers=16, reduce=g.REDUCE_ORDERED, objective=g.OBJECTIVE_R2) as ev:
+        single = [ev.evaluate_csr(w, o, ds) for ds, w, o in pops]
+        rds = [g.ResidentDataset(ev, ds) for ds, _, _ in pops]
+        with g.Batch(ev, [(r, o.shape[0] - 1, int(o[-1])) for r, (_, _, o) in zip(rds, pops)]) as b:
+            for p, (_, w, o) in enumerate(pops):
+                b.set_population(p, w, o)
+            b.evaluate()
+            for p in range(len(pops)):
+                assert np.array_equal(bits(b.fitness(p)), bits(single[p])), p
+    assert all(f[0] > 0.9 for f in single)

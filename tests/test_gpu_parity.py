@@ -14,6 +14,8 @@ Bar (the same one the C ABI header states):
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -373,3 +375,58 @@ def test_kahan32_survives_errors_beyond_float_square_range(native):
     assert fin.sum() >= 4 and (so[fin] > 3.4e38).any()
     assert np.all(np.abs(sk[fin] - so[fin]) <= 1e-6 * so[fin])
     assert np.all(np.abs(fk.astype(np.float64) - fo) <= 1e-6 * np.maximum(fo, 1e-45))
+
+
+# --- the R^2 objective -------------------------------------------------------------------
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+def test_r2_objective_against_oracle(native, orc, variant):
+    """R^2 fitness (src/Evaluator.cpp:49-97): ORDERED bit-identical to the C
+    restatement (itself pinned to the reference) for IEEE-only programs;
+    KAHAN32 within 1e-6; a constant target gives fitness 0."""
+    v = load_vectors(variant)
+    nr, ip = VARIANTS[variant]
+    o = orc.Oracle(orc.PROFILE_REF, nr, ip)
+    words, off = v["words"], v["offsets"]
+    n = len(off) - 1
+    ieee = np.array([program_is_ieee(o, words[off[i]:off[i + 1]], g.PROFILE_REF) for i in range(n)])
+    with g.Evaluator(num_registers=nr, input_protect=ip, reduce=g.REDUCE_ORDERED, objective=g.OBJECTIVE_R2) as ev, \
+            g.Evaluator(num_registers=nr, input_protect=ip, objective=g.OBJECTIVE_R2) as ek:
+        for d in ("d1", "d2", "d3", "d4"):
+            X, y = v[f"{d}_X"], v[f"{d}_y"]
+            ds = g.Dataset(X, y)
+            want = o.evaluate_csr_r2(words, off, X, y)
+            got = ev.evaluate_csr(words, off, ds)
+            assert np.array_equal(bits(got)[ieee], bits(want)[ieee]), d
+            fk = ek.evaluate_csr(words, off, ds)
+            assert np.abs(fk.astype(np.float64) - want)[ieee].max() <= 1e-6, d
+        flat = g.Dataset(v["d1_X"], np.full_like(v["d1_y"], 2.5))
+        assert not ev.evaluate_csr(words, off, flat).any()
+        # device-resident dataset: ss_tot is taken from the device copy of the targets
+        X, y = np.ascontiguousarray(v["d2_X"]), np.ascontiguousarray(v["d2_y"])
+        dx, dy = ev.device_alloc(max(X.nbytes, 4)), ev.device_alloc(max(y.nbytes, 4))
+        try:
+            ev.h2d(dx, X)
+            ev.h2d(dy, y)
+            ev._check(ev._lib.galop_set_dataset_device(ev.handle, dx, dy, X.shape[0], X.shape[1]))
+            ev.dataset = None
+            ev._dataset_key = None
+            fit = np.empty(n, np.float32)
+            ev._check(ev._lib.galop_evaluate_csr(ev.handle, words.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                                 off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), n,
+                                                 fit.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), None))
+            want = o.evaluate_csr_r2(words, off, X, y)
+            assert np.array_equal(bits(fit)[ieee], bits(want)[ieee])
+        finally:
+            ev.device_free(dx)
+            ev.device_free(dy)
+
+
+def test_r2_objective_is_refused_without_allocation(native):
+    opt = g._Options()
+    lib = g.load_library()
+    lib.galop_options_init(ctypes.byref(opt))
+    opt.objective = g.OBJECTIVE_R2
+    rc = lib.galop_evaluate_csr_noalloc(ctypes.byref(opt), None, ctypes.c_void_p(1), 0, 0, None, None, 0, 1024,
+                                        1, None, None, None)
+    assert rc == g.E_INVALID
