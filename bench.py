@@ -61,10 +61,15 @@ def parse():
     ap.add_argument("--reduce", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "stream"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "stream", "evo"],
                     help="single: the headline single-generation workload; batch: many populations in one "
                          "persistent launch per generation (graph replay) vs one plain launch per population; "
-                         "serve: continuous batching of Poisson-arriving GP runs; stream: 2^20-case dataset")
+                         "serve: continuous batching of Poisson-arriving GP runs; stream: 2^20-case dataset; "
+                         "evo: a whole 100-generation run of the reference engine with this backend, beside "
+                         "the reference's own whole-run benchmark on the same GPU")
+    ap.add_argument("--evo-pop", type=int, default=100000, choices=[10000, 100000, 1000000])
+    ap.add_argument("--evo-cases", type=int, default=1024)
+    ap.add_argument("--evo-seed", type=int, default=70)
     ap.add_argument("--scale", type=float, default=1.0 / 32,
                     help="population-size scale of the batch/serve/stream workloads")
     return ap.parse_args()
@@ -567,6 +572,68 @@ def run_stream(args):
     print(json.dumps(line), flush=True)
 
 
+def evo_dataset(path: Path, n_cases: int):
+    """The reference speed grid's synthetic cell: x ~ U(-1,1) from Python's
+    random seeded with 1234, y = x^4 + x^3 + x^2 + x, header "x,y"."""
+    import random
+    rnd = random.Random(1234)
+    with open(path, "w") as f:
+        f.write("x,y\n")
+        for _ in range(n_cases):
+            x = rnd.uniform(-1, 1)
+            f.write(f"{x},{x**4 + x**3 + x**2 + x}\n")
+
+
+def parse_evo(out: str, err: str, name: str) -> dict:
+    row = next(line for line in out.splitlines() if line.startswith(name + ","))
+    f = row.split(",")
+    r = {"pop": int(f[1]), "cases": int(f[2]), "generations": int(f[3]), "mean_length": float(f[4]),
+         "seconds": float(f[5]), "raw_gpops": float(f[6]) / 1e9, "best_mse": float(f[7])}
+    for line in err.splitlines():
+        if line.startswith("BREAKDOWN"):
+            e = line.split("eval=")[1].split("s")[0]
+            r["eval_seconds"] = float(e)
+    return r
+
+
+def run_evo(args):
+    """A whole evolutionary run (reference LGPEngine, GALOP_STANDARD settings,
+    100 generations, selection and variation on the host) with this backend,
+    and the reference's own whole-run benchmark (its CudaEvaluator, warp
+    strategy, built for sm_100a) on the same cell, same seed."""
+    P, D, seed = args.evo_pop, args.evo_cases, args.evo_seed
+    ours_bin = ROOT / "galop_b200" / "drivers" / "_bin" / f"evo_b200_P{P}"
+    with tempfile.TemporaryDirectory() as td:
+        csv = Path(td) / f"grid_D{D}.csv"
+        evo_dataset(csv, D)
+        env = dict(os.environ, OMP_NUM_THREADS=str(min(16, os.cpu_count() or 1)))
+        p = subprocess.run([str(ours_bin), str(csv), str(seed)], capture_output=True, text=True, env=env,
+                           timeout=3000)
+        if p.returncode != 0:
+            raise RuntimeError(f"{ours_bin.name} failed: {p.stderr[-400:]}")
+        ours = parse_evo(p.stdout, p.stderr, "b200")
+        ref = None
+        if not args.no_cpu_baseline:
+            # baseline leg: the reference's own whole-run benchmark, same GPU
+            ref_bin = ROOT / "oracle" / "_ref" / f"cuda_evo_bench_P{P}"
+            if ref_bin.exists():
+                q = subprocess.run([str(ref_bin), str(csv), str(seed), "warp"], capture_output=True, text=True,
+                                   env=env, timeout=3000)
+                ref = parse_evo(q.stdout, q.stderr, "warp") if q.returncode == 0 else \
+                    {"unavailable": q.stderr[-300:]}
+            else:
+                ref = {"unavailable": f"{ref_bin.name} not built"}
+    line = {"metric": "raw GPop/s of a whole 100-generation run (P x mean length x D per generation / wall s)",
+            "value": ours["raw_gpops"], "unit": "GPop/s", "workload": "evo", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded; the reference speed grid's cell)",
+            "config": {"workload": f"reference LGPEngine, GALOP_STANDARD, P={P}, D={D}, 100 generations, seed {seed}; "
+                                   "selection and variation on the host, evaluation by this backend"},
+            "b200": ours, "reference_whole_run_same_b200": ref}
+    if ref and "seconds" in ref:
+        line["speedup_vs_reference_whole_run"] = ref["seconds"] / ours["seconds"]
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     dist = Dist()
@@ -579,6 +646,8 @@ def main():
             run_serve(args)
         elif args.workload == "stream":
             run_stream(args)
+        elif args.workload == "evo":
+            run_evo(args)
         else:
             run_b200(args, dist)
     finally:
