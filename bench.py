@@ -61,12 +61,13 @@ def parse():
     ap.add_argument("--reduce", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "stream", "evo"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "stream", "evo", "capacity"],
                     help="single: the headline single-generation workload; batch: many populations in one "
                          "persistent launch per generation (graph replay) vs one plain launch per population; "
                          "serve: continuous batching of Poisson-arriving GP runs; stream: 2^20-case dataset; "
                          "evo: a whole 100-generation run of the reference engine with this backend, beside "
-                         "the reference's own whole-run benchmark on the same GPU")
+                         "the reference's own whole-run benchmark on the same GPU; capacity: the largest "
+                         "device-resident population that evaluates, and its footprint per program")
     ap.add_argument("--evo-pop", type=int, default=100000, choices=[10000, 100000, 1000000])
     ap.add_argument("--evo-cases", type=int, default=1024)
     ap.add_argument("--evo-seed", type=int, default=70)
@@ -634,6 +635,96 @@ def run_evo(args):
     print(json.dumps(line), flush=True)
 
 
+def run_capacity(args):
+    """Largest device-resident population that evaluates (SURVEY §8(f) item 2,
+    after tests/cuda_capacity.cu): random-word programs of 30 instructions
+    (the reference probe's evolved shape; ~16% effective), 8 registers, a
+    32-case dataset, populations generated on the device (no host copy).
+    The footprint per program is measured on 2^22 programs (caller's words,
+    offsets and fitness plus the evaluator's buffers), the largest population
+    that fits in 92% of the free memory (and in int32 program indices) is
+    then allocated and evaluated once as the proof, and twice more timed."""
+    import torch
+    import galop_b200 as g
+    L, D = 30, 32
+    rng = np.random.default_rng(1234)
+    x = rng.uniform(-1, 1, (D, 1)).astype(np.float32)
+    y = (x[:, 0] ** 3 + x[:, 0] ** 2 + x[:, 0]).astype(np.float32)
+    ds = g.Dataset(x, y)
+    dev = torch.device("cuda", 0)
+    free0, total_mem = torch.cuda.mem_get_info(dev)
+    rows = []
+
+    def population(P):
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(7)
+        w = torch.randint(-2**31, 2**31 - 1, (P * L,), dtype=torch.int32, device=dev, generator=gen)
+        off = torch.arange(P + 1, dtype=torch.int64, device=dev) * L
+        fit = torch.empty(P, dtype=torch.float32, device=dev)
+        return w, off, fit
+
+    for dispatch in (3, 2):
+        # footprint per program from a 2^22-program population
+        P0 = 1 << 22
+        torch.cuda.synchronize()
+        before = torch.cuda.mem_get_info(dev)[0]
+        ev = g.Evaluator(num_registers=8, dispatch=dispatch)
+        ev.set_dataset(ds)
+        w, off, fit = population(P0)
+        ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P0, fit.data_ptr())
+        ev.synchronize()
+        used = before - torch.cuda.mem_get_info(dev)[0]
+        per_prog = used / P0
+        del w, off, fit
+        ev.close()
+        torch.cuda.empty_cache()
+        free_now = torch.cuda.mem_get_info(dev)[0]
+        P = int(min(2**31 - 1, 0.92 * free_now / per_prog))
+        row = {"dispatch": dispatch, "bytes_per_program": round(per_prog, 1), "max_programs": P}
+        for attempt in range(3):
+            try:
+                ev = g.Evaluator(num_registers=8, dispatch=dispatch)
+                ev.set_dataset(ds)
+                w, off, fit = population(P)
+                ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, fit.data_ptr())   # the proof
+                ev.synchronize()
+                ms = []
+                for _ in range(2):
+                    ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, fit.data_ptr())
+                    st = ev.stats
+                    ms.append(st.prepass_ms + st.interp_ms + st.finalize_ms)
+                st = ev.stats
+                row.update({"max_programs": P, "evaluated": True, "eval_ms": min(ms),
+                            "device_used_gb": round((free0 - torch.cuda.mem_get_info(dev)[0]) / 1e9, 1),
+                            "raw_gpops": float(P) * L * D / (min(ms) / 1e3) / 1e9,
+                            "eff_fraction": st.eff_instructions / max(st.raw_instructions, 1)})
+                del w, off, fit
+                ev.close()
+                torch.cuda.empty_cache()
+                break
+            except (g.GalopError, torch.OutOfMemoryError) as e:
+                row.setdefault("retries", []).append(f"P={P}: {e}")
+                try:
+                    del w, off, fit
+                except NameError:
+                    pass
+                try:
+                    ev.close()
+                except Exception:
+                    pass
+                torch.cuda.empty_cache()
+                P = int(P * 0.85)
+        rows.append(row)
+    line = {"metric": "largest device-resident population evaluated (programs)",
+            "value": max(r["max_programs"] for r in rows if r.get("evaluated")), "unit": "programs",
+            "workload": "capacity", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (random words generated on the device)",
+            "config": {"workload": f"programs of {L} random words, 8 registers, {D} cases, intron pass on; "
+                                   f"device memory {total_mem / 1e9:.1f} GB, free at start {free0 / 1e9:.1f} GB"},
+            "by_dispatch": rows}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     dist = Dist()
@@ -648,6 +739,8 @@ def main():
             run_stream(args)
         elif args.workload == "evo":
             run_evo(args)
+        elif args.workload == "capacity":
+            run_capacity(args)
         else:
             run_b200(args, dist)
     finally:

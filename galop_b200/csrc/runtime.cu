@@ -111,9 +111,21 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
         GALOP_CK(cudaMemsetAsync(ctx->eff_off.p, 0, sizeof(int64_t), s), "memset eff_off");
     }
     GALOP_CK(cudaGetLastError(), "pre-pass count/scan launch");
-    // Device buffer for micro-ops sized by the raw total (an upper bound).
+    // Device buffer for the micro-ops.  The raw total bounds the effective
+    // total; when the buffer is smaller than that bound, read the effective
+    // total (the scan's last offset) and size the buffer for exactly that, so
+    // the footprint follows the interpreted instructions, not the raw ones.
     const UopFormat fmt = uop_format(ctx);
-    GALOP_CK(ctx->uops.ensure((size_t)std::max<int64_t>(raw_words_total, 1) * (fmt.wide ? 4 : 1)), "alloc uops");
+    const size_t per = fmt.wide ? 4 : 1;
+    if (ctx->uops.cap < (size_t)std::max<int64_t>(raw_words_total, 1) * per) {
+        int64_t eff_total = raw_words_total;
+        if (strip && n > 0) {
+            GALOP_CK(cudaMemcpyAsync(&eff_total, ctx->eff_off.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s),
+                     "D2H effective total");
+            GALOP_CK(cudaStreamSynchronize(s), "effective total");
+        }
+        GALOP_CK(ctx->uops.ensure((size_t)std::max<int64_t>(eff_total, 1) * per), "alloc uops");
+    }
     if (n > 0) {
         prepass_compact_kernel<Src><<<blocks, tpb, 0, s>>>(src, n, ctx->isa, strip ? 1 : 0,
                                                            ctx->eff_off.p, ctx->uops.p, raw_out, fmt);
@@ -609,6 +621,7 @@ int galop_evaluate_csr_device(galop_ctx* ctx, const uint32_t* d_words, const int
                               int64_t n_programs, float* d_fitness, double* d_sse, void* stream) {
     if (int rc = check_ready(ctx)) return rc;
     if (n_programs < 0 || !d_offsets) return ctx->fail(GALOP_E_INVALID, "bad arguments");
+    if (n_programs > INT32_MAX) return ctx->fail(GALOP_E_CAPACITY, "n_programs > 2^31-1");
     if (n_programs > 0 && (!d_words || !d_fitness)) return ctx->fail(GALOP_E_INVALID, "null pointer");
     GALOP_CK(cudaSetDevice(ctx->device), "set device");
     begin_call(ctx, n_programs);
