@@ -59,6 +59,8 @@ EXPORTED = (
     "galop_batch_append", "galop_batch_population_work", "galop_server_options_init", "galop_server_create",
     "galop_server_destroy", "galop_server_open_run", "galop_server_close_run", "galop_server_submit",
     "galop_server_wait", "galop_server_stats", "galop_autotune", "galop_csv_read", "galop_csv_free",
+    "galop_engine_options_init", "galop_engine_create", "galop_engine_destroy", "galop_engine_evolve",
+    "galop_engine_population", "galop_engine_times_get",
 )
 
 
@@ -75,6 +77,26 @@ class _Options(C.Structure):
 class _CsvDataset(C.Structure):
     _fields_ = [("inputs", C.POINTER(C.c_float)), ("targets", C.POINTER(C.c_float)), ("n_cases", C.c_int64),
                 ("num_inputs", C.c_int32), ("reserved", C.c_int32), ("ss_tot", C.c_double)]
+
+
+class _EngineOptions(C.Structure):
+    _fields_ = [("population", C.c_int64), ("max_program_size", C.c_int32), ("starting_program_size", C.c_int32),
+                ("max_generations", C.c_int32), ("elite_count", C.c_int32), ("tournament_size", C.c_int32),
+                ("macro_inserts", C.c_int32), ("effmut", C.c_int32), ("macro_random_pos", C.c_int32),
+                ("crossover_rate", C.c_float), ("micro_rate", C.c_float), ("micro_per_instr", C.c_float),
+                ("effmut_rate", C.c_float), ("insert_tail_rate", C.c_float), ("delete_tail_rate", C.c_float),
+                ("seed", C.c_uint32), ("reserved", C.c_int32 * 3)]
+
+
+class GenerationStats(C.Structure):
+    """GenerationStats (src/GenerationStats.h)."""
+    _fields_ = [("generation", C.c_int32), ("best_fitness", C.c_float), ("mean_fitness", C.c_float),
+                ("best_length", C.c_int32), ("mean_length", C.c_float), ("best_index", C.c_int32)]
+
+
+class EngineTimes(C.Structure):
+    _fields_ = [("total_s", C.c_double), ("init_s", C.c_double), ("evaluate_s", C.c_double),
+                ("select_vary_s", C.c_double), ("stats_s", C.c_double), ("eff_instructions", C.c_int64)]
 
 
 class TuneResult(C.Structure):
@@ -167,6 +189,12 @@ def load_library(path: Optional[Path] = None) -> C.CDLL:
         "galop_last_stats": (C.c_int, [_P, C.POINTER(Stats)]),
         "galop_csv_read": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(_CsvDataset), C.c_char_p, C.c_int32]),
         "galop_csv_free": (None, [C.POINTER(_CsvDataset)]),
+        "galop_engine_options_init": (C.c_int, [C.POINTER(_EngineOptions)]),
+        "galop_engine_create": (C.c_int, [_P, C.POINTER(_EngineOptions), C.POINTER(_P)]),
+        "galop_engine_destroy": (C.c_int, [_P]),
+        "galop_engine_evolve": (C.c_int, [_P, C.POINTER(GenerationStats), C.c_int32]),
+        "galop_engine_population": (C.c_int, [_P, _U32P, _U8P, _F32P]),
+        "galop_engine_times_get": (C.c_int, [_P, C.POINTER(EngineTimes)]),
         "galop_autotune": (C.c_int, [_P, _U32P, _I64P, C.c_int64, C.c_int64, C.c_int32, C.c_char_p,
                                      C.POINTER(TuneResult)]),
         "galop_synchronize": (C.c_int, [_P]),
@@ -696,6 +724,68 @@ class Server:
     def close(self):
         if self._h and self._h.value:
             self.evaluator._lib.galop_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Engine:
+    """LGPEngine::evolve_sr with the population resident on the GPU
+    (galop_engine_*).  Keyword arguments are galop_engine_options fields;
+    the defaults are the reference's default LGPConfig.  The ISA, constants
+    and reduction are the evaluator's."""
+
+    def __init__(self, ev: "Evaluator", **options):
+        self._ev = ev
+        self._lib = ev._lib
+        o = _EngineOptions()
+        self._lib.galop_engine_options_init(C.byref(o))
+        if "population" in options and "elite_count" not in options:
+            options["elite_count"] = int(np.float32(options["population"]) * np.float32(0.1))
+        for k, v in options.items():
+            if not hasattr(o, k):
+                raise TypeError(f"unknown engine option {k}")
+            setattr(o, k, v)
+        self.options = o
+        self._h = C.c_void_p()
+        ev._check(self._lib.galop_engine_create(ev.handle, C.byref(o), C.byref(self._h)))
+
+    def evolve(self, dataset: Optional[Dataset] = None):
+        """Run init + max_generations; returns the history as a list of
+        GenerationStats rows."""
+        self._ev._ensure_dataset(dataset)
+        hist = (GenerationStats * self.options.max_generations)()
+        self._ev._check(self._lib.galop_engine_evolve(self._h, hist, len(hist)))
+        return list(hist)
+
+    def population(self):
+        P, L = int(self.options.population), int(self.options.max_program_size)
+        w = np.empty(P * L, np.uint32)
+        ln = np.empty(P, np.uint8)
+        f = np.empty(P, np.float32)
+        self._ev._check(self._lib.galop_engine_population(self._h, _ptr(w, C.c_uint32), _ptr(ln, C.c_uint8),
+                                                          _ptr(f, C.c_float)))
+        return w.reshape(P, L), ln, f
+
+    @property
+    def times(self) -> EngineTimes:
+        t = EngineTimes()
+        self._lib.galop_engine_times_get(self._h, C.byref(t))
+        return t
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.galop_engine_destroy(self._h)
             self._h = C.c_void_p()
 
     def __enter__(self):

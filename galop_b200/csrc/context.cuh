@@ -130,6 +130,8 @@ const void* kernel_for(const galop_ctx* ctx, int k, int mode);
 int pick_dispatch(const galop_ctx* ctx);
 UopFormat uop_format(const galop_ctx* ctx);
 size_t interp_smem_bytes(const galop_ctx* ctx, int k, int wpb);
+int evaluate_dense_device(galop_ctx* ctx, const uint32_t* d_words, const uint8_t* d_lens, int64_t stride,
+                          int64_t n, float* d_fitness);
 const void* interp_kernel_nr8(int k, int dispatch, int profile, int reduce, int mode);
 const void* interp_kernel_nr16(int k, int dispatch, int profile, int reduce, int mode);
 }  // namespace galop

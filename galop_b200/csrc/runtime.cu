@@ -272,6 +272,36 @@ int end_call(galop_ctx* ctx) {
     return finish_stats(ctx);
 }
 
+}  // namespace
+
+namespace galop {
+
+// n device-resident programs in the dense layout (program i at
+// d_words + i*stride, d_lens[i] instructions) into d_fitness, on the
+// context's stream, synchronously; stats as the other evaluate calls.
+int evaluate_dense_device(galop_ctx* ctx, const uint32_t* d_words, const uint8_t* d_lens, int64_t stride,
+                          int64_t n, float* d_fitness) {
+    if (int rc = check_ready(ctx)) return rc;
+    begin_call(ctx, n);
+    cudaStream_t s = ctx->stream;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], s), "event");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvH2D], s), "event");
+    DenseSource src{d_words, d_lens, stride};
+    if (int rc = run_prepass(ctx, src, n, n * stride, ctx->opt.intron_prepass != 0, true, nullptr)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvPrepass], s), "event");
+    int32_t chunks = 1;
+    if (int rc = run_interp(ctx, n, kModeFitness, true, d_fitness, nullptr, nullptr, nullptr, &chunks)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvInterp], s), "event");
+    if (int rc = finalize(ctx, n, chunks, d_fitness, nullptr)) return rc;
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvFinalize], s), "event");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvD2H], s), "event");
+    return end_call(ctx);
+}
+
+}  // namespace galop
+
+namespace {
+
 int validate_offsets(galop_ctx* ctx, const int64_t* off, int64_t n) {
     if (off[0] != 0) return ctx->fail(GALOP_E_INVALID, "offsets[0] must be 0 (got %lld)", (long long)off[0]);
     for (int64_t i = 0; i < n; ++i) {

@@ -137,6 +137,75 @@ GALOP_API const char* galop_last_error(const galop_ctx* ctx);
 GALOP_API const char* galop_status_string(int status);
 GALOP_API int galop_abi_version(void);
 
+/* ---- the evolution loop on the device ------------------------------------ */
+
+/* Replaces LGPEngine::evolve_sr (src/LGPEngine.cpp:519-557) with the whole
+ * generation on the GPU: the population stays in device memory; elites
+ * (top_k_indices + copy_elite_to_next, :381-425), tournament selection
+ * (tournament_t, :148-171), crossover (crossover_t, :175-207) and mutation
+ * (mutate_t, micro_mutate_instruction_t, :213-341) run as device kernels with
+ * the engine's own random streams (one PCG32 per pair seeded from two draws
+ * of the engine's mt19937 per generation, :427-456), and evaluation of the
+ * non-elites uses this evaluator on the context's resident dataset.  Given
+ * the same options and seed, the populations, fitness values and history
+ * equal the reference engine's with this evaluator as its backend.
+ * Initialization is the engine's serial one (:49-81): one mt19937 draw per
+ * instruction slot, on the host, uploaded once. */
+typedef struct {
+    int64_t population;            /* POPULATION_SIZE (even non-elite count)  */
+    int32_t max_program_size;      /* MAX_PROGRAM_SIZE (<= 254)                */
+    int32_t starting_program_size; /* STARTING_PROGRAM_SIZE                    */
+    int32_t max_generations;       /* MAX_GENERATIONS (generation 0 included)  */
+    int32_t elite_count;           /* ELITE_COUNT = int(P * ELITES)            */
+    int32_t tournament_size;       /* TOURNAMENT_SIZE                          */
+    int32_t macro_inserts;         /* MACRO_INSERTS                            */
+    int32_t effmut;                /* EFFMUT (effective mutation)              */
+    int32_t macro_random_pos;      /* MACRO_RANDOM_POS                         */
+    float crossover_rate;          /* CROSSOVER_RATE                           */
+    float micro_rate;              /* MICRO_RATE                               */
+    float micro_per_instr;         /* MICRO_PER_INSTR                          */
+    float effmut_rate;             /* EFFMUT_RATE                              */
+    float insert_tail_rate;        /* INSERT_TAIL_RATE                         */
+    float delete_tail_rate;        /* DELETE_TAIL_RATE                         */
+    uint32_t seed;                 /* the engine's seed                        */
+    int32_t reserved[3];
+} galop_engine_options;
+
+/* One row of the run's history (GenerationStats, src/GenerationStats.h). */
+typedef struct {
+    int32_t generation;
+    float best_fitness;
+    float mean_fitness;
+    int32_t best_length;
+    float mean_length;
+    int32_t best_index;
+} galop_generation_stats;
+
+/* Seconds spent per phase over the last run (CUDA events and host clock). */
+typedef struct {
+    double total_s, init_s, evaluate_s, select_vary_s, stats_s;
+    int64_t eff_instructions;      /* interpreted instructions over the run   */
+} galop_engine_times;
+
+typedef struct galop_engine galop_engine;
+
+/* Defaults: the reference's default LGPConfig (P 1000, MAX_PROGRAM_SIZE 50,
+ * start 8, 1000 generations, elites int(P*0.1f), tournament 3, 1 macro
+ * insert, no EFFMUT, random positions, crossover 1.0, micro 0.8, per-instr
+ * 0, EFFMUT rate 1.0, insert 0.8, delete 0.75, seed 42). */
+GALOP_API int galop_engine_options_init(galop_engine_options* o);
+/* Device buffers for two generations, sized once.  The ISA (registers,
+ * input protection, profile, constants) and the reduction are ctx's. */
+GALOP_API int galop_engine_create(galop_ctx* ctx, const galop_engine_options* o, galop_engine** out);
+GALOP_API int galop_engine_destroy(galop_engine* e);
+/* init + max_generations generations on ctx's resident dataset; history gets
+ * max_generations rows (capacity must be at least that). */
+GALOP_API int galop_engine_evolve(galop_engine* e, galop_generation_stats* history, int32_t capacity);
+/* The current generation: dense words (population x max_program_size),
+ * lengths and fitness, copied to host memory (any pointer may be NULL). */
+GALOP_API int galop_engine_population(galop_engine* e, uint32_t* words, uint8_t* lengths, float* fitness);
+GALOP_API int galop_engine_times_get(const galop_engine* e, galop_engine_times* out);
+
 /* ---- CSV datasets ---------------------------------------------------------- */
 
 /* Replaces load_csv_1d (multi = 0) and load_csv_multi (multi = 1)
