@@ -282,6 +282,7 @@ def run_b200(args, dist: Dist):
     fit_check = ev.evaluate_csr(words, offsets)
     st0 = ev.stats
     eff_instr, raw_instr = st0.eff_instructions, st0.raw_instructions
+    interp_instr = st0.interp_instructions
 
     clocks = ClockSampler(dist.local)
     dist.barrier()
@@ -368,6 +369,7 @@ def run_b200(args, dist: Dist):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "programs_per_gpu": n, "cases": wl.n_cases,
                        "raw_instructions_per_gpu": raw_instr, "effective_instructions_per_gpu": eff_instr,
+                       "interpreted_instructions_per_gpu": interp_instr,
                        "cases_per_lane": st0.cases_per_lane, "warps_per_block": st0.warps_per_block,
                        "reduce": ["kahan32", "fp64", "ordered"][args.reduce],
                        "l2": "inputs larger than L2 (raw population %.2f GB per GPU)" % (words.nbytes / 1e9),
@@ -380,7 +382,12 @@ def run_b200(args, dist: Dist):
                          "frac": achieved / peak_gops, "traffic": profile_traffic(),
                          "kernel": profile_summary().get("kernel", "interp_wide_kernel"), "kernel_ms": interp_avg_ms,
                          "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {sm_max:.0f} MHz "
-                                        f"(sm_max_mhz of MEASURED_PEAKS.json)"},
+                                        f"(sm_max_mhz of MEASURED_PEAKS.json)",
+                         "ops_per_launch": float(eff_instr) * wl.n_cases,
+                         # instructions the interpreter actually runs per case: the effective ones
+                         # minus those evaluated once per program (every operand case-independent)
+                         "interpreted_ops_per_launch": float(interp_instr) * wl.n_cases,
+                         "interpreted_achieved": interp_instr * wl.n_cases / (interp_avg_ms / 1e3) / 1e9},
             "clocks": clock,
             "latency_ms": {"p50": float(np.percentile(interp_ms, 50)), "p99": float(np.percentile(interp_ms, 99))},
         }

@@ -119,11 +119,11 @@ class Stats(C.Structure):
         ("interp_ms", C.c_double), ("finalize_ms", C.c_double), ("d2h_ms", C.c_double),
         ("total_ms", C.c_double), ("cases_per_lane", C.c_int32), ("warps_per_block", C.c_int32),
         ("blocks", C.c_int32), ("case_chunks", C.c_int32), ("kernels_launched", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("reserved0", C.c_int32), ("interp_instructions", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
 
 
 class PopulationSpec(C.Structure):

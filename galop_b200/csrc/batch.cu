@@ -20,6 +20,7 @@
 #include "context.cuh"
 #include "prepass.cuh"
 #include "interp_wide.cuh"
+#include "fold.cuh"
 
 using namespace galop;
 
@@ -189,6 +190,15 @@ int enqueue(galop_batch* b) {
     scan_apply_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(b->eff_len.p, G, b->tiles.p, n_tiles, b->eff_off.p);
     prepass_compact_kernel<SpanSource><<<blocks, tpb, 0, s>>>(src, G, ctx->isa, strip ? 1 : 0, b->eff_off.p,
                                                               b->uops.p, nullptr, b->fmt);
+    const bool fold = b->fmt.wide && strip;
+    if (fold) {
+        // constants folded per program with its own population's input count
+        FoldParams fp{ctx->isa.profile, ctx->isa.num_registers, ctx->isa.output_reg,
+                      7u + (uint32_t)__builtin_ctz(b->fmt.stride / 128u), 0, b->descs.p, b->prog_pop.p};
+        fold_kernel<<<blocks, tpb, 0, s>>>(reinterpret_cast<uint4*>(b->uops.p), b->eff_off.p, G, fp, b->eff_len.p,
+                                           b->counters.p + 3);
+        b->launches += 1;
+    }
     batch_key_kernel<<<blocks, tpb, 0, s>>>(b->layout.p, b->prog_pop.p, b->eff_len.p, G, b->key.p);
     order_hist_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p);
     order_scan_kernel<<<1, 1024, 0, s>>>(b->hist.p);
@@ -205,6 +215,7 @@ int enqueue(galop_batch* b) {
     InterpArgs a{};
     a.uops = b->uops.p;
     a.eff_off = b->eff_off.p;
+    a.interp_len = fold ? b->eff_len.p : nullptr;
     a.n_programs = G;
     a.n_chunks = 1;
     a.output_reg = ctx->isa.output_reg;
@@ -547,10 +558,11 @@ int galop_batch_synchronize(galop_batch* b) {
         float ms = 0.0f;
         if (cudaEventElapsedTime(&ms, b->ev0, b->ev1) == cudaSuccess) b->stats.total_ms = ms;
         b->stats.interp_ms = b->stats.total_ms;
-        unsigned long long tot[2] = {0, 0};
+        unsigned long long tot[3] = {0, 0, 0};
         B_CK(cudaMemcpy(tot, b->counters.p + 1, sizeof tot, cudaMemcpyDeviceToHost), "batch stats");
         b->stats.raw_instructions = (int64_t)tot[0];
         b->stats.eff_instructions = (int64_t)tot[1];
+        b->stats.interp_instructions = (b->fmt.wide && ctx->opt.intron_prepass) ? (int64_t)tot[2] : (int64_t)tot[1];
         b->stats.kernels_launched = b->launches;
         b->stats.case_chunks = (int32_t)(b->G ? b->n_items / b->G : 0);
         b->pending = false;

@@ -98,6 +98,7 @@ struct galop_ctx {
     galop_stats stats{};
     int launches = 0;
     bool stats_pending = false;   // device-path call whose timings are not read yet
+    bool folded = false;          // the last pre-pass folded constants (interp lengths in eff_len)
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];

@@ -21,6 +21,8 @@ Emitted for NR in {8, 16} and K in {1, 2, 4, 8}:
            protected DIV is one of the arms
   wide loop  the same arms as one PTX loop over consecutive binary
            instructions (returns at the first unary op or window end)
+  both wide forms also have the broadcast arm (table index 12): t[k] = the
+  micro-op's constant, for instructions folded by the pre-pass
 where OP is one of the single-instruction ops: ADD, SUB, MUL (add/sub/mul
 with explicit .rn rounding, which ptxas never contracts into FMA) and, for
 the REF profile, LT, GT (set.lt/set.gt .f32.f32: 1.0 if the ordered
@@ -38,6 +40,10 @@ NRS = (8, 16)
 KS = (1, 2, 4, 8)
 CHEAP = {0: "add.rn.f32", 1: "sub.rn.f32", 2: "mul.rn.f32", 6: "set.lt.f32.f32", 7: "set.gt.f32.f32"}
 PROFILES = {0: (0, 1, 2, 6, 7), 1: (0, 1, 2)}   # REF, BJ
+# Table slot 8 + BCAST_OP (a SIN "with constant operand", which the pre-pass
+# never emits as such) is the broadcast arm: t = the micro-op's constant, for
+# instructions the pre-pass has evaluated once because every operand is known.
+BCAST_OP = 4
 
 
 def asm_block(lines: list[str], outs: list[str], ins: list[str]) -> str:
@@ -196,11 +202,12 @@ def wide_ops(k: int, profile: int) -> str:
     L = [f".reg .f32 {regs}, c;", WIDE_TEMPS, "mov.b32 c, %4;"]
     L += ld("a", "%1")
     targets = [f"R{op}_%=" if op in ops else "E%=" for op in range(8)] + \
-              [f"C{op}_%=" if op in ops else "E%=" for op in range(8)]
+              [f"C{op}_%=" if op in ops else ("B%=" if op == BCAST_OP else "E%=") for op in range(8)]
     L += ["T%=: .branchtargets " + ", ".join(targets) + ";", "brx.idx.uni %0, T%=;"]
     for op in ops:
         L.append(f"R{op}_%=: " + " ".join(ld("b", "%2") + body(op, False) + st("%3")) + " bra.uni E%=;")
         L.append(f"C{op}_%=: " + " ".join(body(op, True) + st("%3")) + " bra.uni E%=;")
+    L.append("B%=: " + " ".join([f"mov.f32 t{q}, c;" for q in range(k)] + st("%3")) + " bra.uni E%=;")
     L.append("E%=:")
     text = "\\n\\t".join(L)
     return ("    static __device__ __forceinline__ void run(uint32_t idx, uint32_t pa, uint32_t pb, uint32_t pt, "
@@ -247,12 +254,15 @@ def wide_loop(k: int, profile: int) -> str:
               f"add.u32 pa, %1, {x};", f"add.u32 pb, %1, {y};", f"add.u32 pt, %1, {z};", f"mov.b32 c, {y};"]
         L += ld("a", "pa")
         targets = [f"R{here}{op}_%=" if op in ops else f"D%=" for op in range(8)] + \
-                  [f"C{here}{op}_%=" if op in ops else f"D%=" for op in range(8)]
+                  [f"C{here}{op}_%=" if op in ops else (f"B{here}_%=" if op == BCAST_OP else f"D%=")
+                   for op in range(8)]
         L += [f"T{here}%=: .branchtargets " + ", ".join(targets) + ";", f"brx.idx.uni {w}, T{here}%=;"]
         for op in ops:
             L.append(f"R{here}{op}_%=: " + " ".join(ld("b", "pb") + body(op, False) + st("pt"))
                      + f" bra.uni L{there}%=;")
             L.append(f"C{here}{op}_%=: " + " ".join(body(op, True) + st("pt")) + f" bra.uni L{there}%=;")
+        L.append(f"B{here}_%=: " + " ".join([f"mov.f32 t{q}, c;" for q in range(k)] + st("pt"))
+                 + f" bra.uni L{there}%=;")
     L.append("D%=:")
     text = "\\n\\t".join(L)
     return ("    static __device__ __forceinline__ void run(uint32_t& sp, uint32_t base) {\n"

@@ -193,7 +193,7 @@ interp_wide_kernel(InterpArgs args) {
         if ((int64_t)item >= total_items) break;
         const WideItem w = resolve_item(args, item);
         const int64_t p0 = args.eff_off[w.prog];
-        const int64_t L = args.eff_off[w.prog + 1] - p0;
+        const int64_t L = args.interp_len ? (int64_t)args.interp_len[w.prog] : args.eff_off[w.prog + 1] - p0;
         const uint4* __restrict__ pw = uops4 + p0;
 
         float ks = 0.0f, kc = 0.0f;

@@ -73,6 +73,9 @@ __host__ __device__ __forceinline__ uint32_t encode_uop(const Decoded& d) {
 // stride = bytes per register per warp (32 lanes x K cases x 4 bytes).
 constexpr uint32_t kWideSpecial = 0x80000000u;
 constexpr uint32_t kWideEnd = 0xFFFFFFFFu;
+// Broadcast micro-op (table slot 12): dest = the constant in y, for an
+// instruction whose operands are all known before any case is read.
+constexpr uint32_t kWideBcast = 12u;
 
 __device__ __forceinline__ uint4 encode_wide(const Decoded& d, uint32_t stride, const ConstPool& cp) {
     uint4 u;

@@ -20,6 +20,7 @@
 #include "interp.cuh"
 #include "prepass.cuh"
 #include "interp_wide.cuh"
+#include "fold.cuh"
 
 namespace galop {
 const void* interp_kernel_nr8(int k, int dispatch, int profile, int reduce, int mode);
@@ -131,6 +132,16 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
                                                            ctx->eff_off.p, ctx->uops.p, raw_out, fmt);
         ctx->launches += 1;
     }
+    // Constant folding (wide micro-ops of effective code only; the raw-word
+    // output of galop_effective_csr keeps the intron pass's result as is).
+    ctx->folded = fmt.wide && strip && raw_out == nullptr && n > 0;
+    if (ctx->folded) {
+        FoldParams fp{ctx->isa.profile, ctx->isa.num_registers, ctx->isa.output_reg,
+                      7u + (uint32_t)__builtin_ctz((unsigned)pick_k(ctx)), ctx->num_inputs, nullptr, nullptr};
+        fold_kernel<<<blocks, tpb, 0, s>>>(reinterpret_cast<uint4*>(ctx->uops.p), ctx->eff_off.p, n, fp,
+                                           ctx->eff_len.p, ctx->counters.p + 3);
+        ctx->launches += 1;
+    }
     GALOP_CK(cudaGetLastError(), "pre-pass compact launch");
     if (sched && n > 1) {
         GALOP_CK(ctx->order.ensure((size_t)n), "alloc order");
@@ -184,6 +195,7 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     InterpArgs a{};
     a.uops = ctx->uops.p;
     a.eff_off = ctx->eff_off.p;
+    a.interp_len = ctx->folded ? ctx->eff_len.p : nullptr;
     a.order = (sched && n > 1) ? ctx->order.p : nullptr;
     a.n_programs = n;
     a.n_chunks = (int32_t)n_chunks;
@@ -257,11 +269,12 @@ int finish_stats(galop_ctx* ctx) {
     st.finalize_ms = ev_ms(ctx->ev[kEvInterp], ctx->ev[kEvFinalize]);
     st.d2h_ms = ev_ms(ctx->ev[kEvFinalize], ctx->ev[kEvD2H]);
     st.total_ms = ev_ms(ctx->ev[kEvStart], ctx->ev[kEvD2H]);
-    unsigned long long tot[2] = {0, 0};
+    unsigned long long tot[3] = {0, 0, 0};
     if (ctx->counters.p)
         GALOP_CK(cudaMemcpy(tot, ctx->counters.p + 1, sizeof tot, cudaMemcpyDeviceToHost), "stats D2H");
     st.raw_instructions = (int64_t)tot[0];
     st.eff_instructions = (int64_t)tot[1];
+    st.interp_instructions = ctx->folded ? (int64_t)tot[2] : (int64_t)tot[1];
     st.kernels_launched = ctx->launches;
     ctx->stats_pending = false;
     return GALOP_OK;

@@ -120,7 +120,11 @@ typedef struct {
     int32_t blocks;
     int32_t case_chunks;           /* work items per program                    */
     int32_t kernels_launched;      /* this library's kernel launches            */
-    int32_t reserved[3];
+    int32_t reserved0;
+    int64_t interp_instructions;   /* instructions interpreted per case: the
+                                      effective ones minus those evaluated
+                                      once because every operand is known
+                                      (dispatch 3 with the intron pass)      */
 } galop_stats;
 
 /* ---- lifetime ------------------------------------------------------------ */
