@@ -73,6 +73,8 @@ struct galop_ctx {
     int device = 0;
     int sm_count = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;   // host-to-device copies overlapped with compute (lazy)
+    cudaEvent_t seg_ev[8 * 5] = {};        // per segment: copied, pre-pass start/end, interp end, finalize end
     cudaEvent_t ev[kEvCount] = {};
     cudaEvent_t timers[8] = {};
     std::string err;

@@ -89,14 +89,15 @@ float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 // Pre-pass over `src` into ctx->uops / eff_off (and order when sched).
 template <class Src>
 int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_total,
-                bool strip, bool sched, uint32_t* raw_out) {
+                bool strip, bool sched, uint32_t* raw_out, bool reset_totals = true) {
     cudaStream_t s = ctx->stream;
     GALOP_CK(ctx->eff_len.ensure((size_t)std::max<int64_t>(n, 1)), "alloc eff_len");
     GALOP_CK(ctx->eff_off.ensure((size_t)n + 1), "alloc eff_off");
     const int64_t n_tiles = (n + kScanTile - 1) / kScanTile;
     GALOP_CK(ctx->tiles.ensure((size_t)n_tiles + 1), "alloc scan tiles");
     GALOP_CK(ctx->counters.ensure(4), "alloc counters");
-    GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), s), "memset");
+    if (reset_totals)
+        GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), s), "memset");
 
     const int tpb = 256;
     const unsigned blocks = (unsigned)((n + tpb - 1) / tpb);
@@ -158,7 +159,7 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
 
 // Interpreter launch over the pre-passed population.
 int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness, double* d_sse,
-               float* d_outputs, float* d_trace, int32_t* chunks_out) {
+               float* d_outputs, float* d_trace, int32_t* chunks_out, int64_t policy_n = -1) {
     cudaStream_t s = ctx->stream;
     const int k = pick_k(ctx);
     const int wpb = pick_wpb(ctx);
@@ -183,8 +184,11 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     const int64_t pass = 32LL * k;
     const int64_t passes = std::max<int64_t>(1, (ctx->N + pass - 1) / pass);
     int64_t n_chunks = 1;
+    // policy_n: the population size the chunking is decided for (a segment
+    // of a larger call is chunked as the whole call would be)
+    const int64_t pn = policy_n >= 0 ? policy_n : n;
     if (mode == kModeFitness && ctx->opt.reduce != GALOP_REDUCE_ORDERED && n > 0) {
-        if (n < 4 * resident_warps) n_chunks = std::min<int64_t>(passes, (4 * resident_warps + n - 1) / n);
+        if (pn < 4 * resident_warps) n_chunks = std::min<int64_t>(passes, (4 * resident_warps + pn - 1) / pn);
         n_chunks = std::max<int64_t>(n_chunks, std::min<int64_t>(passes, (ctx->N + kMaxItemCases - 1) / kMaxItemCases));
     }
     if (mode != kModeFitness) n_chunks = 1;
@@ -433,6 +437,8 @@ void galop_destroy(galop_ctx* ctx) {
     ctx->sse.release(); ctx->partial.release(); ctx->counters.release(); ctx->hist.release();
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->timers) if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->seg_ev) if (e) cudaEventDestroy(e);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -616,6 +622,80 @@ static int evaluate_uploaded(galop_ctx* ctx, const Src& src, int64_t n, int64_t 
     return end_call(ctx);
 }
 
+// Host-pointer CSR evaluation in segments of programs: the words of segment
+// k+1 are copied on a second stream while segment k is pre-passed and
+// interpreted, so most of the host-to-device copy hides behind compute.
+// Every segment is chunked as the whole call would be, so the fitness is
+// the unsegmented call's bit for bit.
+static int evaluate_csr_segmented(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets, int64_t n,
+                                  int segs, float* fitness_out, double* sse_out) {
+    cudaStream_t s = ctx->stream;
+    if (!ctx->copy_stream) {
+        GALOP_CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
+        for (auto& e : ctx->seg_ev) GALOP_CK(cudaEventCreate(&e), "segment events");
+    }
+    cudaStream_t cs = ctx->copy_stream;
+    const int64_t total = offsets[n];
+    GALOP_CK(ctx->raw_words.ensure((size_t)std::max<int64_t>(total, 1)), "alloc raw words");
+    GALOP_CK(ctx->raw_off.ensure((size_t)n + 1), "alloc raw offsets");
+    GALOP_CK(ctx->fitness.ensure((size_t)std::max<int64_t>(n, 1)), "alloc fitness");
+    GALOP_CK(ctx->sse.ensure((size_t)std::max<int64_t>(n, 1)), "alloc sse");
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], s), "event");
+    GALOP_CK(cudaStreamWaitEvent(cs, ctx->ev[kEvStart], 0), "stream wait");
+    GALOP_CK(cudaMemcpyAsync(ctx->raw_off.p, offsets, (size_t)(n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, cs),
+             "H2D offsets");
+    std::vector<int64_t> b(segs + 1);
+    for (int k = 0; k <= segs; ++k) b[k] = n * k / segs;
+    for (int k = 0; k < segs; ++k) {
+        const int64_t w0 = offsets[b[k]], w1 = offsets[b[k + 1]];
+        if (w1 > w0)
+            GALOP_CK(cudaMemcpyAsync(ctx->raw_words.p + w0, words + w0, (size_t)(w1 - w0) * sizeof(uint32_t),
+                                     cudaMemcpyHostToDevice, cs), "H2D words");
+        GALOP_CK(cudaEventRecord(ctx->seg_ev[5 * k], cs), "event");
+    }
+    GALOP_CK(ctx->counters.ensure(4), "alloc counters");
+    GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), s), "memset");
+    for (int k = 0; k < segs; ++k) {
+        const int64_t nk = b[k + 1] - b[k];
+        GALOP_CK(cudaStreamWaitEvent(s, ctx->seg_ev[5 * k], 0), "stream wait");
+        GALOP_CK(cudaEventRecord(ctx->seg_ev[5 * k + 1], s), "event");
+        CsrSource src{ctx->raw_words.p, ctx->raw_off.p + b[k]};
+        if (int rc = run_prepass(ctx, src, nk, offsets[b[k + 1]] - offsets[b[k]], ctx->opt.intron_prepass != 0,
+                                 true, nullptr, false))
+            return rc;
+        GALOP_CK(cudaEventRecord(ctx->seg_ev[5 * k + 2], s), "event");
+        int32_t chunks = 1;
+        if (int rc = run_interp(ctx, nk, kModeFitness, true, ctx->fitness.p + b[k], ctx->sse.p + b[k], nullptr,
+                                nullptr, &chunks, n))
+            return rc;
+        GALOP_CK(cudaEventRecord(ctx->seg_ev[5 * k + 3], s), "event");
+        if (int rc = finalize(ctx, nk, chunks, ctx->fitness.p + b[k], ctx->sse.p + b[k])) return rc;
+        GALOP_CK(cudaEventRecord(ctx->seg_ev[5 * k + 4], s), "event");
+    }
+    if (n > 0) {
+        GALOP_CK(cudaMemcpyAsync(fitness_out, ctx->fitness.p, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, s),
+                 "D2H fitness");
+        if (sse_out)
+            GALOP_CK(cudaMemcpyAsync(sse_out, ctx->sse.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s),
+                     "D2H sse");
+    }
+    GALOP_CK(cudaEventRecord(ctx->ev[kEvD2H], s), "event");
+    GALOP_CK(cudaStreamSynchronize(s), "evaluate (device execution)");
+    if (int rc = finish_stats(ctx)) return rc;
+    galop_stats& st = ctx->stats;
+    st.h2d_ms = ev_ms(ctx->ev[kEvStart], ctx->seg_ev[5 * (segs - 1)]);
+    st.prepass_ms = st.interp_ms = st.finalize_ms = 0.0;
+    for (int k = 0; k < segs; ++k) {
+        st.prepass_ms += ev_ms(ctx->seg_ev[5 * k + 1], ctx->seg_ev[5 * k + 2]);
+        st.interp_ms += ev_ms(ctx->seg_ev[5 * k + 2], ctx->seg_ev[5 * k + 3]);
+        st.finalize_ms += ev_ms(ctx->seg_ev[5 * k + 3], ctx->seg_ev[5 * k + 4]);
+    }
+    st.d2h_ms = ev_ms(ctx->seg_ev[5 * (segs - 1) + 4], ctx->ev[kEvD2H]);
+    st.total_ms = ev_ms(ctx->ev[kEvStart], ctx->ev[kEvD2H]);
+    st.n_programs = n;
+    return GALOP_OK;
+}
+
 extern "C" {
 
 int galop_evaluate_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets, int64_t n_programs,
@@ -626,6 +706,12 @@ int galop_evaluate_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* off
     if (n_programs > 0 && !fitness_out) return ctx->fail(GALOP_E_INVALID, "null fitness_out");
     GALOP_CK(cudaSetDevice(ctx->device), "set device");
     begin_call(ctx, n_programs);
+    // Large populations: copy and compute overlapped in 4 segments.
+    if (n_programs >= 65536 && offsets && offsets[n_programs] >= (int64_t)(32ll << 20)) {
+        if (!words) return ctx->fail(GALOP_E_INVALID, "null words/offsets");
+        if (int rc = validate_offsets(ctx, offsets, n_programs)) return rc;
+        return evaluate_csr_segmented(ctx, words, offsets, n_programs, 4, fitness_out, sse_out);
+    }
     GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], ctx->stream), "event");
     if (int rc = upload_csr(ctx, words, offsets, n_programs)) return rc;
     CsrSource src{ctx->raw_words.p, ctx->raw_off.p};

@@ -430,3 +430,33 @@ def test_r2_objective_is_refused_without_allocation(native):
     rc = lib.galop_evaluate_csr_noalloc(ctypes.byref(opt), None, ctypes.c_void_p(1), 0, 0, None, None, 0, 1024,
                                         1, None, None, None)
     assert rc == g.E_INVALID
+
+
+@pytest.mark.parametrize("reduce", [g.REDUCE_KAHAN32, g.REDUCE_ORDERED])
+def test_large_host_call_in_segments_matches_device_call(native, reduce):
+    """A host-pointer call above 32 M instructions is copied and computed in
+    overlapped segments; its fitness must equal the one-piece device-resident
+    call bit for bit (same chunking, same folding)."""
+    rng = np.random.default_rng(21)
+    lens = rng.integers(400, 620, 70_000)
+    words, off = W.random_population(rng, lens, 16)
+    assert off[-1] >= 32 << 20
+    X = rng.uniform(-2, 2, (300, 3)).astype(np.float32)
+    y = rng.uniform(-1, 1, 300).astype(np.float32)
+    with g.Evaluator(num_registers=16, reduce=reduce) as ev:
+        ev.set_dataset(g.Dataset(X, y))
+        host = ev.evaluate_csr(words, off)
+        st = ev.stats
+        dw, do, df = ev.device_alloc(words.nbytes), ev.device_alloc(off.nbytes), ev.device_alloc(4 * len(lens))
+        try:
+            ev.h2d(dw, words)
+            ev.h2d(do, off)
+            ev.evaluate_csr_device(dw, do, len(lens), df)
+            ev.synchronize()
+            dev = np.empty(len(lens), np.float32)
+            ev.d2h(dev, df)
+        finally:
+            for p in (dw, do, df):
+                ev.device_free(p)
+    assert st.eff_instructions > 0 and st.kernels_launched > 20      # four segments' launches
+    assert np.array_equal(bits(host), bits(dev))
