@@ -70,7 +70,7 @@ class _Options(C.Structure):
         ("reduce", C.c_int32), ("constants", C.POINTER(C.c_float)), ("device", C.c_int32),
         ("intron_prepass", C.c_int32), ("cases_per_lane", C.c_int32),
         ("warps_per_block", C.c_int32), ("dispatch", C.c_int32), ("objective", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("dedup", C.c_int32), ("reserved", C.c_int32 * 1),
     ]
 
 
@@ -318,7 +318,8 @@ class Evaluator:
     def __init__(self, profile: int = PROFILE_REF, num_registers: int = 8, input_protect: bool = False,
                  reduce: int = REDUCE_KAHAN32, constants: Optional[Sequence[float]] = None,
                  device: int = 0, intron_prepass: bool = True, cases_per_lane: int = 0,
-                 warps_per_block: int = 0, dispatch: Optional[int] = None, objective: int = OBJECTIVE_MSE):
+                 warps_per_block: int = 0, dispatch: Optional[int] = None, objective: int = OBJECTIVE_MSE,
+                 dedup: Optional[bool] = None):
         self._lib = load_library()
         opt = _Options()
         self._lib.galop_options_init(C.byref(opt))
@@ -333,6 +334,8 @@ class Evaluator:
         if dispatch is not None:
             opt.dispatch = dispatch
         opt.objective = objective
+        if dedup is not None:
+            opt.dedup = int(bool(dedup))
         self.constants = None
         if constants is not None:
             self.constants = np.ascontiguousarray(constants, dtype=np.float32)

@@ -101,6 +101,10 @@ struct galop_ctx {
     int launches = 0;
     bool stats_pending = false;   // device-path call whose timings are not read yet
     bool folded = false;          // the last pre-pass folded constants (interp lengths in eff_len)
+    bool deduped = false;         // ... and left identical programs out (representatives in rep)
+    DevBuf<unsigned long long> dkeys, dkeys_sorted;
+    DevBuf<int32_t> dvals, dvals_sorted, rep, dhead;
+    DevBuf<unsigned char> dsort_tmp;
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];

@@ -220,13 +220,19 @@ __global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int st
 }
 
 // Longest-first order: histogram of bins (bin 0 = longest), scan, scatter.
+// A negative length (a copy left out by dedup.cuh) goes to the last bin,
+// after every program that is interpreted.
+__device__ __forceinline__ int order_bin(int l) {
+    if (l < 0) return kOrderBins - 1;
+    if (l > kOrderBins - 2) l = kOrderBins - 2;
+    return kOrderBins - 2 - l;
+}
+
 static __global__ void order_hist_kernel(const int32_t* __restrict__ len, int64_t n,
                                   unsigned int* __restrict__ hist) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int l = len[i];
-    if (l > kOrderBins - 1) l = kOrderBins - 1;
-    atomicAdd(&hist[kOrderBins - 1 - l], 1u);
+    atomicAdd(&hist[order_bin(len[i])], 1u);
 }
 
 static __global__ void order_scan_kernel(unsigned int* __restrict__ hist) {
@@ -254,9 +260,7 @@ static __global__ void order_scatter_kernel(const int32_t* __restrict__ len, int
                                      int32_t* __restrict__ order) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int l = len[i];
-    if (l > kOrderBins - 1) l = kOrderBins - 1;
-    const unsigned int pos = atomicAdd(&cursor[kOrderBins - 1 - l], 1u);
+    const unsigned int pos = atomicAdd(&cursor[order_bin(len[i])], 1u);
     order[pos] = (int32_t)i;
 }
 

@@ -21,6 +21,9 @@
 #include "prepass.cuh"
 #include "interp_wide.cuh"
 #include "fold.cuh"
+#include "dedup.cuh"
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 namespace galop {
 const void* interp_kernel_nr8(int k, int dispatch, int profile, int reduce, int mode);
@@ -89,15 +92,20 @@ float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 // Pre-pass over `src` into ctx->uops / eff_off (and order when sched).
 template <class Src>
 int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_total,
-                bool strip, bool sched, uint32_t* raw_out, bool reset_totals = true) {
+                bool strip, bool sched, uint32_t* raw_out, bool reset_totals = true, bool fitness_mode = false) {
     cudaStream_t s = ctx->stream;
     GALOP_CK(ctx->eff_len.ensure((size_t)std::max<int64_t>(n, 1)), "alloc eff_len");
     GALOP_CK(ctx->eff_off.ensure((size_t)n + 1), "alloc eff_off");
     const int64_t n_tiles = (n + kScanTile - 1) / kScanTile;
     GALOP_CK(ctx->tiles.ensure((size_t)n_tiles + 1), "alloc scan tiles");
-    GALOP_CK(ctx->counters.ensure(4), "alloc counters");
+    // counters: [0] work queue, [1] raw, [2] effective, [3] interpreted
+    // instructions, [4] copies left out by dedup (this pre-pass), [5] their
+    // interpreted instructions
+    GALOP_CK(ctx->counters.ensure(6), "alloc counters");
     if (reset_totals)
-        GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), s), "memset");
+        GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 6 * sizeof(unsigned long long), s), "memset");
+    else
+        GALOP_CK(cudaMemsetAsync(ctx->counters.p + 4, 0, sizeof(unsigned long long), s), "memset");
 
     const int tpb = 256;
     const unsigned blocks = (unsigned)((n + tpb - 1) / tpb);
@@ -142,6 +150,37 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
         fold_kernel<<<blocks, tpb, 0, s>>>(reinterpret_cast<uint4*>(ctx->uops.p), ctx->eff_off.p, n, fp,
                                            ctx->eff_len.p, ctx->counters.p + 3);
         ctx->launches += 1;
+    }
+    // Identical interpreted programs: one representative each (dedup.cuh).
+    ctx->deduped = fitness_mode && ctx->folded && ctx->opt.dedup && sched && n > 1;
+    if (ctx->deduped) {
+        const size_t N1 = (size_t)n;
+        GALOP_CK(ctx->dkeys.ensure(N1), "alloc dedup keys");
+        GALOP_CK(ctx->dkeys_sorted.ensure(N1), "alloc dedup keys");
+        GALOP_CK(ctx->dvals.ensure(N1), "alloc dedup values");
+        GALOP_CK(ctx->dvals_sorted.ensure(N1), "alloc dedup values");
+        GALOP_CK(ctx->rep.ensure(N1), "alloc representatives");
+        GALOP_CK(ctx->dhead.ensure(N1), "alloc dedup runs");
+        size_t tsort = 0, tscan = 0;
+        GALOP_CK(cub::DeviceRadixSort::SortPairs(nullptr, tsort, ctx->dkeys.p, ctx->dkeys_sorted.p, ctx->dvals.p,
+                                                 ctx->dvals_sorted.p, (int)n, 0, 64, s), "dedup sort size");
+        GALOP_CK(cub::DeviceScan::InclusiveScan(nullptr, tscan, ctx->dhead.p, ctx->dvals.p, cub::Max(), (int)n, s),
+                 "dedup scan size");
+        GALOP_CK(ctx->dsort_tmp.ensure(std::max<size_t>(std::max(tsort, tscan), 1)), "alloc dedup sort");
+        size_t tmp = ctx->dsort_tmp.cap;
+        const uint4* u4 = reinterpret_cast<const uint4*>(ctx->uops.p);
+        dedup_hash_kernel<<<blocks, tpb, 0, s>>>(u4, ctx->eff_off.p, ctx->eff_len.p, n, ctx->dkeys.p, ctx->dvals.p,
+                                                 ctx->rep.p);
+        GALOP_CK(cub::DeviceRadixSort::SortPairs(ctx->dsort_tmp.p, tmp, ctx->dkeys.p, ctx->dkeys_sorted.p,
+                                                 ctx->dvals.p, ctx->dvals_sorted.p, (int)n, 0, 64, s), "dedup sort");
+        dedup_run_start_kernel<<<blocks, tpb, 0, s>>>(ctx->dkeys_sorted.p, n, ctx->dhead.p);
+        tmp = ctx->dsort_tmp.cap;
+        GALOP_CK(cub::DeviceScan::InclusiveScan(ctx->dsort_tmp.p, tmp, ctx->dhead.p, ctx->dvals.p, cub::Max(), (int)n,
+                                                s), "dedup scan");
+        dedup_rep_kernel<<<blocks, tpb, 0, s>>>(ctx->dvals.p, ctx->dvals_sorted.p, n, u4, ctx->eff_off.p,
+                                                ctx->eff_len.p, ctx->rep.p, ctx->counters.p + 4);
+        ctx->launches += 5;
+        GALOP_CK(cudaGetLastError(), "dedup launch");
     }
     GALOP_CK(cudaGetLastError(), "pre-pass compact launch");
     if (sched && n > 1) {
@@ -200,6 +239,7 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     a.uops = ctx->uops.p;
     a.eff_off = ctx->eff_off.p;
     a.interp_len = ctx->folded ? ctx->eff_len.p : nullptr;
+    a.n_skipped = ctx->deduped ? ctx->counters.p + 4 : nullptr;
     a.order = (sched && n > 1) ? ctx->order.p : nullptr;
     a.n_programs = n;
     a.n_chunks = (int32_t)n_chunks;
@@ -241,6 +281,16 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
 }
 
 int finalize(galop_ctx* ctx, int64_t n, int32_t n_chunks, float* d_fitness, double* d_sse) {
+    if (ctx->deduped && n > 0) {
+        // chunk sums first (copies get garbage there), then the copies' results
+        if (n_chunks > 1)
+            finalize_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(
+                ctx->partial.p, n, n_chunks, ctx->N, objective_for(ctx, ctx->ss_tot), d_fitness, d_sse);
+        dedup_scatter_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(ctx->rep.p, n, d_fitness, d_sse);
+        ctx->launches += n_chunks > 1 ? 2 : 1;
+        GALOP_CK(cudaGetLastError(), "finalize launch");
+        return GALOP_OK;
+    }
     if (n_chunks <= 1 || n == 0) return GALOP_OK;
     finalize_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(
         ctx->partial.p, n, n_chunks, ctx->N, objective_for(ctx, ctx->ss_tot), d_fitness, d_sse);
@@ -273,12 +323,12 @@ int finish_stats(galop_ctx* ctx) {
     st.finalize_ms = ev_ms(ctx->ev[kEvInterp], ctx->ev[kEvFinalize]);
     st.d2h_ms = ev_ms(ctx->ev[kEvFinalize], ctx->ev[kEvD2H]);
     st.total_ms = ev_ms(ctx->ev[kEvStart], ctx->ev[kEvD2H]);
-    unsigned long long tot[3] = {0, 0, 0};
+    unsigned long long tot[5] = {0, 0, 0, 0, 0};
     if (ctx->counters.p)
         GALOP_CK(cudaMemcpy(tot, ctx->counters.p + 1, sizeof tot, cudaMemcpyDeviceToHost), "stats D2H");
     st.raw_instructions = (int64_t)tot[0];
     st.eff_instructions = (int64_t)tot[1];
-    st.interp_instructions = ctx->folded ? (int64_t)tot[2] : (int64_t)tot[1];
+    st.interp_instructions = ctx->folded ? (int64_t)(tot[2] - tot[4]) : (int64_t)tot[1];
     st.kernels_launched = ctx->launches;
     ctx->stats_pending = false;
     return GALOP_OK;
@@ -304,7 +354,8 @@ int evaluate_dense_device(galop_ctx* ctx, const uint32_t* d_words, const uint8_t
     GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], s), "event");
     GALOP_CK(cudaEventRecord(ctx->ev[kEvH2D], s), "event");
     DenseSource src{d_words, d_lens, stride};
-    if (int rc = run_prepass(ctx, src, n, n * stride, ctx->opt.intron_prepass != 0, true, nullptr)) return rc;
+    if (int rc = run_prepass(ctx, src, n, n * stride, ctx->opt.intron_prepass != 0, true, nullptr, true, true))
+        return rc;
     GALOP_CK(cudaEventRecord(ctx->ev[kEvPrepass], s), "event");
     int32_t chunks = 1;
     if (int rc = run_interp(ctx, n, kModeFitness, true, d_fitness, nullptr, nullptr, nullptr, &chunks)) return rc;
@@ -379,6 +430,7 @@ int galop_options_init(galop_options* opt) {
     opt->cases_per_lane = 0;
     opt->warps_per_block = 0;
     opt->dispatch = 3;
+    opt->dedup = 1;
     return GALOP_OK;
 }
 
@@ -416,7 +468,7 @@ int galop_create(const galop_options* opt, galop_ctx** out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     for (int i = 0; e == cudaSuccess && i < kEvCount; ++i) e = cudaEventCreate(&ctx->ev[i]);
     for (int i = 0; e == cudaSuccess && i < 8; ++i) e = cudaEventCreate(&ctx->timers[i]);
-    if (e == cudaSuccess) e = ctx->counters.ensure(4);
+    if (e == cudaSuccess) e = ctx->counters.ensure(6);
     if (e != cudaSuccess) {
         galop_destroy(ctx);
         return e == cudaErrorMemoryAllocation ? GALOP_E_NOMEM : GALOP_E_CUDA;
@@ -435,6 +487,8 @@ void galop_destroy(galop_ctx* ctx) {
     ctx->eff_len.release(); ctx->order.release();
     ctx->fitness.release(); ctx->outputs.release(); ctx->trace.release();
     ctx->sse.release(); ctx->partial.release(); ctx->counters.release(); ctx->hist.release();
+    ctx->dkeys.release(); ctx->dkeys_sorted.release(); ctx->dvals.release(); ctx->dvals_sorted.release();
+    ctx->rep.release(); ctx->dsort_tmp.release(); ctx->dhead.release();
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->timers) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->seg_ev) if (e) cudaEventDestroy(e);
@@ -601,7 +655,8 @@ static int evaluate_uploaded(galop_ctx* ctx, const Src& src, int64_t n, int64_t 
                              float* fitness_out, double* sse_out) {
     cudaStream_t s = ctx->stream;
     GALOP_CK(cudaEventRecord(ctx->ev[kEvH2D], s), "event");
-    if (int rc = run_prepass(ctx, src, n, raw_total, ctx->opt.intron_prepass != 0, true, nullptr)) return rc;
+    if (int rc = run_prepass(ctx, src, n, raw_total, ctx->opt.intron_prepass != 0, true, nullptr, true, true))
+        return rc;
     GALOP_CK(cudaEventRecord(ctx->ev[kEvPrepass], s), "event");
     GALOP_CK(ctx->fitness.ensure((size_t)std::max<int64_t>(n, 1)), "alloc fitness");
     GALOP_CK(ctx->sse.ensure((size_t)std::max<int64_t>(n, 1)), "alloc sse");
@@ -653,15 +708,15 @@ static int evaluate_csr_segmented(galop_ctx* ctx, const uint32_t* words, const i
                                      cudaMemcpyHostToDevice, cs), "H2D words");
         GALOP_CK(cudaEventRecord(ctx->seg_ev[5 * k], cs), "event");
     }
-    GALOP_CK(ctx->counters.ensure(4), "alloc counters");
-    GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), s), "memset");
+    GALOP_CK(ctx->counters.ensure(6), "alloc counters");
+    GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 6 * sizeof(unsigned long long), s), "memset");
     for (int k = 0; k < segs; ++k) {
         const int64_t nk = b[k + 1] - b[k];
         GALOP_CK(cudaStreamWaitEvent(s, ctx->seg_ev[5 * k], 0), "stream wait");
         GALOP_CK(cudaEventRecord(ctx->seg_ev[5 * k + 1], s), "event");
         CsrSource src{ctx->raw_words.p, ctx->raw_off.p + b[k]};
         if (int rc = run_prepass(ctx, src, nk, offsets[b[k + 1]] - offsets[b[k]], ctx->opt.intron_prepass != 0,
-                                 true, nullptr, false))
+                                 true, nullptr, false, true))
             return rc;
         GALOP_CK(cudaEventRecord(ctx->seg_ev[5 * k + 2], s), "event");
         int32_t chunks = 1;
@@ -769,7 +824,8 @@ int galop_evaluate_csr_device(galop_ctx* ctx, const uint32_t* d_words, const int
     GALOP_CK(cudaStreamSynchronize(s), "read total");
     GALOP_CK(cudaEventRecord(ctx->ev[kEvH2D], s), "event");
     CsrSource src{d_words, d_offsets};
-    if (int rc = run_prepass(ctx, src, n_programs, total, ctx->opt.intron_prepass != 0, true, nullptr)) return rc;
+    if (int rc = run_prepass(ctx, src, n_programs, total, ctx->opt.intron_prepass != 0, true, nullptr, true, true))
+        return rc;
     GALOP_CK(cudaEventRecord(ctx->ev[kEvPrepass], s), "event");
     int32_t chunks = 1;
     if (int rc = run_interp(ctx, n_programs, kModeFitness, true, d_fitness, d_sse, nullptr, nullptr, &chunks))

@@ -97,7 +97,10 @@ typedef struct {
                                  jump tables; 0 = lane registers behind C++
                                  switches.  All give identical results.     */
     int32_t objective;        /* galop_objective (default MSE)                  */
-    int32_t reserved[2];
+    int32_t dedup;            /* 1: programs whose interpreted code is identical
+                                 are interpreted once and share the fitness
+                                 (dispatch 3, intron pass on; default 1)     */
+    int32_t reserved[1];
 } galop_options;
 
 typedef struct galop_ctx galop_ctx;

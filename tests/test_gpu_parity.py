@@ -460,3 +460,34 @@ def test_large_host_call_in_segments_matches_device_call(native, reduce):
                 ev.device_free(p)
     assert st.eff_instructions > 0 and st.kernels_launched > 20      # four segments' launches
     assert np.array_equal(bits(host), bits(dev))
+
+
+@pytest.mark.parametrize("reduce", [g.REDUCE_KAHAN32, g.REDUCE_ORDERED])
+@pytest.mark.parametrize("n_unique,n_cases", [(3000, 777), (12, 200_000)])
+def test_identical_programs_are_interpreted_once(native, reduce, n_unique, n_cases):
+    """Copies of a program that differ only in introns (or not at all) share
+    the representative's fitness: with dedup on or off, every fitness and SSE
+    is the same bit for bit, also when programs are split into case chunks."""
+    rng = np.random.default_rng(5)
+    isa = W.IsaSpec(g.PROFILE_REF, 16)
+    base_w, base_off = W.structured_population(rng, W.uniform_lengths(rng, n_unique, 8, 60), isa, 0.5)
+    progs = [base_w[base_off[i]:base_off[i + 1]] for i in range(n_unique)]
+    out = []
+    for _ in range(4 * n_unique):
+        p = progs[int(rng.integers(0, n_unique))].copy()
+        if rng.random() < 0.5:          # an intron: a last write to a register that is not the output
+            p = np.concatenate([p, W.encode([0], [15], [1], [2], [0])])
+        out.append(p)
+    words = np.concatenate(out).astype(np.uint32)
+    off = W.csr_offsets([len(p) for p in out])
+    X = rng.uniform(-2, 2, (n_cases, 4)).astype(np.float32)
+    y = rng.uniform(-1, 1, n_cases).astype(np.float32)
+    ds = g.Dataset(X, y)
+    res = {}
+    for dd in (False, True):
+        with g.Evaluator(num_registers=16, reduce=reduce, dedup=dd) as ev:
+            res[dd] = ev.evaluate_csr(words, off, ds, with_sse=True)
+            res[(dd, "interp")] = ev.stats.interp_instructions
+    assert np.array_equal(bits(res[True][0]), bits(res[False][0]))
+    assert np.array_equal(res[True][1].view(np.uint64), res[False][1].view(np.uint64))
+    assert res[(True, "interp")] < 0.5 * res[(False, "interp")]
