@@ -21,6 +21,9 @@
 #include "prepass.cuh"
 #include "interp_wide.cuh"
 #include "fold.cuh"
+#include "dedup.cuh"
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 using namespace galop;
 
@@ -75,6 +78,11 @@ struct galop_batch {
     DevBuf<uint32_t> arena, uops;
     DevBuf<int64_t> local_off, starts, eff_off, item_off, first_item, tiles;
     DevBuf<int32_t> lens, prog_pop, eff_len, key, order, cnt, chunks_of_pop;
+    // dedup within each population (dedup.cuh)
+    DevBuf<unsigned long long> dkeys, dkeys_sorted;
+    DevBuf<int32_t> dvals, dvals_sorted, rep, dhead;
+    DevBuf<unsigned char> dtmp;
+    bool dedup = false;
     DevBuf<unsigned long long> items, counters;
     DevBuf<unsigned int> hist;
     DevBuf<float> fitness;
@@ -172,7 +180,7 @@ int enqueue(galop_batch* b) {
     cudaStream_t s = b->stream;
     const int64_t G = b->G;
     b->launches = 0;
-    B_CK(cudaMemsetAsync(b->counters.p, 0, 4 * sizeof(unsigned long long), s), "memset counters");
+    B_CK(cudaMemsetAsync(b->counters.p, 0, 6 * sizeof(unsigned long long), s), "memset counters");
     B_CK(cudaMemsetAsync(b->hist.p, 0, kOrderBins * sizeof(unsigned int), s), "memset hist");
     if (G == 0) return GALOP_OK;
     const int tpb = 256;
@@ -199,11 +207,29 @@ int enqueue(galop_batch* b) {
                                            b->counters.p + 3);
         b->launches += 1;
     }
+    const bool dedup = fold && b->dedup && G > 1;
+    if (dedup) {
+        // copies within a population share the representative's fitness
+        const uint4* u4 = reinterpret_cast<const uint4*>(b->uops.p);
+        size_t tmp = b->dtmp.cap;
+        dedup_hash_kernel<<<blocks, tpb, 0, s>>>(u4, b->eff_off.p, b->eff_len.p, G, b->dkeys.p, b->dvals.p, b->rep.p,
+                                                 b->prog_pop.p);
+        B_CK(cub::DeviceRadixSort::SortPairs(b->dtmp.p, tmp, b->dkeys.p, b->dkeys_sorted.p, b->dvals.p,
+                                             b->dvals_sorted.p, (int)G, 0, 64, s), "dedup sort");
+        dedup_run_start_kernel<<<blocks, tpb, 0, s>>>(b->dkeys_sorted.p, G, b->dhead.p);
+        tmp = b->dtmp.cap;
+        B_CK(cub::DeviceScan::InclusiveScan(b->dtmp.p, tmp, b->dhead.p, b->dvals.p, cub::Max(), (int)G, s),
+             "dedup scan");
+        dedup_rep_kernel<<<blocks, tpb, 0, s>>>(b->dvals.p, b->dvals_sorted.p, G, u4, b->eff_off.p, b->eff_len.p,
+                                                b->rep.p, b->counters.p + 4, b->prog_pop.p);
+        b->launches += 5;
+    }
     batch_key_kernel<<<blocks, tpb, 0, s>>>(b->layout.p, b->prog_pop.p, b->eff_len.p, G, b->key.p);
     order_hist_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p);
     order_scan_kernel<<<1, 1024, 0, s>>>(b->hist.p);
     order_scatter_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p, b->order.p);
-    batch_item_count_kernel<<<blocks, tpb, 0, s>>>(b->order.p, b->prog_pop.p, b->chunks_of_pop.p, G, b->cnt.p);
+    batch_item_count_kernel<<<blocks, tpb, 0, s>>>(b->order.p, b->prog_pop.p, b->chunks_of_pop.p, b->key.p, G,
+                                                   b->cnt.p);
     scan_tile_sums_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(b->cnt.p, G, b->tiles.p);
     scan_tile_offsets_kernel<<<1, kScanThreads, 0, s>>>(b->tiles.p, n_tiles);
     scan_apply_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(b->cnt.p, G, b->tiles.p, n_tiles, b->item_off.p);
@@ -226,11 +252,16 @@ int enqueue(galop_batch* b) {
     a.prog_pop = b->prog_pop.p;
     a.items = b->items.p;
     a.n_items = b->n_items;
+    a.n_items_dev = dedup ? b->item_off.p + G : nullptr;
     void* params[] = {&a};
     B_CK(cudaLaunchKernel(b->interp_fn, dim3((unsigned)b->grid), dim3(b->threads), params, b->smem, s),
          "batched interpreter launch");
     batch_finalize_kernel<<<blocks, tpb, 0, s>>>(b->descs.p, b->prog_pop.p, b->first_item.p, b->partial.p, G);
     b->launches += 2;
+    if (dedup) {
+        batch_dedup_scatter_kernel<<<blocks, tpb, 0, s>>>(b->descs.p, b->prog_pop.p, b->rep.p, G);
+        b->launches += 1;
+    }
     B_CK(cudaGetLastError(), "batch finalize launch");
     return GALOP_OK;
 }
@@ -351,7 +382,22 @@ int allocate(galop_batch* b, int64_t words, int64_t offs, int64_t progs, int64_t
     if (e == cudaSuccess) e = b->tiles.ensure(T1);
     if (e == cudaSuccess) e = b->items.ensure(I1);
     if (e == cudaSuccess) e = b->partial.ensure(I1);
-    if (e == cudaSuccess) e = b->counters.ensure(4);
+    if (e == cudaSuccess) e = b->counters.ensure(6);
+    b->dedup = ctx->opt.dedup && b->fmt.wide && ctx->opt.intron_prepass && progs > 1;
+    if (b->dedup) {
+        if (e == cudaSuccess) e = b->dkeys.ensure(G1);
+        if (e == cudaSuccess) e = b->dkeys_sorted.ensure(G1);
+        if (e == cudaSuccess) e = b->dvals.ensure(G1);
+        if (e == cudaSuccess) e = b->dvals_sorted.ensure(G1);
+        if (e == cudaSuccess) e = b->rep.ensure(G1);
+        if (e == cudaSuccess) e = b->dhead.ensure(G1);
+        size_t tsort = 0, tscan = 0;
+        if (e == cudaSuccess)
+            e = cub::DeviceRadixSort::SortPairs(nullptr, tsort, b->dkeys.p, b->dkeys_sorted.p, b->dvals.p,
+                                                b->dvals_sorted.p, (int)G1, 0, 64);
+        if (e == cudaSuccess) e = cub::DeviceScan::InclusiveScan(nullptr, tscan, b->dhead.p, b->dvals.p, cub::Max(), (int)G1);
+        if (e == cudaSuccess) e = b->dtmp.ensure(std::max<size_t>(std::max(tsort, tscan), 1));
+    }
     if (e == cudaSuccess) e = b->hist.ensure(kOrderBins);
     if (e == cudaSuccess) e = b->fitness.ensure(G1);
     if (e == cudaSuccess) e = b->sse.ensure(G1);
@@ -470,6 +516,8 @@ int galop_batch_destroy(galop_batch* b) {
     b->eff_off.release(); b->item_off.release(); b->first_item.release(); b->tiles.release();
     b->lens.release(); b->prog_pop.release(); b->eff_len.release(); b->key.release(); b->order.release();
     b->cnt.release(); b->chunks_of_pop.release(); b->items.release(); b->counters.release(); b->hist.release();
+    b->dkeys.release(); b->dkeys_sorted.release(); b->dvals.release(); b->dvals_sorted.release(); b->rep.release();
+    b->dhead.release(); b->dtmp.release();
     b->fitness.release(); b->sse.release(); b->partial.release(); b->layout.release(); b->descs.release();
     for (cudaEvent_t e : {b->ev0, b->ev1, b->ev2}) if (e) cudaEventDestroy(e);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -484,6 +532,8 @@ int64_t galop_batch_device_bytes(const galop_batch* b) {
     s += (b->local_off.cap + b->starts.cap + b->eff_off.cap + b->item_off.cap + b->first_item.cap + b->tiles.cap) * 8;
     s += (b->lens.cap + b->prog_pop.cap + b->eff_len.cap + b->key.cap + b->order.cap + b->cnt.cap) * 4;
     s += (b->items.cap + b->partial.cap + b->sse.cap) * 8 + b->fitness.cap * 4;
+    s += (b->dkeys.cap + b->dkeys_sorted.cap) * 8 + (b->dvals.cap + b->dvals_sorted.cap + b->rep.cap + b->dhead.cap) * 4;
+    s += b->dtmp.cap;
     return s;
 }
 
@@ -558,11 +608,12 @@ int galop_batch_synchronize(galop_batch* b) {
         float ms = 0.0f;
         if (cudaEventElapsedTime(&ms, b->ev0, b->ev1) == cudaSuccess) b->stats.total_ms = ms;
         b->stats.interp_ms = b->stats.total_ms;
-        unsigned long long tot[3] = {0, 0, 0};
+        unsigned long long tot[5] = {0, 0, 0, 0, 0};
         B_CK(cudaMemcpy(tot, b->counters.p + 1, sizeof tot, cudaMemcpyDeviceToHost), "batch stats");
         b->stats.raw_instructions = (int64_t)tot[0];
         b->stats.eff_instructions = (int64_t)tot[1];
-        b->stats.interp_instructions = (b->fmt.wide && ctx->opt.intron_prepass) ? (int64_t)tot[2] : (int64_t)tot[1];
+        b->stats.interp_instructions =
+            (b->fmt.wide && ctx->opt.intron_prepass) ? (int64_t)(tot[2] - tot[4]) : (int64_t)tot[1];
         b->stats.kernels_launched = b->launches;
         b->stats.case_chunks = (int32_t)(b->G ? b->n_items / b->G : 0);
         b->pending = false;

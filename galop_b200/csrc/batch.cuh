@@ -65,19 +65,25 @@ static __global__ void batch_key_kernel(const PopLayout* __restrict__ pops, cons
                                         int32_t* __restrict__ key) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_total) return;
+    if (eff_len[g] < 0) {            // a copy left out by dedup: last in the order, no work items
+        key[g] = -1;
+        return;
+    }
     const double work = (double)eff_len[g] * (double)pops[prog_pop[g]].n_cases;
     int k = work >= 1.0 ? (int)(log2(work) * 64.0) + 1 : 0;
-    key[g] = k < 4095 ? k : 4095;
+    key[g] = k < 4094 ? k : 4094;
 }
 
 // Work items per program, by position in the order.
 static __global__ void batch_item_count_kernel(const int32_t* __restrict__ order,
                                                const int32_t* __restrict__ prog_pop,
-                                               const int32_t* __restrict__ chunks_of_pop, int64_t n_total,
+                                               const int32_t* __restrict__ chunks_of_pop,
+                                               const int32_t* __restrict__ key, int64_t n_total,
                                                int32_t* __restrict__ cnt) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_total) return;
-    cnt[i] = chunks_of_pop[prog_pop[order[i]]];
+    const int32_t g = order[i];
+    cnt[i] = key[g] < 0 ? 0 : chunks_of_pop[prog_pop[g]];
 }
 
 static __global__ void batch_item_fill_kernel(const int32_t* __restrict__ order,
@@ -91,6 +97,20 @@ static __global__ void batch_item_fill_kernel(const int32_t* __restrict__ order,
     const int64_t o = item_off[i];
     for (int c = 0; c < cnt[i]; ++c) items[o + c] = ((unsigned long long)g << 20) | (unsigned long long)c;
     first_item[g] = o;
+}
+
+// Copies left out by dedup take their representative's results (same
+// population, so the same output arrays).
+static __global__ void batch_dedup_scatter_kernel(const PopDesc* __restrict__ descs,
+                                                  const int32_t* __restrict__ prog_pop,
+                                                  const int32_t* __restrict__ rep, int64_t n_total) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_total) return;
+    const int32_t r = rep[g];
+    if (r == (int32_t)g) return;
+    const PopDesc d = descs[prog_pop[g]];
+    d.fitness[g - d.prog_base] = d.fitness[r - d.prog_base];
+    if (d.sse) d.sse[g - d.prog_base] = d.sse[r - d.prog_base];
 }
 
 // Programs split into case chunks: sum the chunk partials in chunk order.

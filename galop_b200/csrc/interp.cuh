@@ -78,6 +78,7 @@ struct InterpArgs {
     const int32_t* prog_pop;       // global program -> population
     const unsigned long long* items;
     int64_t n_items;
+    const int64_t* n_items_dev;    // the item count computed on the device (dedup), or null
 };
 
 #define GALOP_CASES16(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) \

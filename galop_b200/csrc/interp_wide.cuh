@@ -184,7 +184,8 @@ interp_wide_kernel(InterpArgs args) {
     __syncwarp();
 
     const int64_t n_work = args.n_skipped ? args.n_programs - (int64_t)*args.n_skipped : args.n_programs;
-    const int64_t total_items = args.pops != nullptr ? args.n_items : n_work * (int64_t)args.n_chunks;
+    const int64_t total_items = args.pops != nullptr ? (args.n_items_dev ? *args.n_items_dev : args.n_items)
+                                                     : n_work * (int64_t)args.n_chunks;
     const uint4* __restrict__ uops4 = reinterpret_cast<const uint4*>(args.uops);
 
     for (;;) {

@@ -170,7 +170,7 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
         size_t tmp = ctx->dsort_tmp.cap;
         const uint4* u4 = reinterpret_cast<const uint4*>(ctx->uops.p);
         dedup_hash_kernel<<<blocks, tpb, 0, s>>>(u4, ctx->eff_off.p, ctx->eff_len.p, n, ctx->dkeys.p, ctx->dvals.p,
-                                                 ctx->rep.p);
+                                                 ctx->rep.p, nullptr);
         GALOP_CK(cub::DeviceRadixSort::SortPairs(ctx->dsort_tmp.p, tmp, ctx->dkeys.p, ctx->dkeys_sorted.p,
                                                  ctx->dvals.p, ctx->dvals_sorted.p, (int)n, 0, 64, s), "dedup sort");
         dedup_run_start_kernel<<<blocks, tpb, 0, s>>>(ctx->dkeys_sorted.p, n, ctx->dhead.p);
@@ -178,7 +178,7 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
         GALOP_CK(cub::DeviceScan::InclusiveScan(ctx->dsort_tmp.p, tmp, ctx->dhead.p, ctx->dvals.p, cub::Max(), (int)n,
                                                 s), "dedup scan");
         dedup_rep_kernel<<<blocks, tpb, 0, s>>>(ctx->dvals.p, ctx->dvals_sorted.p, n, u4, ctx->eff_off.p,
-                                                ctx->eff_len.p, ctx->rep.p, ctx->counters.p + 4);
+                                                ctx->eff_len.p, ctx->rep.p, ctx->counters.p + 4, nullptr);
         ctx->launches += 5;
         GALOP_CK(cudaGetLastError(), "dedup launch");
     }

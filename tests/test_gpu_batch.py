@@ -128,3 +128,37 @@ def test_batch_r2_objective_matches_single_population_calls(native):
             for p in range(len(pops)):
                 assert np.array_equal(bits(b.fitness(p)), bits(single[p])), p
     assert all(f[0] > 0.9 for f in single)
+
+
+@pytest.mark.parametrize("reduce", [g.REDUCE_KAHAN32, g.REDUCE_ORDERED])
+def test_batch_copies_share_fitness_within_a_population(native, reduce):
+    """Populations full of copies (identical effective code, introns apart):
+    with dedup on, copies take their representative's fitness inside their
+    own population; every value equals the dedup-off batch bit for bit."""
+    rng = np.random.default_rng(8)
+    isa = W.IsaSpec(g.PROFILE_REF, 16)
+    base = _populations(9, [(40, 1000, 3, 4, 40), (25, 40000, 2, 8, 60), (60, 3000, 4, 2, 20)])
+    pops = []
+    for ds, w, o in base:
+        progs = [w[o[i]:o[i + 1]] for i in range(len(o) - 1)]
+        out = []
+        for _ in range(10 * len(progs)):
+            p = progs[int(rng.integers(0, len(progs)))]
+            if rng.random() < 0.5:
+                p = np.concatenate([p, W.encode([0], [15], [1], [2], [0])])     # an intron at the end
+            out.append(p)
+        pops.append((ds, np.concatenate(out).astype(np.uint32), W.csr_offsets([len(p) for p in out])))
+    fits = {}
+    for dd in (True, False):
+        with g.Evaluator(num_registers=16, reduce=reduce, dedup=dd) as ev:
+            rds = [g.ResidentDataset(ev, ds) for ds, _, _ in pops]
+            with g.Batch(ev, [(r, o.shape[0] - 1, int(o[-1])) for r, (_, _, o) in zip(rds, pops)]) as b:
+                for p, (_, w, o) in enumerate(pops):
+                    b.set_population(p, w, o)
+                b.evaluate(use_graph=dd)
+                b.synchronize()
+                fits[dd] = [b.fitness(p) for p in range(len(pops))]
+                fits[(dd, "interp")] = b.stats.interp_instructions
+    for a, c in zip(fits[True], fits[False]):
+        assert np.array_equal(bits(a), bits(c))
+    assert fits[(True, "interp")] < 0.3 * fits[(False, "interp")]
