@@ -199,10 +199,12 @@ int enqueue(galop_batch* b) {
     prepass_compact_kernel<SpanSource><<<blocks, tpb, 0, s>>>(src, G, ctx->isa, strip ? 1 : 0, b->eff_off.p,
                                                               b->uops.p, nullptr, b->fmt);
     const bool fold = b->fmt.wide && strip;
-    if (fold) {
+    if (b->fmt.wide) {
         // constants folded per program with its own population's input count
+        // (intron pass on), forwarding flags on every wide stream
         FoldParams fp{ctx->isa.profile, ctx->isa.num_registers, ctx->isa.output_reg,
-                      7u + (uint32_t)__builtin_ctz(b->fmt.stride / 128u), 0, b->descs.p, b->prog_pop.p};
+                      7u + (uint32_t)__builtin_ctz(b->fmt.stride / 128u), 0, b->descs.p, b->prog_pop.p,
+                      fold ? 1 : 0};
         fold_kernel<<<blocks, tpb, 0, s>>>(reinterpret_cast<uint4*>(b->uops.p), b->eff_off.p, G, fp, b->eff_len.p,
                                            b->counters.p + 3);
         b->launches += 1;

@@ -13,6 +13,21 @@
 // instruction reads (broadcasts read nothing), and the survivors are packed
 // to the front of the program's slot.  Per-case outputs and fitness are
 // unchanged; only case-independent work is done once instead of per case.
+//
+// Two rewrites make the survivors cheaper without changing any result:
+//   - a known value read by an instruction that is not folded becomes that
+//     instruction's constant operand: as src2 always (the constant arms
+//     compute OP(a, c) with c the register's exact value), as src1 when the
+//     op is ADD or MUL (IEEE sum and product are commutative) or LT/GT of
+//     the REF profile (a < b is b > a, both false on NaN), by swapping the
+//     operands; the broadcast that wrote the register then usually dies;
+//   - on the final order, each operand that is the previous instruction's
+//     destination is marked as forwarded (kWideFwd1 / kWideFwd2), and a
+//     result is marked to reach the register file (kWideStorePrev on the
+//     next instruction) only when something other than the next
+//     instruction's forwarded operand reads it.
+// With folding off (intron pass off) the kernel only marks forwarding:
+// every stream the interpreter loop runs carries the flags.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -31,7 +46,134 @@ struct FoldParams {
     int num_inputs;              // single population; or per program through pops/prog_pop
     const PopDesc* pops;
     const int32_t* prog_pop;
+    int fold;                    // 0: forwarding flags only (no folding, no dead-code removal)
 };
+
+// Operand swap that keeps the result bits: ADD, MUL, and LT <-> GT of REF.
+__device__ __forceinline__ bool swaps(int profile, uint32_t op) {
+    return op == kAdd || op == kMul || (profile == kProfileRef && (op == kOp6 || op == kOp7));
+}
+
+// Forwarding flags over a program u[0, n) in its final order (see the
+// micro-op format in isa.cuh).  The interpreter loop keeps the last result
+// in registers; an instruction takes it as src1 (binary ops, fwd1) or src2
+// (unary ops, fwd2) when that operand is the previous destination, and a
+// binary op whose src2 is the previous destination swaps its operands first
+// where that keeps the result bits (swaps).  The previous result is written
+// to the register file (store_prev on this instruction) unless this
+// instruction is its only reader: it takes the value forwarded, loads no
+// copy of it, and the value is not read after it (overwritten by it, or
+// dead below it; the output register counts as read after the last
+// instruction).  The first instruction carries no flag: every pass over the
+// cases starts there with nothing pending.  The last result is always
+// stored by the interpreter after the last instruction.
+__device__ __forceinline__ void mark_forwarding(uint4* __restrict__ u, int64_t n, uint32_t sh, int output_reg,
+                                                int profile) {
+    for (int64_t j = 1; j < n; ++j) {
+        uint4 w = u[j];
+        if (w.w == kWideBcast) continue;
+        const uint32_t prev = u[j - 1].z;
+        const bool reg2 = !(w.w & 8u);
+        if (w.w & kWideSpecial) {
+            if (reg2 && w.y == prev) w.w |= kWideFwd2;
+        } else {
+            const uint32_t op = w.w & 7u;
+            if (w.x != prev && reg2 && w.y == prev && swaps(profile, op)) {
+                const uint32_t sop = op == kOp6 ? (uint32_t)kOp7 : op == kOp7 ? (uint32_t)kOp6 : op;
+                const uint32_t x = w.x;
+                w.x = w.y;
+                w.y = x;
+                w.w = (w.w & ~7u) | sop;
+            }
+            if (w.x == prev) w.w |= kWideFwd1;
+        }
+        u[j] = w;
+    }
+    uint32_t live = 1u << output_reg;      // live after instruction j
+    uint32_t live_after_next = 0u;
+    for (int64_t j = n - 1; j >= 0; --j) {
+        const uint4 w = u[j];
+        const uint32_t d = w.z >> sh;
+        const bool bcast = (w.w & ~kWideFlags) == kWideBcast;
+        if (j < n - 1) {
+            const uint4 nx = u[j + 1];
+            const uint32_t nd = nx.z >> sh;
+            const bool fwd = (nx.w & (kWideFwd1 | kWideFwd2)) != 0;
+            const bool loads_d = !(nx.w & kWideSpecial) && !(nx.w & 8u) && (nx.y >> sh) == d &&
+                                 (nx.w & ~kWideFlags) != kWideBcast;
+            const bool read_later = d != nd && ((live_after_next >> d) & 1u);
+            if (!(fwd && !loads_d && !read_later)) u[j + 1].w = nx.w | kWideStorePrev;
+        }
+        live_after_next = live;
+        live &= ~(1u << d);
+        if (!bcast) {
+            if (!(w.w & kWideSpecial)) live |= 1u << (w.x >> sh);
+            if (!(w.w & 8u)) live |= 1u << (w.y >> sh);
+        }
+    }
+}
+
+// Folds one program in place (constants, dead code, packing, forwarding
+// flags) and returns its interpreted length.
+__device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L, const FoldParams& fp,
+                                                 int k_in) {
+    const uint32_t sh = fp.stride_shift;
+    int64_t kept = 0;
+    float vals[kMaxRegisters];
+    uint32_t known = 0;
+    for (int r = 0; r < fp.num_registers; ++r) {
+        vals[r] = 0.0f;
+        if (r >= k_in) known |= 1u << r;
+    }
+    // forward: evaluate what is known
+    for (int64_t j = 0; j < L; ++j) {
+        const uint4 w = u[j];
+        const uint32_t op = w.w & 7u;
+        const bool is_const = (w.w & 8u) != 0;
+        const bool unary = (w.w & kWideSpecial) != 0;
+        const uint32_t s1 = w.x >> sh, s2 = w.y >> sh, d = w.z >> sh;
+        const bool a_known = unary || ((known >> s1) & 1u);
+        const bool b_known = is_const || ((known >> s2) & 1u);
+        if (a_known && b_known) {
+            const float a = unary ? 0.0f : vals[s1];
+            const float b = is_const ? __uint_as_float(w.y) : vals[s2];
+            const float v = fp.profile == kProfileBj ? apply_op<kProfileBj>(op, a, b)
+                                                     : apply_op<kProfileRef>(op, a, b);
+            vals[d] = v;
+            known |= 1u << d;
+            u[j] = make_uint4(0u, __float_as_uint(v), w.z, kWideBcast);
+        } else {
+            if (!unary && b_known && !is_const) {
+                u[j] = make_uint4(w.x, __float_as_uint(vals[s2]), w.z, w.w | 8u);
+            } else if (!unary && a_known && swaps(fp.profile, op)) {
+                const uint32_t sop = op == kOp6 ? (uint32_t)kOp7 : op == kOp7 ? (uint32_t)kOp6 : op;
+                u[j] = make_uint4(w.y, __float_as_uint(vals[s1]), w.z, (w.w & ~7u) | sop | 8u);
+            }
+            known &= ~(1u << d);
+        }
+    }
+    // backward: drop what nothing reads
+    uint32_t live = 1u << fp.output_reg;
+    for (int64_t j = L - 1; j >= 0; --j) {
+        const uint4 w = u[j];
+        const uint32_t d = w.z >> sh;
+        if (!((live >> d) & 1u)) {
+            u[j].w = kWideDead;
+            continue;
+        }
+        live &= ~(1u << d);
+        if (w.w != kWideBcast) {
+            if (!(w.w & kWideSpecial)) live |= 1u << (w.x >> sh);
+            if (!(w.w & 8u)) live |= 1u << (w.y >> sh);
+        }
+    }
+    for (int64_t j = 0; j < L; ++j) {
+        const uint4 w = u[j];
+        if (w.w != kWideDead) u[kept++] = w;
+    }
+    mark_forwarding(u, kept, sh, fp.output_reg, fp.profile);
+    return kept;
+}
 
 static __global__ void fold_kernel(uint4* __restrict__ uops, const int64_t* __restrict__ eff_off, int64_t n,
                                    FoldParams fp, int32_t* __restrict__ interp_len,
@@ -44,53 +186,13 @@ static __global__ void fold_kernel(uint4* __restrict__ uops, const int64_t* __re
         uint4* __restrict__ u = uops + p0;
         const uint32_t sh = fp.stride_shift;
         const int k_in = fp.pops ? fp.pops[fp.prog_pop[i]].num_inputs : fp.num_inputs;
-        float vals[kMaxRegisters];
-        uint32_t known = 0;
-        for (int r = 0; r < fp.num_registers; ++r) {
-            vals[r] = 0.0f;
-            if (r >= k_in) known |= 1u << r;
+        if (!fp.fold) {
+            mark_forwarding(u, L, sh, fp.output_reg, fp.profile);
+            interp_len[i] = (int32_t)L;
+        } else {
+            kept = fold_program(u, L, fp, k_in);
+            interp_len[i] = (int32_t)kept;
         }
-        // forward: evaluate what is known
-        for (int64_t j = 0; j < L; ++j) {
-            const uint4 w = u[j];
-            const uint32_t op = w.w & 7u;
-            const bool is_const = (w.w & 8u) != 0;
-            const bool unary = (w.w & kWideSpecial) != 0;
-            const uint32_t s1 = w.x >> sh, s2 = w.y >> sh, d = w.z >> sh;
-            const bool a_known = unary || ((known >> s1) & 1u);
-            const bool b_known = is_const || ((known >> s2) & 1u);
-            if (a_known && b_known) {
-                const float a = unary ? 0.0f : vals[s1];
-                const float b = is_const ? __uint_as_float(w.y) : vals[s2];
-                const float v = fp.profile == kProfileBj ? apply_op<kProfileBj>(op, a, b)
-                                                         : apply_op<kProfileRef>(op, a, b);
-                vals[d] = v;
-                known |= 1u << d;
-                u[j] = make_uint4(0u, __float_as_uint(v), w.z, kWideBcast);
-            } else {
-                known &= ~(1u << d);
-            }
-        }
-        // backward: drop what nothing reads
-        uint32_t live = 1u << fp.output_reg;
-        for (int64_t j = L - 1; j >= 0; --j) {
-            const uint4 w = u[j];
-            const uint32_t d = w.z >> sh;
-            if (!((live >> d) & 1u)) {
-                u[j].w = kWideDead;
-                continue;
-            }
-            live &= ~(1u << d);
-            if (w.w != kWideBcast) {
-                if (!(w.w & kWideSpecial)) live |= 1u << (w.x >> sh);
-                if (!(w.w & 8u)) live |= 1u << (w.y >> sh);
-            }
-        }
-        for (int64_t j = 0; j < L; ++j) {
-            const uint4 w = u[j];
-            if (w.w != kWideDead) u[kept++] = w;
-        }
-        interp_len[i] = (int32_t)kept;
     }
     __shared__ unsigned long long sk;
     if (threadIdx.x == 0) sk = 0;

@@ -19,8 +19,11 @@ Emitted for NR in {8, 16} and K in {1, 2, 4, 8}:
            load a (and b) from the shared-memory register file, compute,
            store t -- the table index is op | constant-src2 << 3, and
            protected DIV is one of the arms
-  wide loop  the same arms as one PTX loop over consecutive binary
-           instructions (returns at the first unary op or window end)
+  wide loop  the same ops as one PTX loop over consecutive binary
+           instructions (returns at the first unary op or window end), with
+           the last result kept in registers: forwarded src1 operands are
+           not loaded and results only reach the register file when the
+           next instruction's store_prev flag asks for it
   both wide forms also have the broadcast arm (table index 12): t[k] = the
   micro-op's constant, for instructions folded by the pre-pass
 where OP is one of the single-instruction ops: ADD, SUB, MUL (add/sub/mul
@@ -131,11 +134,15 @@ def cheap_table(k: int, profile: int) -> str:
 
 
 # Scratch registers of the wide arms (declared once per asm block).
-WIDE_TEMPS = ".reg .pred dp, dn, dz; .reg .f32 da, db, dq; .reg .b32 ds;"
+WIDE_TEMPS = ".reg .pred dp, dn, dz; .reg .f32 da, db, dq; .reg .b32 ds, dbb;"
 
 
-def wide_body(k: int, op: int, const: bool) -> list[str]:
+def wide_body(k: int, op: int, const: bool, a=None, b=None, t=None) -> list[str]:
     """t[q] = OP(a[q], b[q]) (b = the scalar c for a constant src2).
+
+    a, b, t map q to register names (default a{q}, b{q}, t{q}); t[q] is
+    written once, after the last read of a[q] and b[q], so an operand may be
+    the result register itself (a forwarded operand).
 
     DIV is b != 0 ? a / b : 1.0 (src/ISA.h:224) with IEEE round-to-nearest
     (div.rn.f32), evaluated as:
@@ -146,25 +153,31 @@ def wide_body(k: int, op: int, const: bool) -> list[str]:
       otherwise div.rn on (a, b), with a zero dividend or divisor replaced by
       1.0 so the division only ever sees the operands whose quotient is used.
     Zero dividends are common in LGP code (LT/GT results, x - x)."""
+    a = a or (lambda q: f"a{q}")
+    t = t or (lambda q: f"t{q}")
+    if const:
+        b = lambda q: "c"
+    else:
+        b = b or (lambda q: f"b{q}")
     out = []
     for q in range(k):
-        bq = "c" if const else f"b{q}"
+        aq, bq, tq = a(q), b(q), t(q)
         if op != 3:
-            out.append(f"{CHEAP[op]} t{q}, a{q}, {bq};")
+            out.append(f"{CHEAP[op]} {tq}, {aq}, {bq};")
             continue
         out += [f"setp.neu.f32 dp, {bq}, 0f00000000;",
                 f"setp.num.f32 dn, {bq}, {bq};",
-                f"setp.eq.and.f32 dz, a{q}, 0f00000000, dn;",
-                f"selp.f32 da, 0f3F800000, a{q}, dz;",
+                f"setp.eq.and.f32 dz, {aq}, 0f00000000, dn;",
+                f"selp.f32 da, 0f3F800000, {aq}, dz;",
                 f"selp.f32 db, {bq}, 0f3F800000, dp;",
                 "div.rn.f32 dq, da, db;",
-                f"mov.b32 ds, a{q};",
-                f"mov.b32 t{q}, {bq};",          # t as bit scratch until the select below
-                f"xor.b32 ds, ds, t{q};",
+                f"mov.b32 ds, {aq};",
+                f"mov.b32 dbb, {bq};",
+                "xor.b32 ds, ds, dbb;",
                 "and.b32 ds, ds, 0x80000000;",
-                f"selp.f32 t{q}, dq, 0f3F800000, dp;",
+                f"selp.f32 {tq}, dq, 0f3F800000, dp;",
                 "and.pred dz, dz, dp;",
-                f"@dz mov.b32 t{q}, ds;"]
+                f"@dz mov.b32 {tq}, ds;"]
     return out
 
 
@@ -222,52 +235,80 @@ def wide_loop(k: int, profile: int) -> str:
     until a micro-op whose word w is negative (a unary op or the window's end
     marker); return with %0 pointing at it.
 
+    Operands: %0 the micro-op address (in/out); %1..%K the lane's K values of
+    the last result (in/out); %K+1 the register-file address that result
+    belongs to (in/out); %K+2 the lane's register-file base.  The caller's
+    unary ops and the next call continue from the same result registers.
+
+    The result registers double as the src1 registers: an arm computes
+    a = OP(a, b).  Each (op, constant src2) arm has three entry points, in
+    this order: S stores the pending result to its register, L loads src1,
+    F loads src2 (register arms) then computes, remembers the destination
+    address and jumps on; a fourth, G, stores and jumps to F.  The jump
+    table has 64 entries, indexed by w's low 6 bits (op | const << 3 |
+    fwd1 << 4 | store_prev << 5):
+      store_prev, not fwd1 -> S     neither -> L
+      fwd1, not store_prev -> F     both    -> G
+    The broadcast arm (index 12, | 32) has S and L only: a = the constant.
+
     Two copies of the loop body alternate between two micro-op register sets
     (u, v): each body prefetches the next micro-op into the other set, so no
-    micro-op is ever copied between registers.  %1 is the lane's register-file
-    base address.  The arms are those of wide_ops."""
+    micro-op is ever copied between registers."""
     v = min(k, 4)
     nq = k // v
     ops = tuple(sorted(PROFILES[profile] + (3,)))
     vs = "" if v == 1 else f".v{v}"
+    A = lambda q: f"%{1 + q}"
+    PT = f"%{k + 1}"
+    base = f"%{k + 2}"
 
-    def ld(dst: str, addr: str) -> list[str]:
-        return [f"ld.shared{vs}.f32 {_vec([f'{dst}{q * v + e}' for e in range(v)])}, [{addr}+{q * 128 * v}];"
+    def ld(names, addr: str) -> list[str]:
+        return [f"ld.shared{vs}.f32 {_vec([names(q * v + e) for e in range(v)])}, [{addr}+{q * 128 * v}];"
                 for q in range(nq)]
 
     def st(addr: str) -> list[str]:
-        return [f"st.shared{vs}.f32 [{addr}+{q * 128 * v}], {_vec([f't{q * v + e}' for e in range(v)])};"
+        return [f"st.shared{vs}.f32 [{addr}+{q * 128 * v}], {_vec([A(q * v + e) for e in range(v)])};"
                 for q in range(nq)]
 
-    def body(op: int, const: bool) -> list[str]:
-        return wide_body(k, op, const)
-
-    regs = ", ".join(f"{n}<{k}>" for n in "abt")
-    L = [f".reg .f32 {regs}, c;", WIDE_TEMPS, ".reg .pred q;",
-         ".reg .u32 ux, uy, uz, uw, vx, vy, vz, vw, pa, pb, pt;",
+    bregs = lambda q: f"b{q}"
+    L = [f".reg .f32 b<{k}>, c;", WIDE_TEMPS, ".reg .pred q;",
+         ".reg .u32 ux, uy, uz, uw, vx, vy, vz, vw, pa, pb;",
          "ld.shared.v4.u32 {ux, uy, uz, uw}, [%0];"]
+    entry = {(1, 0): "S", (0, 0): "L", (0, 1): "F", (1, 1): "G"}
     for cur, nxt, here, there in (("u", "v", "A", "B"), ("v", "u", "B", "A")):
         x, y, z, w = (f"{cur}{f}" for f in "xyzw")
         L += [f"L{here}%=: setp.lt.s32 q, {w}, 0;", "@q bra.uni D%=;",
               f"ld.shared.v4.u32 {{{nxt}x, {nxt}y, {nxt}z, {nxt}w}}, [%0+16];",
-              "add.u32 %0, %0, 16;",
-              f"add.u32 pa, %1, {x};", f"add.u32 pb, %1, {y};", f"add.u32 pt, %1, {z};", f"mov.b32 c, {y};"]
-        L += ld("a", "pa")
-        targets = [f"R{here}{op}_%=" if op in ops else f"D%=" for op in range(8)] + \
-                  [f"C{here}{op}_%=" if op in ops else (f"B{here}_%=" if op == BCAST_OP else f"D%=")
-                   for op in range(8)]
+              "add.u32 %0, %0, 16;", f"mov.b32 c, {y};"]
+        nxt_jump = [f"add.u32 {PT}, {base}, {z};", f"bra.uni L{there}%=;"]
+        targets = []
+        for idx in range(64):
+            op, cst, f1, sp = idx & 7, (idx >> 3) & 1, (idx >> 4) & 1, (idx >> 5) & 1
+            if op == BCAST_OP and cst and not f1:
+                targets.append(f"{'S' if sp else 'L'}{here}B_%=")
+            elif op in ops:
+                targets.append(f"{entry[(sp, f1)]}{here}{op}{cst}_%=")
+            else:
+                targets.append("D%=")
         L += [f"T{here}%=: .branchtargets " + ", ".join(targets) + ";", f"brx.idx.uni {w}, T{here}%=;"]
         for op in ops:
-            L.append(f"R{here}{op}_%=: " + " ".join(ld("b", "pb") + body(op, False) + st("pt"))
-                     + f" bra.uni L{there}%=;")
-            L.append(f"C{here}{op}_%=: " + " ".join(body(op, True) + st("pt")) + f" bra.uni L{there}%=;")
-        L.append(f"B{here}_%=: " + " ".join([f"mov.f32 t{q}, c;" for q in range(k)] + st("pt"))
-                 + f" bra.uni L{there}%=;")
+            for cst in (0, 1):
+                nm = f"{here}{op}{cst}_%="
+                L.append(f"S{nm}: " + " ".join(st(PT)))
+                L.append(f"L{nm}: " + " ".join([f"add.u32 pa, {base}, {x};"] + ld(A, "pa")))
+                body = [] if cst else [f"add.u32 pb, {base}, {y};"] + ld(bregs, "pb")
+                body += wide_body(k, op, bool(cst), a=A, b=bregs, t=A)
+                L.append(f"F{nm}: " + " ".join(body + nxt_jump))
+                L.append(f"G{nm}: " + " ".join(st(PT) + [f"bra.uni F{nm};"]))
+        L.append(f"S{here}B_%=: " + " ".join(st(PT)))
+        L.append(f"L{here}B_%=: " + " ".join([f"mov.f32 {A(q)}, c;" for q in range(k)] + nxt_jump))
     L.append("D%=:")
     text = "\\n\\t".join(L)
-    return ("    static __device__ __forceinline__ void run(uint32_t& sp, uint32_t base) {\n"
+    outs = ", ".join(['"+r"(sp)'] + [f'"+f"(a[{q}])' for q in range(k)] + ['"+r"(pt)'])
+    return (f"    static __device__ __forceinline__ void run(uint32_t& sp, float (&a)[{k}], uint32_t& pt, "
+            f"uint32_t base) {{\n"
             f'    asm volatile("{{\\n\\t{text}\\n\\t}}"\n'
-            '        : "+r"(sp)\n        : "r"(base)\n        : "memory");\n    }\n')
+            f'        : {outs}\n        : "r"(base)\n        : "memory");\n    }}\n')
 
 
 def main() -> None:

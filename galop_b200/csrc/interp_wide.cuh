@@ -11,10 +11,17 @@
 //     window is staged in shared memory; the next micro-op is prefetched
 //     into a second register set, the loop body existing twice),
 //   a sign test (unary ops and the window end leave the loop),
-//   three address adds, the src1 load, and one jump table (16 arms: 8 ops x
-//     register/constant src2) whose arm loads src2, computes and stores.
-// The unary ops (SIN/COS, and EXP/LOG of the BJ profile) run in C++ on the
-// slow branch with the CUDA math library.
+//   one jump table (16 arms: 8 ops x register/constant src2, each with
+//     entry points that skip what the micro-op's flags make unnecessary)
+//     whose arm stores the previous result if the flags ask for it, loads
+//     src1 unless it is the previous result, loads src2 (register arms),
+//     and computes into the result registers, which are also the src1
+//     registers.
+// The result registers a[K] and the address of the register they belong to
+// live across the whole pass: the unary ops (SIN/COS, and EXP/LOG of the BJ
+// profile), which run in C++ on the slow branch with the CUDA math library,
+// read and write them too, and the last result is stored after the last
+// instruction.  The folding pass sets the flags (isa.cuh, fold.cuh).
 //
 // Semantics are those of interp.cuh (src/Interpreter.cpp:36-59,
 // src/ISA.h:219-231, src/Evaluator.cpp:11-45 and :88-91).
@@ -224,6 +231,10 @@ interp_wide_kernel(InterpArgs args) {
             }
             if constexpr (MODE == kModeTrace) wide_trace<NR, K>(args.trace, 0, base, lane);
 
+            float a[K];       // result of the last instruction executed
+            uint32_t pt = 0;  // its register's address
+#pragma unroll
+            for (int k = 0; k < K; ++k) a[k] = 0.0f;
             for (int64_t wb = 0; wb < L; wb += 32) {
                 const int64_t n = (L - wb < 32) ? L - wb : 32;
                 const uint4 mine = (lane < n) ? __ldg(pw + wb + lane) : kEnd4;
@@ -236,33 +247,52 @@ interp_wide_kernel(InterpArgs args) {
                         // One instruction at a time, the register file dumped after each.
                         u = lds_u4(sp);
                         while ((int32_t)u.w >= 0) {
-                            WideOps<K, PROFILE>::run(u.w, base + u.x, base + u.y, base + u.z, u.y);
+                            // every result is stored here: the flags do not apply
+                            WideOps<K, PROFILE>::run(u.w & 15u, base + u.x, base + u.y, base + u.z, u.y);
                             wide_trace<NR, K>(args.trace, wb + (sp - stage) / 16u + 1, base, lane);
                             sp += 16u;
                             u = lds_u4(sp);
                         }
                     } else {
                         // Every binary instruction up to the next unary op or the end marker.
-                        WideLoop<K, PROFILE>::run(sp, base);
+                        WideLoop<K, PROFILE>::run(sp, a, pt, base);
                         u = lds_u4(sp);
                     }
                     if (u.w == kWideEnd) break;
-                    // Unary op on src2 (register or constant).
-                    float b[K], t[K];
-                    if (u.w & 8u) {
-                        const float c = __uint_as_float(u.y);
+                    // Unary op on src2 (register, constant or the previous result).
+                    float b[K];
+                    if constexpr (MODE == kModeTrace) {
+                        if (u.w & 8u) {
+                            const float c = __uint_as_float(u.y);
 #pragma unroll
-                        for (int k = 0; k < K; ++k) b[k] = c;
-                    } else {
-                        WR::load(base + u.y, b);
-                    }
-                    slow_op<K, PROFILE>(u.w & 7u, b, b, t);
-                    WR::store(base + u.z, t);
-                    if constexpr (MODE == kModeTrace)
+                            for (int k = 0; k < K; ++k) b[k] = c;
+                        } else {
+                            WR::load(base + u.y, b);
+                        }
+                        slow_op<K, PROFILE>(u.w & 7u, b, b, a);
+                        WR::store(base + u.z, a);
                         wide_trace<NR, K>(args.trace, wb + (sp - stage) / 16u + 1, base, lane);
+                    } else {
+                        if (u.w & kWideStorePrev) WR::store(pt, a);
+                        if (u.w & 8u) {
+                            const float c = __uint_as_float(u.y);
+#pragma unroll
+                            for (int k = 0; k < K; ++k) b[k] = c;
+                        } else if (u.w & kWideFwd2) {
+#pragma unroll
+                            for (int k = 0; k < K; ++k) b[k] = a[k];
+                        } else {
+                            WR::load(base + u.y, b);
+                        }
+                        slow_op<K, PROFILE>(u.w & 7u, b, b, a);
+                        pt = base + u.z;
+                    }
                     sp += 16u;
                 }
                 __syncwarp();
+            }
+            if constexpr (MODE != kModeTrace) {
+                if (L > 0) WR::store(pt, a);   // the last result
             }
 
             float o[K];

@@ -69,10 +69,25 @@ __host__ __device__ __forceinline__ uint32_t encode_uop(const Decoded& d) {
 //   x = src1 * stride            (0 for unary ops)
 //   y = src2 * stride, or the constant's bits when src2 is a constant
 //   z = dest * stride
-//   w = op | const << 3 | unary << 31   (kWideEnd ends a window)
+//   w = op | const << 3 | fwd1 << 4 | store_prev << 5 | fwd2 << 6
+//       | unary << 31   (kWideEnd ends a window)
 // stride = bytes per register per warp (32 lanes x K cases x 4 bytes).
+// The flag bits describe the program's final instruction order (fold.cuh
+// sets them) for the interpreter loop, which keeps the last result in
+// registers and writes it to the register file only when the next
+// instruction says so:
+//   fwd1        src1 (binary op) is the previous instruction's destination:
+//               the operand is the previous result, not loaded;
+//   fwd2        the same for src2 of a unary op;
+//   store_prev  the previous result must reach the register file (something
+//               other than this instruction's forwarded operand reads it);
+//               it is stored before this instruction reads any operand.
 constexpr uint32_t kWideSpecial = 0x80000000u;
 constexpr uint32_t kWideEnd = 0xFFFFFFFFu;
+constexpr uint32_t kWideFwd1 = 16u;
+constexpr uint32_t kWideStorePrev = 32u;
+constexpr uint32_t kWideFwd2 = 64u;
+constexpr uint32_t kWideFlags = kWideFwd1 | kWideStorePrev | kWideFwd2;
 // Broadcast micro-op (table slot 12): dest = the constant in y, for an
 // instruction whose operands are all known before any case is read.
 constexpr uint32_t kWideBcast = 12u;

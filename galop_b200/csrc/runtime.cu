@@ -142,11 +142,13 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
         ctx->launches += 1;
     }
     // Constant folding (wide micro-ops of effective code only; the raw-word
-    // output of galop_effective_csr keeps the intron pass's result as is).
+    // output of galop_effective_csr keeps the intron pass's result as is),
+    // and the forwarding flags every wide stream carries (fold.cuh).
     ctx->folded = fmt.wide && strip && raw_out == nullptr && n > 0;
-    if (ctx->folded) {
+    if (fmt.wide && raw_out == nullptr && n > 0) {
         FoldParams fp{ctx->isa.profile, ctx->isa.num_registers, ctx->isa.output_reg,
-                      7u + (uint32_t)__builtin_ctz((unsigned)pick_k(ctx)), ctx->num_inputs, nullptr, nullptr};
+                      7u + (uint32_t)__builtin_ctz((unsigned)pick_k(ctx)), ctx->num_inputs, nullptr, nullptr,
+                      ctx->folded ? 1 : 0};
         fold_kernel<<<blocks, tpb, 0, s>>>(reinterpret_cast<uint4*>(ctx->uops.p), ctx->eff_off.p, n, fp,
                                            ctx->eff_len.p, ctx->counters.p + 3);
         ctx->launches += 1;
