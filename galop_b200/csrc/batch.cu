@@ -78,6 +78,7 @@ struct galop_batch {
     DevBuf<uint32_t> arena, uops;
     DevBuf<int64_t> local_off, starts, eff_off, item_off, first_item, tiles;
     DevBuf<int32_t> lens, prog_pop, eff_len, key, order, cnt, chunks_of_pop;
+    DevBuf<uint32_t> livein;
     // dedup within each population (dedup.cuh)
     DevBuf<unsigned long long> dkeys, dkeys_sorted;
     DevBuf<int32_t> dvals, dvals_sorted, rep, dhead;
@@ -206,6 +207,7 @@ int enqueue(galop_batch* b) {
                       7u + (uint32_t)__builtin_ctz(b->fmt.stride / 128u), 0, b->descs.p, b->prog_pop.p,
                       fold ? 1 : 0};
         fold_kernel<<<blocks, tpb, 0, s>>>(reinterpret_cast<uint4*>(b->uops.p), b->eff_off.p, G, fp, b->eff_len.p,
+                                           b->livein.p,
                                            b->counters.p + 3);
         b->launches += 1;
     }
@@ -244,6 +246,7 @@ int enqueue(galop_batch* b) {
     a.uops = b->uops.p;
     a.eff_off = b->eff_off.p;
     a.interp_len = fold ? b->eff_len.p : nullptr;
+    a.livein = b->fmt.wide ? b->livein.p : nullptr;
     a.n_programs = G;
     a.n_chunks = 1;
     a.output_reg = ctx->isa.output_reg;
@@ -375,6 +378,7 @@ int allocate(galop_batch* b, int64_t words, int64_t offs, int64_t progs, int64_t
     if (e == cudaSuccess) e = b->lens.ensure(G1);
     if (e == cudaSuccess) e = b->prog_pop.ensure(G1);
     if (e == cudaSuccess) e = b->eff_len.ensure(G1);
+    if (e == cudaSuccess) e = b->livein.ensure(G1);
     if (e == cudaSuccess) e = b->eff_off.ensure(G1 + 1);
     if (e == cudaSuccess) e = b->key.ensure(G1);
     if (e == cudaSuccess) e = b->order.ensure(G1);
@@ -516,7 +520,7 @@ int galop_batch_destroy(galop_batch* b) {
     drop_graph(b);
     b->arena.release(); b->uops.release(); b->local_off.release(); b->starts.release();
     b->eff_off.release(); b->item_off.release(); b->first_item.release(); b->tiles.release();
-    b->lens.release(); b->prog_pop.release(); b->eff_len.release(); b->key.release(); b->order.release();
+    b->lens.release(); b->prog_pop.release(); b->eff_len.release(); b->livein.release(); b->key.release(); b->order.release();
     b->cnt.release(); b->chunks_of_pop.release(); b->items.release(); b->counters.release(); b->hist.release();
     b->dkeys.release(); b->dkeys_sorted.release(); b->dvals.release(); b->dvals_sorted.release(); b->rep.release();
     b->dhead.release(); b->dtmp.release();
@@ -532,7 +536,7 @@ int64_t galop_batch_device_bytes(const galop_batch* b) {
     int64_t s = 0;
     s += (b->arena.cap + b->uops.cap) * 4;
     s += (b->local_off.cap + b->starts.cap + b->eff_off.cap + b->item_off.cap + b->first_item.cap + b->tiles.cap) * 8;
-    s += (b->lens.cap + b->prog_pop.cap + b->eff_len.cap + b->key.cap + b->order.cap + b->cnt.cap) * 4;
+    s += (b->lens.cap + b->prog_pop.cap + b->eff_len.cap + b->livein.cap + b->key.cap + b->order.cap + b->cnt.cap) * 4;
     s += (b->items.cap + b->partial.cap + b->sse.cap) * 8 + b->fitness.cap * 4;
     s += (b->dkeys.cap + b->dkeys_sorted.cap) * 8 + (b->dvals.cap + b->dvals_sorted.cap + b->rep.cap + b->dhead.cap) * 4;
     s += b->dtmp.cap;

@@ -91,6 +91,7 @@ struct galop_ctx {
     DevBuf<uint8_t> raw_lens8;
     DevBuf<int64_t> raw_off, eff_off, tiles;
     DevBuf<int32_t> eff_len, order;
+    DevBuf<uint32_t> livein;      // registers each program reads before writing them (fold.cuh)
     DevBuf<float> fitness, outputs, trace;
     DevBuf<double> sse, partial;
     DevBuf<unsigned long long> counters;   // [0] queue head, [1..2] totals
@@ -100,6 +101,7 @@ struct galop_ctx {
     galop_stats stats{};
     int launches = 0;
     bool stats_pending = false;   // device-path call whose timings are not read yet
+    bool flagged = false;         // the last pre-pass marked forwarding and live-in registers
     bool folded = false;          // the last pre-pass folded constants (interp lengths in eff_len)
     bool deduped = false;         // ... and left identical programs out (representatives in rep)
     DevBuf<unsigned long long> dkeys, dkeys_sorted;

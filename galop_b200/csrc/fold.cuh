@@ -65,10 +65,14 @@ __device__ __forceinline__ bool swaps(int profile, uint32_t op) {
 // copy of it, and the value is not read after it (overwritten by it, or
 // dead below it; the output register counts as read after the last
 // instruction).  The first instruction carries no flag: every pass over the
-// cases starts there with nothing pending.  The last result is always
-// stored by the interpreter after the last instruction.
-__device__ __forceinline__ void mark_forwarding(uint4* __restrict__ u, int64_t n, uint32_t sh, int output_reg,
-                                                int profile) {
+// cases starts there with nothing pending.  The last result is never
+// stored: the interpreter takes the output from it when the last
+// instruction wrote the output register.
+// Returns the registers the program reads before writing them (the
+// output register counts as read after the last instruction): the only
+// ones the interpreter must initialise before each pass over the cases.
+__device__ __forceinline__ uint32_t mark_forwarding(uint4* __restrict__ u, int64_t n, uint32_t sh, int output_reg,
+                                                    int profile) {
     for (int64_t j = 1; j < n; ++j) {
         uint4 w = u[j];
         if (w.w == kWideBcast) continue;
@@ -111,12 +115,13 @@ __device__ __forceinline__ void mark_forwarding(uint4* __restrict__ u, int64_t n
             if (!(w.w & 8u)) live |= 1u << (w.y >> sh);
         }
     }
+    return live;
 }
 
 // Folds one program in place (constants, dead code, packing, forwarding
-// flags) and returns its interpreted length.
+// flags), returns its interpreted length and sets its live-in registers.
 __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L, const FoldParams& fp,
-                                                 int k_in) {
+                                                 int k_in, uint32_t& livein) {
     const uint32_t sh = fp.stride_shift;
     int64_t kept = 0;
     float vals[kMaxRegisters];
@@ -171,13 +176,13 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
         const uint4 w = u[j];
         if (w.w != kWideDead) u[kept++] = w;
     }
-    mark_forwarding(u, kept, sh, fp.output_reg, fp.profile);
+    livein = mark_forwarding(u, kept, sh, fp.output_reg, fp.profile);
     return kept;
 }
 
 static __global__ void fold_kernel(uint4* __restrict__ uops, const int64_t* __restrict__ eff_off, int64_t n,
                                    FoldParams fp, int32_t* __restrict__ interp_len,
-                                   unsigned long long* __restrict__ total) {
+                                   uint32_t* __restrict__ livein, unsigned long long* __restrict__ total) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t kept = 0;
     if (i < n) {
@@ -187,10 +192,12 @@ static __global__ void fold_kernel(uint4* __restrict__ uops, const int64_t* __re
         const uint32_t sh = fp.stride_shift;
         const int k_in = fp.pops ? fp.pops[fp.prog_pop[i]].num_inputs : fp.num_inputs;
         if (!fp.fold) {
-            mark_forwarding(u, L, sh, fp.output_reg, fp.profile);
+            livein[i] = mark_forwarding(u, L, sh, fp.output_reg, fp.profile);
             interp_len[i] = (int32_t)L;
         } else {
-            kept = fold_program(u, L, fp, k_in);
+            uint32_t in = 0u;
+            kept = fold_program(u, L, fp, k_in, in);
+            livein[i] = in;
             interp_len[i] = (int32_t)kept;
         }
     }

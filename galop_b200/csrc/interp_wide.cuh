@@ -204,6 +204,8 @@ interp_wide_kernel(InterpArgs args) {
         const int64_t p0 = args.eff_off[w.prog];
         const int64_t L = args.interp_len ? (int64_t)args.interp_len[w.prog] : args.eff_off[w.prog + 1] - p0;
         const uint4* __restrict__ pw = uops4 + p0;
+        const uint32_t livein = (MODE == kModeTrace || args.livein == nullptr) ? (1u << NR) - 1u
+                                                                              : args.livein[w.prog];
 
         float ks = 0.0f, kc = 0.0f;
         double big = 0.0;
@@ -212,8 +214,10 @@ interp_wide_kernel(InterpArgs args) {
         for (int64_t cb = w.cbeg; cb < w.cend; cb += kPass) {
             // Case of element q*V+e of this lane: cb + (q*32 + lane)*V + e.
             const int64_t c0 = cb + (int64_t)lane * V;
-#pragma unroll
-            for (int f = 0; f < NR; ++f) {
+            // Only the registers the program reads before writing them are
+            // initialised (all of them for a register trace).
+            for (uint32_t m = livein; m != 0u; m &= m - 1u) {
+                const int f = __ffs(m) - 1;
                 float v[K];
                 if (f < w.num_inputs) {
 #pragma unroll
@@ -291,12 +295,16 @@ interp_wide_kernel(InterpArgs args) {
                 }
                 __syncwarp();
             }
-            if constexpr (MODE != kModeTrace) {
-                if (L > 0) WR::store(pt, a);   // the last result
-            }
-
+            // The output register: the last result when the last instruction
+            // wrote it (never stored), else the register file.
             float o[K];
-            WR::load(base + (uint32_t)args.output_reg * S, o);
+            const uint32_t out_addr = base + (uint32_t)args.output_reg * S;
+            if (MODE != kModeTrace && L > 0 && pt == out_addr) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) o[k] = a[k];
+            } else {
+                WR::load(out_addr, o);
+            }
             if constexpr (MODE == kModeOutputs) {
 #pragma unroll
                 for (int q = 0; q < K / V; ++q)

@@ -95,6 +95,7 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
                 bool strip, bool sched, uint32_t* raw_out, bool reset_totals = true, bool fitness_mode = false) {
     cudaStream_t s = ctx->stream;
     GALOP_CK(ctx->eff_len.ensure((size_t)std::max<int64_t>(n, 1)), "alloc eff_len");
+    GALOP_CK(ctx->livein.ensure((size_t)std::max<int64_t>(n, 1)), "alloc livein");
     GALOP_CK(ctx->eff_off.ensure((size_t)n + 1), "alloc eff_off");
     const int64_t n_tiles = (n + kScanTile - 1) / kScanTile;
     GALOP_CK(ctx->tiles.ensure((size_t)n_tiles + 1), "alloc scan tiles");
@@ -145,12 +146,13 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
     // output of galop_effective_csr keeps the intron pass's result as is),
     // and the forwarding flags every wide stream carries (fold.cuh).
     ctx->folded = fmt.wide && strip && raw_out == nullptr && n > 0;
-    if (fmt.wide && raw_out == nullptr && n > 0) {
+    ctx->flagged = fmt.wide && raw_out == nullptr && n > 0;
+    if (ctx->flagged) {
         FoldParams fp{ctx->isa.profile, ctx->isa.num_registers, ctx->isa.output_reg,
                       7u + (uint32_t)__builtin_ctz((unsigned)pick_k(ctx)), ctx->num_inputs, nullptr, nullptr,
                       ctx->folded ? 1 : 0};
         fold_kernel<<<blocks, tpb, 0, s>>>(reinterpret_cast<uint4*>(ctx->uops.p), ctx->eff_off.p, n, fp,
-                                           ctx->eff_len.p, ctx->counters.p + 3);
+                                           ctx->eff_len.p, ctx->livein.p, ctx->counters.p + 3);
         ctx->launches += 1;
     }
     // Identical interpreted programs: one representative each (dedup.cuh).
@@ -241,6 +243,7 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     a.uops = ctx->uops.p;
     a.eff_off = ctx->eff_off.p;
     a.interp_len = ctx->folded ? ctx->eff_len.p : nullptr;
+    a.livein = ctx->flagged ? ctx->livein.p : nullptr;
     a.n_skipped = ctx->deduped ? ctx->counters.p + 4 : nullptr;
     a.order = (sched && n > 1) ? ctx->order.p : nullptr;
     a.n_programs = n;
@@ -486,7 +489,7 @@ void galop_destroy(galop_ctx* ctx) {
     ctx->X.release(); ctx->y.release(); ctx->stage_aos.release(); ctx->stage_y.release();
     ctx->raw_words.release(); ctx->uops.release(); ctx->eff_raw.release(); ctx->raw_lens8.release();
     ctx->raw_off.release(); ctx->eff_off.release(); ctx->tiles.release();
-    ctx->eff_len.release(); ctx->order.release();
+    ctx->eff_len.release(); ctx->order.release(); ctx->livein.release();
     ctx->fitness.release(); ctx->outputs.release(); ctx->trace.release();
     ctx->sse.release(); ctx->partial.release(); ctx->counters.release(); ctx->hist.release();
     ctx->dkeys.release(); ctx->dkeys_sorted.release(); ctx->dvals.release(); ctx->dvals_sorted.release();
