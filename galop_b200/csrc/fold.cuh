@@ -139,20 +139,29 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
         const uint32_t s1 = w.x >> sh, s2 = w.y >> sh, d = w.z >> sh;
         const bool a_known = unary || ((known >> s1) & 1u);
         const bool b_known = is_const || ((known >> s2) & 1u);
-        if (a_known && b_known) {
-            const float a = unary ? 0.0f : vals[s1];
-            const float b = is_const ? __uint_as_float(w.y) : vals[s2];
-            const float v = fp.profile == kProfileBj ? apply_op<kProfileBj>(op, a, b)
+        const float a = a_known && !unary ? vals[s1] : 0.0f;
+        const float b = is_const ? __uint_as_float(w.y) : (b_known ? vals[s2] : 0.0f);
+        // Results known whatever the other operand: protected division by a
+        // zero (src/ISA.h:224: 1.0 for every dividend, NaN included), and
+        // LT/GT of the REF profile with a NaN operand (0.0: ordered
+        // comparisons with NaN are false).
+        const bool div0 = !unary && op == kDiv && b_known && b == 0.0f;
+        const bool cmp_nan = fp.profile == kProfileRef && (op == kOp6 || op == kOp7) &&
+                             ((a_known && isnan(a)) || (b_known && isnan(b)));
+        if ((a_known && b_known) || div0 || cmp_nan) {
+            const float v = div0 ? 1.0f
+                          : cmp_nan ? 0.0f
+                          : fp.profile == kProfileBj ? apply_op<kProfileBj>(op, a, b)
                                                      : apply_op<kProfileRef>(op, a, b);
             vals[d] = v;
             known |= 1u << d;
             u[j] = make_uint4(0u, __float_as_uint(v), w.z, kWideBcast);
         } else {
             if (!unary && b_known && !is_const) {
-                u[j] = make_uint4(w.x, __float_as_uint(vals[s2]), w.z, w.w | 8u);
+                u[j] = make_uint4(w.x, __float_as_uint(b), w.z, w.w | 8u);
             } else if (!unary && a_known && swaps(fp.profile, op)) {
                 const uint32_t sop = op == kOp6 ? (uint32_t)kOp7 : op == kOp7 ? (uint32_t)kOp6 : op;
-                u[j] = make_uint4(w.y, __float_as_uint(vals[s1]), w.z, (w.w & ~7u) | sop | 8u);
+                u[j] = make_uint4(w.y, __float_as_uint(a), w.z, (w.w & ~7u) | sop | 8u);
             }
             known &= ~(1u << d);
         }

@@ -236,6 +236,76 @@ def test_prepass_on_off_and_tile_shapes_bitwise(native):
                     assert np.array_equal(bits(fit), bits(base[1])), (pre, k, wpb, disp)
 
 
+def _chained_program(rng, nr: int, length: int, ops=tuple(range(8))) -> np.ndarray:
+    """Random instructions biased toward reading and rewriting the previous
+    destination: chains forwarded through src1, unary ops on the previous
+    result, both operands the previous result, SUB/DIV with src2 the
+    previous result, and results read again further down."""
+    prev = int(rng.integers(0, nr))
+    f = []
+    for _ in range(length):
+        op = int(rng.choice(ops))
+        dest = prev if rng.random() < 0.3 else int(rng.integers(0, nr))
+        s1 = prev if rng.random() < 0.5 else int(rng.integers(0, nr))
+        s2 = prev if rng.random() < 0.35 else int(rng.integers(0, nr))
+        f.append((op, dest, s1, s2, int(rng.random() < 0.25)))
+        prev = dest
+    return W.encode(*np.array(f, dtype=np.int64).T)
+
+
+def _nan_and_zero_program() -> np.ndarray:
+    """Constants folded into an infinity (doubling), a NaN (inf - inf) that
+    LT/GT then compare with, and divisions by a register still at 0 -- all
+    known before any case is read -- feeding the output with x0."""
+    ins = [(W.OP_ADD, 2, 0, 1, 1), (W.OP_ADD, 2, 2, 2, 0)]      # r2 = x0 + c1 (case-dependent)
+    ins += [(W.OP_ADD, 3, 7, 1, 1)]                             # r3 = 0 + c1
+    ins += [(W.OP_ADD, 3, 3, 3, 0)] * 140                       # r3 -> inf
+    ins += [(W.OP_SUB, 4, 3, 3, 0),                              # r4 = inf - inf = NaN
+            (W.OP_6, 5, 0, 4, 0), (W.OP_7, 6, 4, 0, 0),          # x0 < NaN, NaN > x0 -> 0
+            (W.OP_DIV, 1, 0, 7, 0),                              # x0 / 0 -> 1
+            (W.OP_DIV, 7, 2, 6, 0),                              # r2 / 0 -> 1
+            (W.OP_ADD, 0, 0, 5, 0), (W.OP_SUB, 0, 0, 6, 0), (W.OP_MUL, 0, 0, 1, 0),
+            (W.OP_ADD, 0, 0, 7, 0), (W.OP_MUL, 0, 0, 2, 0)]
+    return W.encode(*np.array(ins, dtype=np.int64).T)
+
+
+@pytest.mark.parametrize("nr", [8, 16])
+def test_forwarding_and_folding_patterns(native, orc, nr):
+    """The 16-byte micro-op loop (dispatch 3: constants folded into their
+    consumers, operands forwarded from the previous result, stores deferred
+    to where another reader needs them, only live-in registers initialised)
+    gives the per-case outputs and fitness of the 32-bit micro-op kernel
+    (dispatch 2, none of that) bit for bit, with the intron pass on and off,
+    on programs built to hit every forwarding pattern and window crossing;
+    IEEE-only programs also equal the oracle."""
+    rng = np.random.default_rng(21 + nr)
+    progs = [_nan_and_zero_program()] if nr == 8 else []
+    progs += [_chained_program(rng, nr, int(L)) for L in rng.integers(1, 110, 400)]
+    progs += [_chained_program(rng, nr, int(L), tuple(IEEE_REF)) for L in rng.integers(1, 110, 150)]
+    words = np.concatenate(progs).astype(np.uint32)
+    off = W.csr_offsets(np.array([len(p) for p in progs]))
+    X = rng.uniform(-3, 3, (1000, 1)).astype(np.float32)
+    y = rng.uniform(-2, 2, 1000).astype(np.float32)
+    ds = g.Dataset(X, y)
+    res = {}
+    for disp in (2, 3):
+        for pre in (True, False):
+            with g.Evaluator(num_registers=nr, intron_prepass=pre, reduce=g.REDUCE_ORDERED, dispatch=disp) as ev:
+                res[disp, pre] = (ev.case_outputs(words, off, ds), ev.evaluate_csr(words, off, ds))
+    base = res[2, True]
+    for key, (outs, fit) in res.items():
+        assert np.array_equal(bits(fit), bits(base[1])), key
+        assert same_or_nan(outs, base[0]).all(), key
+    o = orc.Oracle(orc.PROFILE_REF, nr)
+    want = o.evaluate_csr(words, off, X, y)
+    ieee = np.array([program_is_ieee(o, p, 0) for p in progs])
+    assert ieee.sum() >= 150
+    assert np.array_equal(bits(base[1])[ieee], bits(want)[ieee])
+    if nr == 8:
+        ref = o.case_outputs(progs[0], X)
+        assert same_or_nan(res[3, True][0][0], ref).all()
+
+
 # --- reductions ------------------------------------------------------------------------
 
 def test_reduction_modes_against_fp64_sum_of_gpu_outputs(native):
