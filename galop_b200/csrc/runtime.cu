@@ -685,10 +685,24 @@ static int evaluate_uploaded(galop_ctx* ctx, const Src& src, int64_t n, int64_t 
 // Host-pointer CSR evaluation in segments of programs: the words of segment
 // k+1 are copied on a second stream while segment k is pre-passed and
 // interpreted, so most of the host-to-device copy hides behind compute.
-// Every segment is chunked as the whole call would be, so the fitness is
-// the unsegmented call's bit for bit.
+// Segment k ends at program n * kSegEnd[k] / 32: the first segment is
+// small, so only its short copy is exposed, and each later one is copied
+// while the previous (at least as large) computes.  The offsets are
+// checked while the copies run (only the segment boundaries, which size
+// the copies, before).  Every segment is chunked as the whole call would
+// be, so the fitness is the unsegmented call's bit for bit.
+constexpr int kSegs = 5;
+constexpr int64_t kSegEnd[kSegs] = {1, 4, 8, 16, 32};
+
 static int evaluate_csr_segmented(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets, int64_t n,
-                                  int segs, float* fitness_out, double* sse_out) {
+                                  float* fitness_out, double* sse_out) {
+    const int segs = kSegs;
+    std::vector<int64_t> b(segs + 1);
+    b[0] = 0;
+    for (int k = 0; k < segs; ++k) b[k + 1] = n * kSegEnd[k] / 32;
+    bool bounds_ok = offsets[0] == 0;
+    for (int k = 0; k < segs; ++k) bounds_ok = bounds_ok && offsets[b[k + 1]] >= offsets[b[k]];
+    if (!bounds_ok) return validate_offsets(ctx, offsets, n);
     cudaStream_t s = ctx->stream;
     if (!ctx->copy_stream) {
         GALOP_CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
@@ -704,14 +718,16 @@ static int evaluate_csr_segmented(galop_ctx* ctx, const uint32_t* words, const i
     GALOP_CK(cudaStreamWaitEvent(cs, ctx->ev[kEvStart], 0), "stream wait");
     GALOP_CK(cudaMemcpyAsync(ctx->raw_off.p, offsets, (size_t)(n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, cs),
              "H2D offsets");
-    std::vector<int64_t> b(segs + 1);
-    for (int k = 0; k <= segs; ++k) b[k] = n * k / segs;
     for (int k = 0; k < segs; ++k) {
         const int64_t w0 = offsets[b[k]], w1 = offsets[b[k + 1]];
         if (w1 > w0)
             GALOP_CK(cudaMemcpyAsync(ctx->raw_words.p + w0, words + w0, (size_t)(w1 - w0) * sizeof(uint32_t),
                                      cudaMemcpyHostToDevice, cs), "H2D words");
         GALOP_CK(cudaEventRecord(ctx->seg_ev[5 * k], cs), "event");
+    }
+    if (int rc = validate_offsets(ctx, offsets, n)) {
+        cudaStreamSynchronize(cs);   // the copies read the caller's buffers
+        return rc;
     }
     GALOP_CK(ctx->counters.ensure(6), "alloc counters");
     GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 6 * sizeof(unsigned long long), s), "memset");
@@ -766,11 +782,10 @@ int galop_evaluate_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* off
     if (n_programs > 0 && !fitness_out) return ctx->fail(GALOP_E_INVALID, "null fitness_out");
     GALOP_CK(cudaSetDevice(ctx->device), "set device");
     begin_call(ctx, n_programs);
-    // Large populations: copy and compute overlapped in 4 segments.
+    // Large populations: copy and compute overlapped in segments.
     if (n_programs >= 65536 && offsets && offsets[n_programs] >= (int64_t)(32ll << 20)) {
         if (!words) return ctx->fail(GALOP_E_INVALID, "null words/offsets");
-        if (int rc = validate_offsets(ctx, offsets, n_programs)) return rc;
-        return evaluate_csr_segmented(ctx, words, offsets, n_programs, 4, fitness_out, sse_out);
+        return evaluate_csr_segmented(ctx, words, offsets, n_programs, fitness_out, sse_out);
     }
     GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], ctx->stream), "event");
     if (int rc = upload_csr(ctx, words, offsets, n_programs)) return rc;

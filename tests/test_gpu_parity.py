@@ -528,8 +528,19 @@ def test_large_host_call_in_segments_matches_device_call(native, reduce):
         finally:
             for p in (dw, do, df):
                 ev.device_free(p)
-    assert st.eff_instructions > 0 and st.kernels_launched > 20      # four segments' launches
+    assert st.eff_instructions > 0 and st.kernels_launched > 20      # one set of launches per segment
     assert np.array_equal(bits(host), bits(dev))
+    # Offsets are checked while the segments' copies run: a bad one away
+    # from the segment boundaries is still refused, and the evaluator stays
+    # usable.
+    bad = off.copy()
+    bad[3] = bad[2] - 1
+    with g.Evaluator(num_registers=16, reduce=reduce) as ev:
+        ev.set_dataset(g.Dataset(X, y))
+        with pytest.raises(g.GalopError) as e:
+            ev.evaluate_csr(words, bad)
+        assert e.value.status == g.E_INVALID
+        assert np.array_equal(bits(ev.evaluate_csr(words, off)), bits(host))
 
 
 @pytest.mark.parametrize("reduce", [g.REDUCE_KAHAN32, g.REDUCE_ORDERED])
