@@ -31,7 +31,7 @@ static __global__ void dedup_hash_kernel(const uint4* __restrict__ uops, const i
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int32_t L = len[i];
-    const uint4* p = uops + eff_off[i];
+    const uint4* p = uops + eff_off[i + 1] - L;   // packed against the slot's end (fold.cuh)
     unsigned long long h = 0xcbf29ce484222325ull;
     auto mix = [&](uint32_t w) {
         h ^= w;
@@ -78,8 +78,8 @@ static __global__ void dedup_rep_kernel(const int32_t* __restrict__ head_pos, co
             const int32_t head = vals[h], i = vals[j];
             L = len[head];
             if (len[i] == L && (!group || group[i] == group[head])) {
-                const uint4* hp = uops + eff_off[head];
-                const uint4* ip = uops + eff_off[i];
+                const uint4* hp = uops + eff_off[head + 1] - L;
+                const uint4* ip = uops + eff_off[i + 1] - L;
                 copy = true;
                 for (int32_t k = 0; k < L && copy; ++k) {
                     const uint4 a = hp[k], b = ip[k];

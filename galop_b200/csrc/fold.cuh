@@ -10,9 +10,11 @@
 // __fadd_rn, IEEE division, sinf, ... on this device), hence the same bits --
 // and becomes a broadcast micro-op (dest = that constant).  A second,
 // backward liveness pass then drops instructions whose results no remaining
-// instruction reads (broadcasts read nothing), and the survivors are packed
-// to the front of the program's slot.  Per-case outputs and fitness are
-// unchanged; only case-independent work is done once instead of per case.
+// instruction reads (broadcasts read nothing) and packs the survivors
+// against the end of the program's slot: the interpreted micro-ops of
+// program i are u[eff_off[i + 1] - interp_len[i], eff_off[i + 1]).
+// Per-case outputs and fitness are unchanged; only case-independent work is
+// done once instead of per case.
 //
 // Two rewrites make the survivors cheaper without changing any result:
 //   - a known value read by an instruction that is not folded becomes that
@@ -21,11 +23,11 @@
 //     op is ADD or MUL (IEEE sum and product are commutative) or LT/GT of
 //     the REF profile (a < b is b > a, both false on NaN), by swapping the
 //     operands; the broadcast that wrote the register then usually dies;
-//   - on the final order, each operand that is the previous instruction's
-//     destination is marked as forwarded (kWideFwd1 / kWideFwd2), and a
-//     result is marked to reach the register file (kWideStorePrev on the
-//     next instruction) only when something other than the next
-//     instruction's forwarded operand reads it.
+//   - on the final order (in the same backward pass), each operand that is
+//     the previous instruction's destination is marked as forwarded
+//     (kWideFwd1 / kWideFwd2), and a result is marked to reach the register
+//     file (kWideStorePrev on the next instruction) only when something
+//     other than the next instruction's forwarded operand reads it.
 // With folding off (intron pass off) the kernel only marks forwarding:
 // every stream the interpreter loop runs carries the flags.
 #pragma once
@@ -54,6 +56,50 @@ __device__ __forceinline__ bool swaps(int profile, uint32_t op) {
     return op == kAdd || op == kMul || (profile == kProfileRef && (op == kOp6 || op == kOp7));
 }
 
+// Registers a micro-op reads (broadcasts none, unary ops only src2, a
+// constant src2 none).
+__device__ __forceinline__ uint32_t uop_reads(const uint4& w, uint32_t sh) {
+    if ((w.w & ~kWideFlags) == kWideBcast) return 0u;
+    uint32_t r = 0u;
+    if (!(w.w & kWideSpecial)) r |= 1u << (w.x >> sh);
+    if (!(w.w & 8u)) r |= 1u << (w.y >> sh);
+    return r;
+}
+
+// fwd1 / fwd2 on micro-op w whose predecessor wrote the register at byte
+// offset prev, swapping the operands of a binary op first when only src2
+// is that register and the swap keeps the result bits.
+__device__ __forceinline__ void set_fwd(uint4& w, uint32_t prev, int profile) {
+    if (w.w == kWideBcast) return;
+    const bool reg2 = !(w.w & 8u);
+    if (w.w & kWideSpecial) {
+        if (reg2 && w.y == prev) w.w |= kWideFwd2;
+        return;
+    }
+    const uint32_t op = w.w & 7u;
+    if (w.x != prev && reg2 && w.y == prev && swaps(profile, op)) {
+        const uint32_t sop = op == kOp6 ? (uint32_t)kOp7 : op == kOp7 ? (uint32_t)kOp6 : op;
+        const uint32_t x = w.x;
+        w.x = w.y;
+        w.y = x;
+        w.w = (w.w & ~7u) | sop;
+    }
+    if (w.x == prev) w.w |= kWideFwd1;
+}
+
+// Whether the result of the instruction before nx (register d) must reach
+// the register file: unless nx takes it forwarded, loads no copy of it, and
+// nothing after nx reads it (live_after_next: registers live after nx).
+__device__ __forceinline__ bool needs_store(const uint4& nx, uint32_t d, uint32_t live_after_next, uint32_t sh) {
+    const uint32_t nd = nx.z >> sh;
+    const bool fwd = (nx.w & (kWideFwd1 | kWideFwd2)) != 0;
+    // a binary op loads src2 (never forwarded); src1 equal to d is forwarded
+    const bool loads_d = !(nx.w & kWideSpecial) && !(nx.w & 8u) && (nx.y >> sh) == d &&
+                         (nx.w & ~kWideFlags) != kWideBcast;
+    const bool read_later = d != nd && ((live_after_next >> d) & 1u);
+    return !(fwd && !loads_d && !read_later);
+}
+
 // Forwarding flags over a program u[0, n) in its final order (see the
 // micro-op format in isa.cuh).  The interpreter loop keeps the last result
 // in registers; an instruction takes it as src1 (binary ops, fwd1) or src2
@@ -73,47 +119,15 @@ __device__ __forceinline__ bool swaps(int profile, uint32_t op) {
 // ones the interpreter must initialise before each pass over the cases.
 __device__ __forceinline__ uint32_t mark_forwarding(uint4* __restrict__ u, int64_t n, uint32_t sh, int output_reg,
                                                     int profile) {
-    for (int64_t j = 1; j < n; ++j) {
-        uint4 w = u[j];
-        if (w.w == kWideBcast) continue;
-        const uint32_t prev = u[j - 1].z;
-        const bool reg2 = !(w.w & 8u);
-        if (w.w & kWideSpecial) {
-            if (reg2 && w.y == prev) w.w |= kWideFwd2;
-        } else {
-            const uint32_t op = w.w & 7u;
-            if (w.x != prev && reg2 && w.y == prev && swaps(profile, op)) {
-                const uint32_t sop = op == kOp6 ? (uint32_t)kOp7 : op == kOp7 ? (uint32_t)kOp6 : op;
-                const uint32_t x = w.x;
-                w.x = w.y;
-                w.y = x;
-                w.w = (w.w & ~7u) | sop;
-            }
-            if (w.x == prev) w.w |= kWideFwd1;
-        }
-        u[j] = w;
-    }
+    for (int64_t j = 1; j < n; ++j) set_fwd(u[j], u[j - 1].z, profile);
     uint32_t live = 1u << output_reg;      // live after instruction j
     uint32_t live_after_next = 0u;
     for (int64_t j = n - 1; j >= 0; --j) {
         const uint4 w = u[j];
         const uint32_t d = w.z >> sh;
-        const bool bcast = (w.w & ~kWideFlags) == kWideBcast;
-        if (j < n - 1) {
-            const uint4 nx = u[j + 1];
-            const uint32_t nd = nx.z >> sh;
-            const bool fwd = (nx.w & (kWideFwd1 | kWideFwd2)) != 0;
-            const bool loads_d = !(nx.w & kWideSpecial) && !(nx.w & 8u) && (nx.y >> sh) == d &&
-                                 (nx.w & ~kWideFlags) != kWideBcast;
-            const bool read_later = d != nd && ((live_after_next >> d) & 1u);
-            if (!(fwd && !loads_d && !read_later)) u[j + 1].w = nx.w | kWideStorePrev;
-        }
+        if (j < n - 1 && needs_store(u[j + 1], d, live_after_next, sh)) u[j + 1].w |= kWideStorePrev;
         live_after_next = live;
-        live &= ~(1u << d);
-        if (!bcast) {
-            if (!(w.w & kWideSpecial)) live |= 1u << (w.x >> sh);
-            if (!(w.w & 8u)) live |= 1u << (w.y >> sh);
-        }
+        live = (live & ~(1u << d)) | uop_reads(w, sh);
     }
     return live;
 }
@@ -166,26 +180,31 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
             known &= ~(1u << d);
         }
     }
-    // backward: drop what nothing reads
-    uint32_t live = 1u << fp.output_reg;
+    // backward: drop what nothing reads, pack the survivors against the end
+    // of the slot, and set each survivor's forwarding flags once its
+    // predecessor (the next survivor met) is known
+    uint32_t live = 1u << fp.output_reg;   // live after instruction j
+    int64_t pos = L;                       // survivors occupy u[pos, L)
+    bool pending = false;
+    uint4 nx = make_uint4(0u, 0u, 0u, 0u); // the survivor after j, not yet written
+    uint32_t live_after_nx = 0u;
     for (int64_t j = L - 1; j >= 0; --j) {
         const uint4 w = u[j];
         const uint32_t d = w.z >> sh;
-        if (!((live >> d) & 1u)) {
-            u[j].w = kWideDead;
-            continue;
+        if (!((live >> d) & 1u)) continue;
+        if (pending) {
+            set_fwd(nx, w.z, fp.profile);
+            if (needs_store(nx, d, live_after_nx, sh)) nx.w |= kWideStorePrev;
+            u[--pos] = nx;              // pos > j: never a micro-op still to be read
         }
-        live &= ~(1u << d);
-        if (w.w != kWideBcast) {
-            if (!(w.w & kWideSpecial)) live |= 1u << (w.x >> sh);
-            if (!(w.w & 8u)) live |= 1u << (w.y >> sh);
-        }
+        nx = w;
+        pending = true;
+        live_after_nx = live;
+        live = (live & ~(1u << d)) | uop_reads(w, sh);
     }
-    for (int64_t j = 0; j < L; ++j) {
-        const uint4 w = u[j];
-        if (w.w != kWideDead) u[kept++] = w;
-    }
-    livein = mark_forwarding(u, kept, sh, fp.output_reg, fp.profile);
+    if (pending) u[--pos] = nx;         // the first survivor: no flags
+    livein = live;
+    kept = L - pos;
     return kept;
 }
 

@@ -51,7 +51,8 @@ struct PopDesc {
 struct InterpArgs {
     const uint32_t* uops;          // micro-ops, CSR by eff_off
     const int64_t* eff_off;        // [n_programs + 1]
-    const int32_t* interp_len;     // interpreted length per program after folding, or null
+    const int32_t* interp_len;     // interpreted length per program after folding (the last interp_len
+                                   // micro-ops of the program's slot), or null
     const uint32_t* livein;        // per program: registers read before written (wide kernel), or null: all
     const unsigned long long* n_skipped;  // copies left out of the order (dedup), or null
     const int32_t* order;          // slot -> program (longest first), or null

@@ -201,8 +201,10 @@ interp_wide_kernel(InterpArgs args) {
         item = __shfl_sync(0xffffffffu, item, 0);
         if ((int64_t)item >= total_items) break;
         const WideItem w = resolve_item(args, item);
-        const int64_t p0 = args.eff_off[w.prog];
-        const int64_t L = args.interp_len ? (int64_t)args.interp_len[w.prog] : args.eff_off[w.prog + 1] - p0;
+        // folded programs are packed against the end of their slot (fold.cuh)
+        const int64_t L = args.interp_len ? (int64_t)args.interp_len[w.prog]
+                                          : args.eff_off[w.prog + 1] - args.eff_off[w.prog];
+        const int64_t p0 = args.eff_off[w.prog + 1] - L;
         const uint4* __restrict__ pw = uops4 + p0;
         const uint32_t livein = (MODE == kModeTrace || args.livein == nullptr) ? (1u << NR) - 1u
                                                                               : args.livein[w.prog];
