@@ -144,9 +144,9 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
         vals[r] = 0.0f;
         if (r >= k_in) known |= 1u << r;
     }
-    // forward: evaluate what is known
-    for (int64_t j = 0; j < L; ++j) {
-        const uint4 w = u[j];
+    // forward: evaluate what is known (micro-ops read four at a time, so
+    // that several loads are in flight; each step writes only u[j])
+    auto forward = [&](const uint4 w, const int64_t j) {
         const uint32_t op = w.w & 7u;
         const bool is_const = (w.w & 8u) != 0;
         const bool unary = (w.w & kWideSpecial) != 0;
@@ -179,6 +179,14 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
             }
             known &= ~(1u << d);
         }
+    };
+    for (int64_t j0 = 0; j0 < L; j0 += 4) {
+        uint4 g[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) g[q] = j0 + q < L ? u[j0 + q] : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (j0 + q < L) forward(g[q], j0 + q);
     }
     // backward: drop what nothing reads, pack the survivors against the end
     // of the slot, and set each survivor's forwarding flags once its
@@ -188,19 +196,26 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
     bool pending = false;
     uint4 nx = make_uint4(0u, 0u, 0u, 0u); // the survivor after j, not yet written
     uint32_t live_after_nx = 0u;
-    for (int64_t j = L - 1; j >= 0; --j) {
-        const uint4 w = u[j];
+    auto backward = [&](const uint4 w) {
         const uint32_t d = w.z >> sh;
-        if (!((live >> d) & 1u)) continue;
+        if (!((live >> d) & 1u)) return;
         if (pending) {
             set_fwd(nx, w.z, fp.profile);
             if (needs_store(nx, d, live_after_nx, sh)) nx.w |= kWideStorePrev;
-            u[--pos] = nx;              // pos > j: never a micro-op still to be read
+            u[--pos] = nx;              // past the micro-op in hand: never one still to be read
         }
         nx = w;
         pending = true;
         live_after_nx = live;
         live = (live & ~(1u << d)) | uop_reads(w, sh);
+    };
+    for (int64_t j0 = L - 1; j0 >= 0; j0 -= 4) {
+        uint4 g[4];                     // u[j0 - 3 .. j0], read before any of them is processed
+#pragma unroll
+        for (int q = 0; q < 4; ++q) g[q] = j0 - q >= 0 ? u[j0 - q] : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (j0 - q >= 0) backward(g[q]);
     }
     if (pending) u[--pos] = nx;         // the first survivor: no flags
     livein = live;

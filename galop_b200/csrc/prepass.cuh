@@ -58,6 +58,7 @@ __global__ void prepass_count_kernel(Src src, int64_t n, IsaParams isa, int stri
             cnt = raw;
         } else {
             uint32_t live = 1u << isa.output_reg;
+#pragma unroll 4
             for (int64_t pc = raw - 1; pc >= 0; --pc) {
                 const Decoded d = decode_raw(isa, __ldg(src.words + s + pc));
                 if (!((live >> d.dest) & 1u)) continue;
@@ -206,6 +207,7 @@ __global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int st
     }
     int64_t pos = eff_off[i + 1];   // fill backwards
     uint32_t live = 1u << isa.output_reg;
+#pragma unroll 4
     for (int64_t pc = raw - 1; pc >= 0; --pc) {
         const uint32_t w = __ldg(src.words + s + pc);
         const Decoded d = decode_raw(isa, w);
