@@ -285,6 +285,10 @@ def test_forwarding_and_folding_patterns(native, orc, nr):
     words = np.concatenate(progs).astype(np.uint32)
     off = W.csr_offsets(np.array([len(p) for p in progs]))
     X = rng.uniform(-3, 3, (1000, 1)).astype(np.float32)
+    # special inputs in a few cases: zeros of both signs, infinities, NaN,
+    # denormals, huge values (DIV's zero paths, NaN comparisons, overflow)
+    special = np.array([0.0, -0.0, np.inf, -np.inf, np.nan, 1e-40, -1e-40, 3e38, -3e38, 1.0], np.float32)
+    X[-len(special):, 0] = special
     y = rng.uniform(-2, 2, 1000).astype(np.float32)
     ds = g.Dataset(X, y)
     res = {}
