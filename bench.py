@@ -183,6 +183,17 @@ def profile_summary() -> dict:
     return {}
 
 
+def hbm_view(traffic, kernel_ms: float, peaks: dict):
+    """DRAM bytes per launch over the launch time, against the measured
+    copy bandwidth (or the fallback figure when no measurement exists)."""
+    if not traffic or kernel_ms <= 0:
+        return None
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = traffic / (kernel_ms / 1e3) / 1e9
+    return {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": "hbm_gbs of MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback"}
+
+
 def profile_traffic():
     return profile_summary().get("dram_bytes_per_launch_full")
 
@@ -391,7 +402,10 @@ def run_b200(args, dist: Dist):
                          # instructions the interpreter actually runs per case: the effective ones
                          # minus those evaluated once per program (every operand case-independent)
                          "interpreted_ops_per_launch": float(interp_instr) * wl.n_cases,
-                         "interpreted_achieved": interp_instr * wl.n_cases / (interp_avg_ms / 1e3) / 1e9},
+                         "interpreted_achieved": interp_instr * wl.n_cases / (interp_avg_ms / 1e3) / 1e9,
+                         # the same kernel read against HBM (it streams each program once)
+                         "hbm_view": hbm_view(profile_traffic(), interp_avg_ms, peaks),
+                         "issue_slots_active": profile_summary().get("issue_slots_active")},
             "clocks": clock,
             "latency_ms": {"p50": float(np.percentile(interp_ms, 50)), "p99": float(np.percentile(interp_ms, 99))},
         }
