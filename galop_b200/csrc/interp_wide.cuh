@@ -20,8 +20,11 @@
 // The result registers a[K] and the address of the register they belong to
 // live across the whole pass: the unary ops (SIN/COS, and EXP/LOG of the BJ
 // profile), which run in C++ on the slow branch with the CUDA math library,
-// read and write them too, and the last result is stored after the last
-// instruction.  The folding pass sets the flags (isa.cuh, fold.cuh).
+// read and write them too.  The last result is never stored: the output
+// is taken from it when the last instruction wrote the output register.
+// Each pass initialises only the registers the program reads before
+// writing them (args.livein).  The folding pass sets the flags and the
+// masks (isa.cuh, fold.cuh).
 //
 // Semantics are those of interp.cuh (src/Interpreter.cpp:36-59,
 // src/ISA.h:219-231, src/Evaluator.cpp:11-45 and :88-91).
