@@ -183,6 +183,21 @@ def profile_summary() -> dict:
     return {}
 
 
+def fp32_issue_peak(device: int, peaks: dict):
+    """SMs x 128 FP32 lanes x the measured maximum SM clock, in G lane-ops/s."""
+    sm_count = 148
+    try:
+        import ctypes
+        cudart = ctypes.CDLL("libcudart.so")
+        v = ctypes.c_int()
+        if cudart.cudaDeviceGetAttribute(ctypes.byref(v), 16, device) == 0:
+            sm_count = v.value
+    except OSError:
+        pass
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    return sm_count * 128 * sm_max * 1e6 / 1e9, sm_count, sm_max
+
+
 def hbm_view(traffic, kernel_ms: float, peaks: dict):
     """DRAM bytes per launch over the launch time, against the measured
     copy bandwidth (or the fallback figure when no measurement exists)."""
@@ -335,17 +350,7 @@ def run_b200(args, dist: Dist):
 
     # ---- roofline of the interpreter (FP32 issue) -------------------------------
     peaks = measured_peaks()
-    sm_count = 148
-    try:
-        import ctypes
-        cudart = ctypes.CDLL("libcudart.so")
-        v = ctypes.c_int()
-        if cudart.cudaDeviceGetAttribute(ctypes.byref(v), 16, dist.local if dist.world > 1 else 0) == 0:
-            sm_count = v.value
-    except OSError:
-        pass
-    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
-    peak_gops = sm_count * 128 * sm_max * 1e6 / 1e9
+    peak_gops, sm_count, sm_max = fp32_issue_peak(dist.local if dist.world > 1 else 0, peaks)
     interp_avg_ms = float(np.mean(interp_ms))
     achieved = eff_instr * wl.n_cases / (interp_avg_ms / 1e3) / 1e9
 
@@ -506,6 +511,12 @@ def run_batch(args):
         "kernels_per_generation": st.kernels_launched,
         "autotune": {k: v for k, v in tune.as_dict().items() if k != "key"},
     }
+    peak_gops, sm_count, sm_max = fp32_issue_peak(0, measured_peaks())
+    line["roofline"] = {"bound": "fp32_issue", "achieved": batched, "peak": peak_gops, "unit": UNIT,
+                        "frac": batched / peak_gops, "traffic": None,
+                        "scope": "whole generation (pre-pass, interpreter, finalize), device time",
+                        "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {sm_max:.0f} MHz "
+                                       f"(sm_max_mhz of MEASURED_PEAKS.json)"}
     rd.close()
     ev.close()
     print(json.dumps(line), flush=True)
