@@ -718,12 +718,15 @@ def run_capacity(args):
         fit = torch.empty(P, dtype=torch.float32, device=dev)
         return w, off, fit
 
-    for dispatch in (3, 2):
+    # dispatch 3 with dedup (the default), without it (its per-program sort
+    # buffers are the price of interpreting identical programs once), and the
+    # 4-byte micro-op interpreter
+    for dispatch, dedup in ((3, True), (3, False), (2, False)):
         # footprint per program from a 2^22-program population
         P0 = 1 << 22
         torch.cuda.synchronize()
         before = torch.cuda.mem_get_info(dev)[0]
-        ev = g.Evaluator(num_registers=8, dispatch=dispatch)
+        ev = g.Evaluator(num_registers=8, dispatch=dispatch, dedup=dedup)
         ev.set_dataset(ds)
         w, off, fit = population(P0)
         ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P0, fit.data_ptr())
@@ -735,10 +738,10 @@ def run_capacity(args):
         torch.cuda.empty_cache()
         free_now = torch.cuda.mem_get_info(dev)[0]
         P = int(min(2**31 - 1, 0.92 * free_now / per_prog))
-        row = {"dispatch": dispatch, "bytes_per_program": round(per_prog, 1), "max_programs": P}
+        row = {"dispatch": dispatch, "dedup": dedup, "bytes_per_program": round(per_prog, 1), "max_programs": P}
         for attempt in range(3):
             try:
-                ev = g.Evaluator(num_registers=8, dispatch=dispatch)
+                ev = g.Evaluator(num_registers=8, dispatch=dispatch, dedup=dedup)
                 ev.set_dataset(ds)
                 w, off, fit = population(P)
                 ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, fit.data_ptr())   # the proof
