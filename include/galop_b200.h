@@ -124,10 +124,12 @@ typedef struct {
     int32_t case_chunks;           /* work items per program                    */
     int32_t kernels_launched;      /* this library's kernel launches            */
     int32_t reserved0;
-    int64_t interp_instructions;   /* instructions interpreted per case: the
-                                      effective ones minus those evaluated
-                                      once because every operand is known
-                                      (dispatch 3 with the intron pass)      */
+    int64_t interp_instructions;   /* instructions interpreted per case
+                                      (dispatch 3 with the intron pass): the
+                                      effective ones minus those whose result
+                                      is known before any case is read (done
+                                      once per program) and minus the copies
+                                      of programs interpreted once (dedup)  */
 } galop_stats;
 
 /* ---- lifetime ------------------------------------------------------------ */
