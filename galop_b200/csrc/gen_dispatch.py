@@ -260,7 +260,9 @@ def wide_loop(k: int, profile: int) -> str:
     vs = "" if v == 1 else f".v{v}"
     A = lambda q: f"%{1 + q}"
     PT = f"%{k + 1}"
-    base = f"%{k + 2}"
+    LV = [f"%{k + 2 + i}" for i in range(4)]      # out: the micro-op that leaves
+    base = f"%{k + 6}"
+    CUR = [f"%{k + 7 + i}" for i in range(4)]     # in: the micro-op at %0
 
     def ld(names, addr: str) -> list[str]:
         return [f"ld.shared{vs}.f32 {_vec([names(q * v + e) for e in range(v)])}, [{addr}+{q * 128 * v}];"
@@ -273,11 +275,11 @@ def wide_loop(k: int, profile: int) -> str:
     bregs = lambda q: f"b{q}"
     L = [f".reg .f32 b<{k}>, c;", WIDE_TEMPS, ".reg .pred q;",
          ".reg .u32 ux, uy, uz, uw, vx, vy, vz, vw, pa, pb;",
-         "ld.shared.v4.u32 {ux, uy, uz, uw}, [%0];"]
+         f"mov.b32 ux, {CUR[0]}; mov.b32 uy, {CUR[1]}; mov.b32 uz, {CUR[2]}; mov.b32 uw, {CUR[3]};"]
     entry = {(1, 0): "S", (0, 0): "L", (0, 1): "F", (1, 1): "G"}
     for cur, nxt, here, there in (("u", "v", "A", "B"), ("v", "u", "B", "A")):
         x, y, z, w = (f"{cur}{f}" for f in "xyzw")
-        L += [f"L{here}%=: setp.lt.s32 q, {w}, 0;", "@q bra.uni D%=;",
+        L += [f"L{here}%=: setp.lt.s32 q, {w}, 0;", f"@q bra.uni D{here}%=;",
               f"ld.shared.v4.u32 {{{nxt}x, {nxt}y, {nxt}z, {nxt}w}}, [%0+16];",
               "add.u32 %0, %0, 16;", f"mov.b32 c, {y};"]
         nxt_jump = [f"add.u32 {PT}, {base}, {z};", f"bra.uni L{there}%=;"]
@@ -289,7 +291,7 @@ def wide_loop(k: int, profile: int) -> str:
             elif op in ops:
                 targets.append(f"{entry[(sp, f1)]}{here}{op}{cst}_%=")
             else:
-                targets.append("D%=")
+                targets.append(f"D{here}%=")
         L += [f"T{here}%=: .branchtargets " + ", ".join(targets) + ";", f"brx.idx.uni {w}, T{here}%=;"]
         for op in ops:
             for cst in (0, 1):
@@ -302,13 +304,18 @@ def wide_loop(k: int, profile: int) -> str:
                 L.append(f"G{nm}: " + " ".join(st(PT) + [f"bra.uni F{nm};"]))
         L.append(f"S{here}B_%=: " + " ".join(st(PT)))
         L.append(f"L{here}B_%=: " + " ".join([f"mov.f32 {A(q)}, c;" for q in range(k)] + nxt_jump))
+    for here, cur in (("A", "u"), ("B", "v")):
+        L.append(f"D{here}%=: " + " ".join(f"mov.b32 {LV[i]}, {cur}{f};" for i, f in enumerate("xyzw"))
+                 + (" bra.uni D%=;" if here == "A" else ""))
     L.append("D%=:")
     text = "\\n\\t".join(L)
-    outs = ", ".join(['"+r"(sp)'] + [f'"+f"(a[{q}])' for q in range(k)] + ['"+r"(pt)'])
+    outs = ", ".join(['"+r"(sp)'] + [f'"+f"(a[{q}])' for q in range(k)] + ['"+r"(pt)']
+                     + [f'"=r"(lv.{f})' for f in "xyzw"])
+    ins = ", ".join(['"r"(base)'] + [f'"r"(cur.{f})' for f in "xyzw"])
     return (f"    static __device__ __forceinline__ void run(uint32_t& sp, float (&a)[{k}], uint32_t& pt, "
-            f"uint32_t base) {{\n"
+            f"uint32_t base, uint4 cur, uint4& lv) {{\n"
             f'    asm volatile("{{\\n\\t{text}\\n\\t}}"\n'
-            f'        : {outs}\n        : "r"(base)\n        : "memory");\n    }}\n')
+            f'        : {outs}\n        : {ins}\n        : "memory");\n    }}\n')
 
 
 def main() -> None:

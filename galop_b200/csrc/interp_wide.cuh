@@ -176,6 +176,23 @@ __device__ __forceinline__ void wide_trace(float* __restrict__ trace, int64_t ro
     }
 }
 
+// The unary ops of the profile on K cases: SIN/COS (REF), SIN/COS/EXP/LOG
+// (BJ), with the CUDA math library as everywhere else.
+template <int K, int PROFILE>
+__device__ __forceinline__ void unary_op(uint32_t op, const float (&b)[K], float (&t)[K]) {
+    if constexpr (PROFILE == kProfileRef) {
+        if (op == kSin) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = sinf(b[k]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] = cosf(b[k]);
+        }
+    } else {
+        slow_op<K, PROFILE>(op, b, b, t);
+    }
+}
+
 template <int NR, int K, int PROFILE, int REDUCE, int MODE>
 __global__ void __launch_bounds__(256, 3)
 interp_wide_kernel(InterpArgs args) {
@@ -250,27 +267,19 @@ interp_wide_kernel(InterpArgs args) {
                 sts_u4(stage + (uint32_t)lane * 16u, mine);
                 __syncwarp();
                 uint32_t sp = stage;
-                for (;;) {
-                    uint4 u;
-                    if constexpr (MODE == kModeTrace) {
-                        // One instruction at a time, the register file dumped after each.
-                        u = lds_u4(sp);
+                if constexpr (MODE == kModeTrace) {
+                    // One instruction at a time, the register file dumped after
+                    // each; every result is stored, the flags do not apply.
+                    for (;;) {
+                        uint4 u = lds_u4(sp);
                         while ((int32_t)u.w >= 0) {
-                            // every result is stored here: the flags do not apply
                             WideOps<K, PROFILE>::run(u.w & 15u, base + u.x, base + u.y, base + u.z, u.y);
                             wide_trace<NR, K>(args.trace, wb + (sp - stage) / 16u + 1, base, lane);
                             sp += 16u;
                             u = lds_u4(sp);
                         }
-                    } else {
-                        // Every binary instruction up to the next unary op or the end marker.
-                        WideLoop<K, PROFILE>::run(sp, a, pt, base);
-                        u = lds_u4(sp);
-                    }
-                    if (u.w == kWideEnd) break;
-                    // Unary op on src2 (register, constant or the previous result).
-                    float b[K];
-                    if constexpr (MODE == kModeTrace) {
+                        if (u.w == kWideEnd) break;
+                        float b[K];
                         if (u.w & 8u) {
                             const float c = __uint_as_float(u.y);
 #pragma unroll
@@ -281,8 +290,20 @@ interp_wide_kernel(InterpArgs args) {
                         slow_op<K, PROFILE>(u.w & 7u, b, b, a);
                         WR::store(base + u.z, a);
                         wide_trace<NR, K>(args.trace, wb + (sp - stage) / 16u + 1, base, lane);
-                    } else {
+                        sp += 16u;
+                    }
+                } else {
+                    uint4 cur = lds_u4(sp);
+                    for (;;) {
+                        // Every binary instruction up to the next unary op or the
+                        // end marker; u is the micro-op that stopped the loop.
+                        uint4 u;
+                        WideLoop<K, PROFILE>::run(sp, a, pt, base, cur, u);
+                        if (u.w == kWideEnd) break;
+                        const uint4 next = lds_u4(sp + 16u);   // the end marker at most
+                        // Unary op on src2 (register, constant or the previous result).
                         if (u.w & kWideStorePrev) WR::store(pt, a);
+                        float b[K];
                         if (u.w & 8u) {
                             const float c = __uint_as_float(u.y);
 #pragma unroll
@@ -293,10 +314,11 @@ interp_wide_kernel(InterpArgs args) {
                         } else {
                             WR::load(base + u.y, b);
                         }
-                        slow_op<K, PROFILE>(u.w & 7u, b, b, a);
+                        unary_op<K, PROFILE>(u.w & 7u, b, a);
                         pt = base + u.z;
+                        sp += 16u;
+                        cur = next;
                     }
-                    sp += 16u;
                 }
                 __syncwarp();
             }
