@@ -291,7 +291,7 @@ def wide_loop(k: int, profile: int) -> str:
             elif op in ops:
                 targets.append(f"{entry[(sp, f1)]}{here}{op}{cst}_%=")
             else:
-                targets.append(f"D{here}%=")
+                targets.append(f"X{here}%=")
         L += [f"T{here}%=: .branchtargets " + ", ".join(targets) + ";", f"brx.idx.uni {w}, T{here}%=;"]
         for op in ops:
             for cst in (0, 1):
@@ -304,6 +304,11 @@ def wide_loop(k: int, profile: int) -> str:
                 L.append(f"G{nm}: " + " ".join(st(PT) + [f"bra.uni F{nm};"]))
         L.append(f"S{here}B_%=: " + " ".join(st(PT)))
         L.append(f"L{here}B_%=: " + " ".join([f"mov.f32 {A(q)}, c;" for q in range(k)] + nxt_jump))
+    # Table entries no micro-op uses (the pre-pass never writes them) leave
+    # too, after the dispatch has already stepped to the next micro-op: X
+    # steps back so that the caller gets this micro-op and %0 at it.
+    for here in ("A", "B"):
+        L.append(f"X{here}%=: sub.u32 %0, %0, 16; bra.uni D{here}%=;")
     for here, cur in (("A", "u"), ("B", "v")):
         L.append(f"D{here}%=: " + " ".join(f"mov.b32 {LV[i]}, {cur}{f};" for i, f in enumerate("xyzw"))
                  + (" bra.uni D%=;" if here == "A" else ""))
