@@ -52,6 +52,28 @@ def test_batch_matches_single_population_calls(native, reduce, dispatch):
             assert rel.size == 0 or rel.max() <= 1e-6, p
 
 
+def test_batch_with_intron_pass_off_matches_on(native):
+    """With the intron pass off the batch interprets every raw instruction
+    (the pre-pass then only marks forwarding and live-in registers); the
+    fitness must equal the default batch's bit for bit (ORDERED)."""
+    pops = _populations(3, SPECS)
+    got = {}
+    for pre in (True, False):
+        with g.Evaluator(num_registers=16, reduce=g.REDUCE_ORDERED, intron_prepass=pre) as ev:
+            rds = [g.ResidentDataset(ev, ds) for ds, _, _ in pops]
+            with g.Batch(ev, [(r, max(o.shape[0] - 1, 1), max(int(o[-1]), 1)) for r, (_, _, o) in zip(rds, pops)]) as b:
+                for p, (_, w, o) in enumerate(pops):
+                    b.set_population(p, w, o)
+                b.evaluate()
+                b.synchronize()
+                got[pre] = [b.fitness(p) for p in range(len(pops))]
+                st = b.stats
+        if not pre:
+            assert st.eff_instructions == st.raw_instructions
+    for p, (a, c) in enumerate(zip(got[True], got[False])):
+        assert np.array_equal(bits(a), bits(c)), p
+
+
 @pytest.mark.parametrize("dispatch", [2, 3])
 def test_population_fitness_is_identical_alone_and_in_a_mix(native, dispatch):
     """Case chunking depends on a population's own case count only, so its
