@@ -297,7 +297,7 @@ def run_b200(args, dist: Dist):
     ev.h2d(d_off, offsets)
 
     def step_device():
-        ev.evaluate_csr_device(d_words, d_off, n, d_fit, d_sse)
+        ev.evaluate_csr_device(d_words, d_off, n, int(offsets[-1]), d_fit, d_sse)
         ev.synchronize()
         st = ev.stats
         return st
@@ -729,7 +729,7 @@ def run_capacity(args):
         ev = g.Evaluator(num_registers=8, dispatch=dispatch, dedup=dedup)
         ev.set_dataset(ds)
         w, off, fit = population(P0)
-        ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P0, fit.data_ptr())
+        ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P0, P0 * L, fit.data_ptr())
         ev.synchronize()
         used = before - torch.cuda.mem_get_info(dev)[0]
         per_prog = used / P0
@@ -744,11 +744,11 @@ def run_capacity(args):
                 ev = g.Evaluator(num_registers=8, dispatch=dispatch, dedup=dedup)
                 ev.set_dataset(ds)
                 w, off, fit = population(P)
-                ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, fit.data_ptr())   # the proof
+                ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, P * L, fit.data_ptr())   # the proof
                 ev.synchronize()
                 ms = []
                 for _ in range(2):
-                    ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, fit.data_ptr())
+                    ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, P * L, fit.data_ptr())
                     st = ev.stats
                     ms.append(st.prepass_ms + st.interp_ms + st.finalize_ms)
                 st = ev.stats

@@ -182,7 +182,7 @@ def load_library(path: Optional[Path] = None) -> C.CDLL:
         "galop_set_dataset_device": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32]),
         "galop_evaluate_population": (C.c_int, [_P, _U32P, _U8P, C.c_int64, C.c_int64, _F32P]),
         "galop_evaluate_csr": (C.c_int, [_P, _U32P, _I64P, C.c_int64, _F32P, _F64P]),
-        "galop_evaluate_csr_device": (C.c_int, [_P, _P, _P, C.c_int64, _P, _P, _P]),
+        "galop_evaluate_csr_device": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int64, _P, _P, _P]),
         "galop_case_outputs_csr": (C.c_int, [_P, _U32P, _I64P, C.c_int64, _F32P]),
         "galop_trace_program": (C.c_int, [_P, _U32P, C.c_int64, _F32P, _I64P]),
         "galop_effective_csr": (C.c_int, [_P, _U32P, _I64P, C.c_int64, _I64P, _U32P]),
@@ -438,9 +438,11 @@ class Evaluator:
                                                  n, _ptr(fit, C.c_float), _ptr(sse, C.c_double)))
         return (fit, sse) if with_sse else fit
 
-    def evaluate_csr_device(self, d_words: int, d_offsets: int, n_programs: int, d_fitness: int,
-                            d_sse: int = 0, stream: int = 0):
-        self._check(self._lib.galop_evaluate_csr_device(self._ctx, d_words, d_offsets, n_programs,
+    def evaluate_csr_device(self, d_words: int, d_offsets: int, n_programs: int, total_words: int,
+                            d_fitness: int, d_sse: int = 0, stream: int = 0):
+        """Queue an evaluation of device-resident CSR programs on `stream`
+        (0: the context's stream) without waiting; ``stats`` waits for it."""
+        self._check(self._lib.galop_evaluate_csr_device(self._ctx, d_words, d_offsets, n_programs, total_words,
                                                         d_fitness, d_sse or None, stream or None))
 
     def case_outputs(self, words: np.ndarray, offsets: np.ndarray, dataset: Optional[Dataset] = None):

@@ -5,6 +5,10 @@
 Objects go to ``galop_b200/_build`` (not committed).  nvcc cross-compiles, so
 this runs on a machine without a GPU.
 
+``csrc/dispatch_gen.cuh`` is generated: the build first renders it from
+``csrc/gen_dispatch.py`` and rewrites it when the text differs, so the
+compiled tables always come from the generator.
+
 Floating-point flags matter for parity with the CPU interpreter: no
 ``--use_fast_math``, ``--fmad=false`` (no FMA contraction, like the
 reference's ISO C++ build), IEEE division and denormals (``-prec-div=true
@@ -58,8 +62,19 @@ def _compile(src: Path, verbose: bool) -> Path:
     return obj
 
 
+def regenerate_dispatch() -> bool:
+    """Render csrc/dispatch_gen.cuh from csrc/gen_dispatch.py; True if the
+    file was stale and has been rewritten."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("galop_gen_dispatch", CSRC / "gen_dispatch.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.write_if_changed(CSRC / "dispatch_gen.cuh")
+
+
 def build(verbose: bool = False, jobs: int | None = None) -> Path:
     BUILD.mkdir(exist_ok=True)
+    regenerate_dispatch()
     srcs = sources()
     with ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))

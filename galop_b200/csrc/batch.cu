@@ -193,12 +193,12 @@ int enqueue(galop_batch* b) {
                                                b->prog_pop.p);
     SpanSource src{b->arena.p, b->starts.p, b->lens.p};
     prepass_count_kernel<SpanSource><<<blocks, tpb, 0, s>>>(src, G, ctx->isa, strip ? 1 : 0, b->eff_len.p,
-                                                            b->counters.p + 1);
+                                                            b->counters.p + 1, nullptr);
     scan_tile_sums_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(b->eff_len.p, G, b->tiles.p);
     scan_tile_offsets_kernel<<<1, kScanThreads, 0, s>>>(b->tiles.p, n_tiles);
     scan_apply_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(b->eff_len.p, G, b->tiles.p, n_tiles, b->eff_off.p);
     prepass_compact_kernel<SpanSource><<<blocks, tpb, 0, s>>>(src, G, ctx->isa, strip ? 1 : 0, b->eff_off.p,
-                                                              b->uops.p, nullptr, b->fmt);
+                                                              b->uops.p, nullptr, b->fmt, nullptr);
     const bool fold = b->fmt.wide && strip;
     if (b->fmt.wide) {
         // constants folded per program with its own population's input count
@@ -229,9 +229,9 @@ int enqueue(galop_batch* b) {
         b->launches += 5;
     }
     batch_key_kernel<<<blocks, tpb, 0, s>>>(b->layout.p, b->prog_pop.p, b->eff_len.p, G, b->key.p);
-    order_hist_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p);
-    order_scan_kernel<<<1, 1024, 0, s>>>(b->hist.p);
-    order_scatter_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p, b->order.p);
+    order_hist_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p, nullptr, 0);
+    order_scan_kernel<<<1, 1024, 0, s>>>(b->hist.p, nullptr);
+    order_scatter_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p, b->order.p, nullptr, 0);
     batch_item_count_kernel<<<blocks, tpb, 0, s>>>(b->order.p, b->prog_pop.p, b->chunks_of_pop.p, b->key.p, G,
                                                    b->cnt.p);
     scan_tile_sums_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(b->cnt.p, G, b->tiles.p);

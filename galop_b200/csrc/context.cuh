@@ -61,10 +61,12 @@ inline double targets_ss_tot(const float* y, int64_t n) {
     return ss;
 }
 
-// Most cases one work item of the persistent interpreter covers (a
-// multiple of every pass width 32*K): longer case ranges are split into
-// chunks whose partial sums are added in chunk order.
-constexpr int64_t kMaxItemCases = 16384;
+// Device counters of a context: [0] work-queue head, [1..5] instruction
+// totals of the call (raw, effective, interpreted, dedup copies and their
+// instructions), [6] set when caller-stated device offsets are inconsistent,
+// [7] size of the first register-file class in the order.
+constexpr int kCounters = 8;
+constexpr int kCounterBadOffsets = 6;
 
 struct galop_ctx {
     galop_options opt{};
@@ -94,7 +96,7 @@ struct galop_ctx {
     DevBuf<uint32_t> livein;      // registers each program reads before writing them (fold.cuh)
     DevBuf<float> fitness, outputs, trace;
     DevBuf<double> sse, partial;
-    DevBuf<unsigned long long> counters;   // [0] queue head, [1..2] totals
+    DevBuf<unsigned long long> counters;   // kCounters entries; layout in run_prepass
     DevBuf<unsigned int> hist;
     std::vector<int64_t> host_tmp;
 

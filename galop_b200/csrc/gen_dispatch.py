@@ -1,21 +1,15 @@
-"""Generate dispatch_gen.cuh: jump-table register access for the interpreter.
+"""Generate dispatch_gen.cuh: PTX jump tables of the interpreters.
 
-The LGP register file of a lane lives in real registers, float r[NR][K]
-(K fitness cases per lane).  An instruction names its registers at run time
-(warp-uniform), so reading r[s1] must select one of NR register groups.
-Written as a C++ switch, the compiler turns that into predicated selects
-costing NR*K instructions per access.  These helpers instead emit PTX
-``brx.idx`` over a ``.branchtargets`` table: one indirect branch, then K
-moves (or K arithmetic instructions) in the selected arm.
+The LGP register file of a warp lives in shared memory and an instruction's
+operands are addresses, so the only run-time dispatch is on the opcode.
+These helpers emit PTX ``brx.idx`` over a ``.branchtargets`` table: one
+indirect branch, then the K arithmetic instructions of the selected op.
 
-Emitted for NR in {8, 16} and K in {1, 2, 4, 8}:
-  cheap    t[k] = OP(a[k], b[k]) on the opcode alone (register file in
-           shared memory, operands already loaded)
-  gather   out[k] = r[idx][k]
-  scatter  r[idx][k] = v[k]
-  od_vec   r[d][k] = OP(a[k], b[k])   table index op*NR + d
-  od_sca   r[d][k] = OP(a[k], c)      (constant src2, one scalar)
-  wide     one whole binary instruction of the 16-byte micro-op kernel:
+Emitted for K in {1, 2, 4, 8} and both ISA profiles:
+  cheap    t[k] = OP(a[k], b[k]) on the opcode alone (dispatch 2: operands
+           already loaded from the shared-memory register file)
+  wide     one whole binary instruction of the 16-byte micro-op kernel
+           (dispatch 3, one instruction at a time: register traces):
            load a (and b) from the shared-memory register file, compute,
            store t -- the table index is op | constant-src2 << 3, and
            protected DIV is one of the arms
@@ -33,13 +27,14 @@ comparison holds, else 0.0 -- false for NaN operands, like the C++ `a < b ?
 1.0f : 0.0f`).  Table entries of other opcodes fall through to the end
 label (never taken: the interpreter routes those ops elsewhere).
 
-Run: python galop_b200/csrc/gen_dispatch.py   (rewrites dispatch_gen.cuh)
+The build (galop_b200/build.py) calls render() and rewrites dispatch_gen.cuh
+whenever its text differs, so the header cannot drift from this generator.
+Run by hand: python galop_b200/csrc/gen_dispatch.py
 """
 from __future__ import annotations
 
 from pathlib import Path
 
-NRS = (8, 16)
 KS = (1, 2, 4, 8)
 CHEAP = {0: "add.rn.f32", 1: "sub.rn.f32", 2: "mul.rn.f32", 6: "set.lt.f32.f32", 7: "set.gt.f32.f32"}
 PROFILES = {0: (0, 1, 2, 6, 7), 1: (0, 1, 2)}   # REF, BJ
@@ -54,66 +49,6 @@ def asm_block(lines: list[str], outs: list[str], ins: list[str]) -> str:
     return (f'    asm("{{\\n\\t{body}\\n\\t}}"\n'
             f'        : {", ".join(outs) if outs else ""}\n'
             f'        : {", ".join(ins)});\n')
-
-
-def gather(nr: int, k: int) -> str:
-    # outputs %0..%k-1 ; inputs: idx %k, r[j][q] %(k+1 + j*k + q)
-    lines = ["Lt%=: .branchtargets " + ", ".join(f"L{j}_%=" for j in range(nr)) + ";", f"brx.idx %{k}, Lt%=;"]
-    for j in range(nr):
-        movs = " ".join(f"mov.f32 %{q}, %{k + 1 + j * k + q};" for q in range(k))
-        tail = " bra.uni Le%=;" if j < nr - 1 else ""
-        lines.append(f"L{j}_%=: {movs}{tail}")
-    lines.append("Le%=:")
-    outs = [f'"=f"(o[{q}])' for q in range(k)]
-    ins = ['"r"(idx)'] + [f'"f"(r[{j}][{q}])' for j in range(nr) for q in range(k)]
-    return (f"    static __device__ __forceinline__ void gather(const float (&r)[{nr}][{k}], uint32_t idx, "
-            f"float (&o)[{k}]) {{\n" + asm_block(lines, outs, ins) + "    }\n")
-
-
-def scatter(nr: int, k: int) -> str:
-    # outputs r[j][q] "+f" %(j*k+q) ; inputs idx %(nr*k), v[q] %(nr*k+1+q)
-    no = nr * k
-    lines = ["Lt%=: .branchtargets " + ", ".join(f"L{j}_%=" for j in range(nr)) + ";", f"brx.idx %{no}, Lt%=;"]
-    for j in range(nr):
-        movs = " ".join(f"mov.f32 %{j * k + q}, %{no + 1 + q};" for q in range(k))
-        tail = " bra.uni Le%=;" if j < nr - 1 else ""
-        lines.append(f"L{j}_%=: {movs}{tail}")
-    lines.append("Le%=:")
-    outs = [f'"+f"(r[{j}][{q}])' for j in range(nr) for q in range(k)]
-    ins = ['"r"(idx)'] + [f'"f"(v[{q}])' for q in range(k)]
-    return (f"    static __device__ __forceinline__ void scatter(float (&r)[{nr}][{k}], uint32_t idx, "
-            f"const float (&v)[{k}]) {{\n" + asm_block(lines, outs, ins) + "    }\n")
-
-
-def od(nr: int, k: int, profile: int, scalar: bool) -> str:
-    # outputs r[j][q] "+f" %(j*k+q); inputs idx %no, a[q] %(no+1+q), b[q] %(no+1+k+q) or c %(no+1+k)
-    no = nr * k
-    ops = PROFILES[profile]
-    labels = []
-    for op in range(8):
-        for d in range(nr):
-            labels.append(f"L{op}_{d}_%=" if op in ops else "Le%=")
-    lines = ["Lt%=: .branchtargets " + ", ".join(labels) + ";", f"brx.idx %{no}, Lt%=;"]
-    for op in ops:
-        for d in range(nr):
-            ins_ = []
-            for q in range(k):
-                bsrc = f"%{no + 1 + k}" if scalar else f"%{no + 1 + k + q}"
-                ins_.append(f"{CHEAP[op]} %{d * k + q}, %{no + 1 + q}, {bsrc};")
-            lines.append(f"L{op}_{d}_%=: " + " ".join(ins_) + " bra.uni Le%=;")
-    lines.append("Le%=:")
-    outs = [f'"+f"(r[{j}][{q}])' for j in range(nr) for q in range(k)]
-    ins = ['"r"(od)'] + [f'"f"(a[{q}])' for q in range(k)]
-    if scalar:
-        ins.append('"f"(c)')
-        sig = f"const float (&a)[{k}], float c"
-        name = "od_sca"
-    else:
-        ins += [f'"f"(b[{q}])' for q in range(k)]
-        sig = f"const float (&a)[{k}], const float (&b)[{k}]"
-        name = "od_vec"
-    return (f"    static __device__ __forceinline__ void {name}(float (&r)[{nr}][{k}], uint32_t od, {sig}) {{\n"
-            + asm_block(lines, outs, ins) + "    }\n")
 
 
 def cheap_table(k: int, profile: int) -> str:
@@ -323,21 +258,14 @@ def wide_loop(k: int, profile: int) -> str:
             f'        : {outs}\n        : {ins}\n        : "memory");\n    }}\n')
 
 
-def main() -> None:
+HEADER_PATH = Path(__file__).resolve().parent / "dispatch_gen.cuh"
+
+
+def render() -> str:
     out = ["// dispatch_gen.cuh -- GENERATED by gen_dispatch.py; do not edit by hand.",
-           "// Jump-table (PTX brx.idx) register access for the LGP interpreter; see",
-           "// gen_dispatch.py for what each helper does.",
-           "#pragma once", "#include <cstdint>", "", "namespace galop {", "",
-           "template <int NR, int K, int PROFILE>", "struct Brx;", ""]
-    for nr in NRS:
-        for k in KS:
-            for prof in PROFILES:
-                out.append(f"template <>\nstruct Brx<{nr}, {k}, {prof}> {{")
-                out.append(gather(nr, k))
-                out.append(scatter(nr, k))
-                out.append(od(nr, k, prof, False))
-                out.append(od(nr, k, prof, True))
-                out.append("};\n")
+           "// PTX jump tables (brx.idx) of the LGP interpreters; see gen_dispatch.py",
+           "// for what each helper does.",
+           "#pragma once", "#include <cstdint>", "", "namespace galop {", ""]
     out.append("template <int K, int PROFILE>\nstruct CheapOps;\n")
     for k in KS:
         for prof in PROFILES:
@@ -357,9 +285,21 @@ def main() -> None:
             out.append(wide_loop(k, prof))
             out.append("};\n")
     out.append("}  // namespace galop\n")
-    path = Path(__file__).resolve().parent / "dispatch_gen.cuh"
-    path.write_text("\n".join(out))
-    print(path)
+    return "\n".join(out)
+
+
+def write_if_changed(path: Path = HEADER_PATH) -> bool:
+    """Rewrite the header when its text differs from render(); True if it did."""
+    text = render()
+    if path.exists() and path.read_text() == text:
+        return False
+    path.write_text(text)
+    return True
+
+
+def main() -> None:
+    changed = write_if_changed()
+    print(HEADER_PATH, "(rewritten)" if changed else "(up to date)")
 
 
 if __name__ == "__main__":

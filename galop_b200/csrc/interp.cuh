@@ -1,24 +1,26 @@
-// interp.cuh -- the warp-per-individual LGP interpreter for sm_100a.
+// interp.cuh -- shared definitions of the warp-per-individual interpreters
+// and the compact interpreter (dispatch 2).
 //
 // One warp evaluates one program (or one case chunk of it); lane l of the warp
-// owns K consecutive fitness cases of every 32*K-case pass and keeps their
-// NR-entry register files in real registers (float r[NR][K]).  Register
-// indices in an instruction are warp-uniform, so "read register s1" is a
-// switch whose every arm moves K values with static indices: no local-memory
-// register array (the reference's program_partial_sse keeps reg[] in local
-// memory, src/EvaluatorCuda.cu:127, :151-153).
-//
-// Instruction stream: 32 micro-ops at a time are read with one coalesced load
-// (lane j holds word j) and broadcast with a shuffle.
+// owns K fitness cases of every 32*K-case pass.  The LGP register file of
+// those cases lives in shared memory, so a register index is an address
+// offset: no local-memory register array (the reference's
+// program_partial_sse keeps reg[] in local memory, src/EvaluatorCuda.cu:127,
+// :151-153) and no select chains over NR registers.
 //
 // Fitness cases: feature-major (SoA) arrays padded to a multiple of 1024
-// cases; a lane reads its K consecutive cases of a feature with one 8/16-byte
-// vector load, so a warp reads 32*K contiguous floats per feature.
+// cases; a lane reads its cases of a feature with 8/16-byte vector loads,
+// so a warp reads 32*K contiguous floats per feature.
 //
 // Semantics per case follow src/Interpreter.cpp:36-59: r0..k-1 = inputs, the
 // rest 0, execute every instruction in order, output r[OUTPUT_REG].  Fitness
 // follows src/Evaluator.cpp:11-45 and :88-91 (see galop_reduce in the header
 // for the three accumulation modes).
+//
+// The default interpreter (dispatch 3) is interp_wide.cuh; this file keeps
+// the compact one (dispatch 2: 32-bit micro-ops, one instruction at a time),
+// which the no-allocation entry point uses and the parity tests hold to the
+// same bar.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -83,39 +85,6 @@ struct InterpArgs {
     const int64_t* n_items_dev;    // the item count computed on the device (dedup), or null
 };
 
-#define GALOP_CASES16(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) \
-                         X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15)
-
-template <int NR, int K>
-__device__ __forceinline__ void read_reg(const float (&r)[NR][K], uint32_t idx, float (&out)[K]) {
-    switch (idx) {
-#define GALOP_RD(j)                                                        \
-        case j:                                                            \
-            if constexpr (j < NR) {                                        \
-                _Pragma("unroll") for (int k = 0; k < K; ++k) out[k] = r[j][k]; \
-            }                                                              \
-            break;
-        GALOP_CASES16(GALOP_RD)
-#undef GALOP_RD
-        default: break;
-    }
-}
-
-template <int NR, int K>
-__device__ __forceinline__ void write_reg(float (&r)[NR][K], uint32_t idx, const float (&v)[K]) {
-    switch (idx) {
-#define GALOP_WR(j)                                                        \
-        case j:                                                            \
-            if constexpr (j < NR) {                                        \
-                _Pragma("unroll") for (int k = 0; k < K; ++k) r[j][k] = v[k]; \
-            }                                                              \
-            break;
-        GALOP_CASES16(GALOP_WR)
-#undef GALOP_WR
-        default: break;
-    }
-}
-
 template <int K>
 __device__ __forceinline__ void load_cases(const float* __restrict__ p, float (&v)[K]) {
     if constexpr (K % 4 == 0) {
@@ -133,129 +102,10 @@ __device__ __forceinline__ void load_cases(const float* __restrict__ p, float (&
     }
 }
 
-// One instruction over the lane's K cases.
-template <int NR, int K, int PROFILE>
-__device__ __forceinline__ void step(float (&r)[NR][K], uint32_t u, const ConstPool& cp) {
-    const uint32_t op = uop_op(u);
-    float a[K], b[K], t[K];
-    read_reg<NR, K>(r, uop_src1(u), a);
-    if (uop_is_const(u)) {
-        const float c = cp.c[uop_src2(u)];
-#pragma unroll
-        for (int k = 0; k < K; ++k) b[k] = c;
-    } else {
-        read_reg<NR, K>(r, uop_src2(u), b);
-    }
-    switch (op) {
-        case kAdd:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = __fadd_rn(a[k], b[k]);
-            break;
-        case kSub:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = __fsub_rn(a[k], b[k]);
-            break;
-        case kMul:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = __fmul_rn(a[k], b[k]);
-            break;
-        case kDiv:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = (b[k] != 0.0f) ? __fdiv_rn(a[k], b[k]) : 1.0f;
-            break;
-        case kSin:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = sinf(b[k]);
-            break;
-        case kCos:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = cosf(b[k]);
-            break;
-        case kOp6:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp6, a[k], b[k]);
-            break;
-        default:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp7, a[k], b[k]);
-            break;
-    }
-    write_reg<NR, K>(r, uop_dest(u), t);
-}
-
-// ---- dispatch strategy 1: jump tables (default) --------------------------------
-//
-// The C++ switches above are compiled into predicated select chains: every
-// register read or write costs NR*K instructions.  Strategy 1 uses the PTX
-// brx.idx helpers of dispatch_gen.cuh instead: one indirect branch per
-// access, then K moves.  Single-instruction binary ops (ADD, SUB, MUL, and
-// LT, GT in the REF profile) are fused with their destination: one branch on
-// op*NR+dest lands on K arithmetic instructions that write r[dest] directly,
-// with a constant src2 kept as one scalar.  DIV and the unary ops gather,
-// compute in C++ and scatter: their own cost dwarfs the moves.
-template <int NR, int K, int PROFILE>
-__device__ __forceinline__ void step_brx(float (&r)[NR][K], uint32_t u, const ConstPool& cp) {
-    using B = Brx<NR, K, PROFILE>;
-    const uint32_t op = uop_op(u);
-    const uint32_t dest = uop_dest(u);
-    const bool konst = uop_is_const(u);
-    const uint32_t s2 = uop_src2(u);
-    if (u & 0x40u) {                       // unary: reads src2 only
-        float b[K], t[K];
-        if (konst) {
-            const float c = cp.c[s2];
-#pragma unroll
-            for (int k = 0; k < K; ++k) b[k] = c;
-        } else {
-            B::gather(r, s2, b);
-        }
-        switch (op) {
-            case kSin:
-#pragma unroll
-                for (int k = 0; k < K; ++k) t[k] = sinf(b[k]);
-                break;
-            case kCos:
-#pragma unroll
-                for (int k = 0; k < K; ++k) t[k] = cosf(b[k]);
-                break;
-            case kOp6:
-#pragma unroll
-                for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp6, 0.0f, b[k]);
-                break;
-            default:
-#pragma unroll
-                for (int k = 0; k < K; ++k) t[k] = apply_op<PROFILE>(kOp7, 0.0f, b[k]);
-                break;
-        }
-        B::scatter(r, dest, t);
-        return;
-    }
-    float a[K];
-    B::gather(r, uop_src1(u), a);
-    if (op == kDiv) {
-        float t[K];
-        if (konst) {
-            const float c = cp.c[s2];
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = (c != 0.0f) ? __fdiv_rn(a[k], c) : 1.0f;
-        } else {
-            float b[K];
-            B::gather(r, s2, b);
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = (b[k] != 0.0f) ? __fdiv_rn(a[k], b[k]) : 1.0f;
-        }
-        B::scatter(r, dest, t);
-        return;
-    }
-    const uint32_t od = op * NR + dest;
-    if (konst) {
-        B::od_sca(r, od, a, cp.c[s2]);
-    } else {
-        float b[K];
-        B::gather(r, s2, b);
-        B::od_vec(r, od, a, b);
-    }
-}
+// Most cases one work item of the persistent interpreter covers (a
+// multiple of every pass width 32*K): longer case ranges are split into
+// chunks whose partial sums are added in chunk order.
+constexpr int64_t kMaxItemCases = 16384;
 
 // KAHAN32 keeps squared errors in FP32 only while |error| <= 2^52: a square
 // is then <= 2^104 and a lane's compensated sum of up to 2^20 of them stays
@@ -269,148 +119,7 @@ __device__ __forceinline__ double warp_sum_f64(double v) {
     return v;
 }
 
-// src/Evaluator.cpp:44 then :88-91.
-
-template <int NR, int K, int PROFILE, int REDUCE, int MODE, int DISPATCH>
-__global__ void __launch_bounds__(256, 1)
-interp_kernel(InterpArgs args) {
-    const int lane = threadIdx.x & 31;
-    const int64_t total_items = args.n_programs * (int64_t)args.n_chunks;
-    constexpr int kPass = 32 * K;
-
-    for (;;) {
-        unsigned long long item = 0;
-        if (lane == 0) item = atomicAdd(args.counter, 1ull);
-        item = __shfl_sync(0xffffffffu, item, 0);
-        if ((int64_t)item >= total_items) break;
-
-        const int64_t slot = (int64_t)item / args.n_chunks;
-        const int chunk = (int)((int64_t)item % args.n_chunks);
-        const int64_t prog = args.order ? (int64_t)args.order[slot] : slot;
-        const int64_t p0 = args.eff_off[prog];
-        const int64_t L = args.eff_off[prog + 1] - p0;
-        const uint32_t* __restrict__ pw = args.uops + p0;
-
-        const int64_t cbeg = (int64_t)chunk * args.chunk_cases;
-        int64_t cend = cbeg + args.chunk_cases;
-        if (cend > args.N) cend = args.N;
-
-        float ks = 0.0f, kc = 0.0f;   // Kahan sum / compensation (KAHAN32)
-        double big = 0.0;             // KAHAN32: squares of errors beyond kKahanMaxError
-        double acc = 0.0;             // FP64 / ORDERED accumulator
-
-        for (int64_t base = cbeg; base < cend; base += kPass) {
-            const int64_t c0 = base + (int64_t)lane * K;
-            float r[NR][K];
-#pragma unroll
-            for (int f = 0; f < NR; ++f) {
-                if (f < args.num_inputs) {
-                    load_cases<K>(args.X + (int64_t)f * args.Np + c0, r[f]);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < K; ++k) r[f][k] = 0.0f;
-                }
-            }
-            if constexpr (MODE == kModeTrace) {
-#pragma unroll
-                for (int j = 0; j < NR; ++j)
-#pragma unroll
-                    for (int k = 0; k < K; ++k)
-                        args.trace[(int64_t)j * kPass + lane * K + k] = r[j][k];
-            }
-
-            for (int64_t wb = 0; wb < L; wb += 32) {
-                const uint32_t win = (wb + lane < L) ? __ldg(pw + wb + lane) : 0u;
-                const int n = (L - wb < 32) ? (int)(L - wb) : 32;
-                for (int j = 0; j < n; ++j) {
-                    const uint32_t u = __shfl_sync(0xffffffffu, win, j);
-                    if constexpr (DISPATCH == 1) step_brx<NR, K, PROFILE>(r, u, args.consts);
-                    else step<NR, K, PROFILE>(r, u, args.consts);
-                    if constexpr (MODE == kModeTrace) {
-                        const int64_t row = (wb + j + 1) * NR;
-#pragma unroll
-                        for (int q = 0; q < NR; ++q)
-#pragma unroll
-                            for (int k = 0; k < K; ++k)
-                                args.trace[(row + q) * kPass + lane * K + k] = r[q][k];
-                    }
-                }
-            }
-
-            float o[K];
-            if constexpr (DISPATCH >= 1) Brx<NR, K, PROFILE>::gather(r, (uint32_t)args.output_reg, o);
-            else read_reg<NR, K>(r, (uint32_t)args.output_reg, o);
-
-            if constexpr (MODE == kModeOutputs) {
-#pragma unroll
-                for (int k = 0; k < K; ++k)
-                    if (c0 + k < cend) args.outputs[prog * args.N + c0 + k] = o[k];
-            } else if constexpr (MODE == kModeFitness) {
-                float t[K];
-                load_cases<K>(args.y + c0, t);
-                if constexpr (REDUCE == kReduceKahan32) {
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        const float e = __fsub_rn(o[k], t[k]);
-                        const bool valid = c0 + k < cend;
-                        const bool huge = !(fabsf(e) <= kKahanMaxError);
-                        const float q = (valid && !huge) ? __fmul_rn(e, e) : 0.0f;
-                        if (valid && huge) big = __dadd_rn(big, __dmul_rn((double)e, (double)e));
-                        const float yk = __fsub_rn(q, kc);
-                        const float tt = __fadd_rn(ks, yk);
-                        kc = __fsub_rn(__fsub_rn(tt, ks), yk);
-                        ks = tt;
-                    }
-                } else if constexpr (REDUCE == kReduceFp64) {
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        const double e = (double)o[k] - (double)t[k];
-                        if (c0 + k < cend) acc = __dadd_rn(acc, __dmul_rn(e, e));
-                    }
-                } else {
-                    // Strict case order: base+0, base+1, ... (lane-major, K per lane).
-                    double q[K];
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        const double e = (double)o[k] - (double)t[k];
-                        q[k] = __dmul_rn(e, e);
-                    }
-                    for (int j = 0; j < 32; ++j) {
-#pragma unroll
-                        for (int k = 0; k < K; ++k) {
-                            const double v = __shfl_sync(0xffffffffu, q[k], j);
-                            if (base + (int64_t)j * K + k < cend) acc = __dadd_rn(acc, v);
-                        }
-                    }
-                }
-            }
-            if constexpr (MODE == kModeTrace) break;  // one pass
-        }
-
-        if constexpr (MODE == kModeFitness) {
-            double sse;
-            if constexpr (REDUCE == kReduceKahan32) {
-                sse = warp_sum_f64((double)ks - (double)kc + big);
-            } else if constexpr (REDUCE == kReduceFp64) {
-                sse = warp_sum_f64(acc);
-            } else {
-                sse = acc;  // identical in every lane
-            }
-            if (lane == 0) {
-                if (args.n_chunks == 1) {
-                    args.fitness[prog] = fitness_of(sse, args.N, args.obj);
-                    if (args.sse) args.sse[prog] = sse;
-                } else {
-                    args.partial[prog * args.n_chunks + chunk] = sse;
-                }
-            }
-        }
-        if constexpr (MODE == kModeTrace) break;
-    }
-}
-
-
-// ---- dispatch strategy 2 (default): the LGP register file in shared memory -----
+// ---- dispatch 2: the LGP register file in shared memory, 32-bit micro-ops -----
 //
 // Each lane keeps its K cases' NR registers in its own shared-memory slots:
 // register j of the warp is a block of 32*K floats, lane l owns the K

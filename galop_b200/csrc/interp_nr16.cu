@@ -2,20 +2,7 @@
 #include "interp.cuh"
 #include "interp_wide.cuh"
 
-
 namespace galop {
-
-template <int K, int P, int D>
-static const void* pick_mode(int reduce, int mode) {
-    if (mode == kModeOutputs) return (const void*)&interp_kernel<16, K, P, kReduceFp64, kModeOutputs, D>;
-    if (mode == kModeTrace) return (const void*)&interp_kernel<16, K, P, kReduceFp64, kModeTrace, D>;
-    switch (reduce) {
-        case kReduceKahan32: return (const void*)&interp_kernel<16, K, P, kReduceKahan32, kModeFitness, D>;
-        case kReduceFp64: return (const void*)&interp_kernel<16, K, P, kReduceFp64, kModeFitness, D>;
-        case kReduceOrdered: return (const void*)&interp_kernel<16, K, P, kReduceOrdered, kModeFitness, D>;
-        default: return nullptr;
-    }
-}
 
 template <int K, int P>
 static const void* pick_wide_mode(int reduce, int mode) {
@@ -41,13 +28,6 @@ static const void* pick_smem_mode(int reduce, int mode) {
     }
 }
 
-template <int K, int D>
-static const void* pick_profile(int profile, int reduce, int mode) {
-    if (profile == kProfileRef) return pick_mode<K, kProfileRef, D>(reduce, mode);
-    if (profile == kProfileBj) return pick_mode<K, kProfileBj, D>(reduce, mode);
-    return nullptr;
-}
-
 template <int K>
 static const void* pick_dispatch(int dispatch, int profile, int reduce, int mode) {
     if (dispatch == 3) {
@@ -60,8 +40,7 @@ static const void* pick_dispatch(int dispatch, int profile, int reduce, int mode
         if (profile == kProfileBj) return pick_smem_mode<K, kProfileBj>(reduce, mode);
         return nullptr;
     }
-    if (dispatch == 1) return pick_profile<K, 1>(profile, reduce, mode);
-    return pick_profile<K, 0>(profile, reduce, mode);
+    return nullptr;
 }
 
 const void* interp_kernel_nr16(int k, int dispatch, int profile, int reduce, int mode) {

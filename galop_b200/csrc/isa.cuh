@@ -101,6 +101,17 @@ __device__ __forceinline__ uint4 encode_wide(const Decoded& d, uint32_t stride, 
     return u;
 }
 
+// Per-program word the folding pass writes for the interpreter (one uint32
+// per program): registers read before written (bits 0-15; the i-th set bit
+// is loaded into register-file slot i), slots the program's values use
+// (bits 16-20), slot that holds the output value at the end (bits 24-27).
+__host__ __device__ __forceinline__ uint32_t pack_livein(uint32_t regs, uint32_t slots, uint32_t out_slot) {
+    return (regs & 0xFFFFu) | (slots << 16) | (out_slot << 24);
+}
+__host__ __device__ __forceinline__ uint32_t livein_regs(uint32_t w) { return w & 0xFFFFu; }
+__host__ __device__ __forceinline__ uint32_t livein_slots(uint32_t w) { return (w >> 16) & 31u; }
+__host__ __device__ __forceinline__ uint32_t livein_out_slot(uint32_t w) { return (w >> 24) & 15u; }
+
 // Which micro-op form the pre-pass writes.
 struct UopFormat {
     int wide;              // 0: 32-bit micro-ops, 1: 16-byte wide micro-ops

@@ -2,18 +2,21 @@
 //
 // Every other entry point keeps its working buffers (micro-ops, offsets,
 // evaluation order, work-queue counters, per-chunk partial sums) in device
-// memory it obtains with cudaMalloc and grows as populations grow.  Some
-// callers cannot let a library do that: cudaMalloc and cudaFree synchronise
-// the whole device and are not permitted while a stream is being captured,
-// and hosts that own a fixed device-memory budget (a framework's own pool,
-// a serving process that must never hit an out-of-memory error mid-run)
-// cannot have a library allocate behind their back.
+// memory that it obtains with cudaMalloc and grows as populations grow.
+// Some callers cannot let a library do that:
+//   - hosts that own all device memory through their own pool allocator
+//     (a framework's caching allocator, a serving process with a fixed
+//     per-model budget) and must never see an out-of-memory failure, or
+//     memory they did not account for, in the middle of a run;
+//   - loops that must not stall: cudaMalloc and cudaFree can synchronise
+//     the whole device.
 //
-// galop_evaluate_csr_noalloc runs the same pre-pass and interpreter kernels
-// as galop_evaluate_csr_device, but its working buffers live in one
-// file-scope __device__ array of fixed size (about 11 MiB) that every GPU
-// loading this library holds until the process exits.  It allocates nothing:
-// no cudaMalloc, no cudaFree, no allocating library routine.
+// galop_evaluate_csr_noalloc runs the same pre-pass and the compact
+// interpreter (dispatch 2: one 32-bit micro-op per instruction) on the
+// caller's device buffers, with its working buffers in one file-scope
+// __device__ array of fixed size (about 11 MiB) that every GPU loading this
+// library holds until the process exits.  It allocates nothing: no
+// cudaMalloc, no cudaFree, no allocating library routine.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <mutex>
@@ -35,6 +38,7 @@ constexpr int64_t kNaMaxPrograms = GALOP_NOALLOC_MAX_PROGRAMS;
 constexpr int64_t kNaMaxWords = GALOP_NOALLOC_MAX_WORDS;
 constexpr int64_t kNaMaxPartials = 4 * GALOP_NOALLOC_MAX_PROGRAMS;
 constexpr int64_t kNaMaxTiles = (kNaMaxPrograms + kScanTile - 1) / kScanTile;
+constexpr int kNaDispatch = 2;   // 32-bit micro-ops: one scratch word per instruction
 
 struct NoAllocScratch {
     uint32_t uops[kNaMaxWords];
@@ -44,7 +48,9 @@ struct NoAllocScratch {
     int32_t eff_len[kNaMaxPrograms];
     int32_t order[kNaMaxPrograms];
     unsigned int hist[kOrderBins];
-    unsigned long long counters[4];   // [0] work-queue head, [1..2] length totals
+    // [0] work-queue head, [1..2] length totals, [3] set by
+    // check_offsets_kernel when the caller's offsets are inconsistent
+    unsigned long long counters[4];
 };
 
 // The scratch itself.  Host code must not pass `g_noalloc_scratch` to a
@@ -56,13 +62,47 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 NoAllocScratch* g_scratch_addr[kMaxDevices] = {};
 
-// Once per device, with that device current: the scratch's device address.
+// Every kernel this entry point can launch, loaded on the current device
+// (cudaFuncGetAttributes makes the runtime load a kernel's code), so that
+// no later call, whatever its options, loads code on the device.
+cudaError_t preload_kernels() {
+    cudaFuncAttributes fa{};
+    const void* fixed[] = {
+        (const void*)&check_offsets_kernel,
+        (const void*)&prepass_count_kernel<CsrSource>,
+        (const void*)&scan_tile_sums_kernel,
+        (const void*)&scan_tile_offsets_kernel,
+        (const void*)&scan_apply_kernel,
+        (const void*)&prepass_compact_kernel<CsrSource>,
+        (const void*)&order_hist_kernel,
+        (const void*)&order_scan_kernel,
+        (const void*)&order_scatter_kernel,
+        (const void*)&finalize_kernel,
+        (const void*)&poison_results_kernel,
+    };
+    for (const void* f : fixed)
+        if (cudaError_t e = cudaFuncGetAttributes(&fa, f)) return e;
+    for (int nr : {8, 16})
+        for (int k : {1, 2, 4, 8})
+            for (int profile : {kProfileRef, kProfileBj})
+                for (int reduce : {kReduceKahan32, kReduceFp64, kReduceOrdered}) {
+                    const void* f = nr == 8 ? interp_kernel_nr8(k, kNaDispatch, profile, reduce, kModeFitness)
+                                            : interp_kernel_nr16(k, kNaDispatch, profile, reduce, kModeFitness);
+                    if (!f) return cudaErrorInvalidDeviceFunction;
+                    if (cudaError_t e = cudaFuncGetAttributes(&fa, f)) return e;
+                }
+    return cudaSuccess;
+}
+
+// Once per device, with that device current: the scratch's device address
+// (checked return code) and the kernels' code.
 cudaError_t scratch_for_device(int device, NoAllocScratch** out) {
     if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_addr[device]) {
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e == cudaSuccess) e = preload_kernels();
         if (e != cudaSuccess) return e;
         g_scratch_addr[device] = static_cast<NoAllocScratch*>(p);
     }
@@ -94,9 +134,11 @@ extern "C" int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32
     if (n_programs > 0 && (!d_fitness || !d_targets || (num_inputs > 0 && !d_inputs))) return GALOP_E_INVALID;
     if (n_programs == 0) return GALOP_OK;
 
+    // An error that an earlier CUDA call of the caller left pending is the
+    // caller's to read: report it without clearing it.
+    if (cudaPeekAtLastError() != cudaSuccess) return GALOP_E_CUDA;
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return GALOP_E_NO_DEVICE; }
-    cudaGetLastError();   // a stale error of an earlier call must not be reported as ours
     NoAllocScratch* sc = nullptr;
     if (scratch_for_device(device, &sc) != cudaSuccess) { cudaGetLastError(); return GALOP_E_CUDA; }
     int sm_count = 0;
@@ -115,49 +157,55 @@ extern "C" int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32
     const int k = (opt->cases_per_lane == 1 || opt->cases_per_lane == 2 || opt->cases_per_lane == 4 ||
                    opt->cases_per_lane == 8) ? opt->cases_per_lane : 4;
     const int wpb = (opt->warps_per_block >= 1 && opt->warps_per_block <= 8) ? opt->warps_per_block : 4;
-    // 32-bit micro-ops only (the static scratch holds one word per
-    // instruction): the wide interpreter (3) maps to the shared-memory one.
-    const int dispatch = (opt->dispatch >= 0 && opt->dispatch <= 2) ? opt->dispatch : 2;
 
-    // The work-queue head, the length totals and the order histogram carry
-    // the previous call's values: clear them first.
+    // The scratch keeps the previous call's contents: the work-queue head,
+    // the length totals, the order histogram and the offset-check flag
+    // must start at zero.
     cudaError_t e = cudaMemsetAsync(sc->counters, 0, sizeof(sc->counters), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(sc->hist, 0, sizeof(sc->hist), s);
     if (e != cudaSuccess) { cudaGetLastError(); return GALOP_E_CUDA; }
 
+    // The caller's offsets are checked against total_words on the device
+    // before any word is read: with inconsistent offsets every program is
+    // treated as empty (nothing beyond total_words is read, nothing beyond
+    // the scratch written) and every result becomes NaN.
+    const int64_t n = n_programs;
+    unsigned long long* bad = sc->counters + 3;
+    check_offsets_kernel<<<(unsigned)((n + 256) / 256), 256, 0, s>>>(d_offsets, n, total_words, bad);
+
     // Intron pass, scan, compaction, longest-first order (prepass.cuh).
     CsrSource src{d_words, d_offsets};
-    const int64_t n = n_programs;
     const int tpb = 256;
     const unsigned blocks = (unsigned)((n + tpb - 1) / tpb);
     const int64_t n_tiles = (n + kScanTile - 1) / kScanTile;
     prepass_count_kernel<CsrSource><<<blocks, tpb, 0, s>>>(src, n, isa, strip ? 1 : 0, sc->eff_len,
-                                                           sc->counters + 1);
+                                                           sc->counters + 1, bad);
     scan_tile_sums_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(sc->eff_len, n, sc->tiles);
     scan_tile_offsets_kernel<<<1, kScanThreads, 0, s>>>(sc->tiles, n_tiles);
     scan_apply_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(sc->eff_len, n, sc->tiles, n_tiles, sc->eff_off);
     prepass_compact_kernel<CsrSource><<<blocks, tpb, 0, s>>>(src, n, isa, strip ? 1 : 0, sc->eff_off, sc->uops,
-                                                             nullptr, UopFormat{});
+                                                             nullptr, UopFormat{}, bad);
     const bool sched = n > 1;
     if (sched) {
-        order_hist_kernel<<<blocks, tpb, 0, s>>>(sc->eff_len, n, sc->hist);
-        order_scan_kernel<<<1, 1024, 0, s>>>(sc->hist);
-        order_scatter_kernel<<<blocks, tpb, 0, s>>>(sc->eff_len, n, sc->hist, sc->order);
+        order_hist_kernel<<<blocks, tpb, 0, s>>>(sc->eff_len, n, sc->hist, nullptr, 0);
+        order_scan_kernel<<<1, 1024, 0, s>>>(sc->hist, nullptr);
+        order_scatter_kernel<<<blocks, tpb, 0, s>>>(sc->eff_len, n, sc->hist, sc->order, nullptr, 0);
     }
     if (cudaGetLastError() != cudaSuccess) return GALOP_E_CUDA;
 
-    // Interpreter: same kernel selection and case chunking as the other entry points.
-    const void* fn = opt->num_registers == 8 ? interp_kernel_nr8(k, dispatch, opt->profile, opt->reduce, kModeFitness)
-                                             : interp_kernel_nr16(k, dispatch, opt->profile, opt->reduce, kModeFitness);
+    // Interpreter: the kernel selection and case chunking of the other
+    // entry points (enough work items for every resident warp, none longer
+    // than kMaxItemCases cases), within the scratch's partial sums.
+    const void* fn = opt->num_registers == 8
+                         ? interp_kernel_nr8(k, kNaDispatch, opt->profile, opt->reduce, kModeFitness)
+                         : interp_kernel_nr16(k, kNaDispatch, opt->profile, opt->reduce, kModeFitness);
     if (!fn) return GALOP_E_INVALID;
     const int threads = 32 * wpb;
-    const size_t smem = dispatch == 2 ? (size_t)(threads + 32) * opt->num_registers * k * sizeof(float) : 0;
-    if (smem) {
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-        if (e != cudaSuccess) { cudaGetLastError(); return GALOP_E_CUDA; }
-    }
+    const size_t smem = (size_t)(threads + 32) * opt->num_registers * k * sizeof(float);
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) { cudaGetLastError(); return GALOP_E_CUDA; }
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) {
         cudaGetLastError();
@@ -168,9 +216,11 @@ extern "C" int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32
     const int64_t pass = 32LL * k;
     const int64_t passes = std::max<int64_t>(1, (n_cases + pass - 1) / pass);
     int64_t n_chunks = 1;
-    if (opt->reduce != GALOP_REDUCE_ORDERED && n < 4 * resident_warps)
-        n_chunks = std::min<int64_t>(passes, (4 * resident_warps + n - 1) / n);
-    n_chunks = std::min<int64_t>(n_chunks, kNaMaxPartials / n);
+    if (opt->reduce != GALOP_REDUCE_ORDERED) {
+        if (n < 4 * resident_warps) n_chunks = std::min<int64_t>(passes, (4 * resident_warps + n - 1) / n);
+        n_chunks = std::max<int64_t>(n_chunks, std::min<int64_t>(passes, (n_cases + kMaxItemCases - 1) / kMaxItemCases));
+    }
+    n_chunks = std::max<int64_t>(1, std::min<int64_t>(n_chunks, kNaMaxPartials / n));
     const int64_t chunk_cases = ((passes + n_chunks - 1) / n_chunks) * pass;
     n_chunks = std::max<int64_t>(1, (std::max<int64_t>(n_cases, 1) + chunk_cases - 1) / chunk_cases);
 
@@ -202,6 +252,7 @@ extern "C" int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32
     if (n_chunks > 1)
         finalize_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(sc->partial, n, (int)n_chunks, n_cases,
                                                                   Objective{}, d_fitness, d_sse);
+    poison_results_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(bad, n, d_fitness, d_sse);
     if (cudaGetLastError() != cudaSuccess) return GALOP_E_CUDA;
     return GALOP_OK;
 }

@@ -45,13 +45,46 @@ constexpr int kScanItems = 4;                       // per thread
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kOrderBins = 4096;                    // lengths >= kOrderBins-1 share a bin
 
+// Device-side check of CSR offsets that a caller states for a
+// device-resident population, before anything reads the program words:
+// offsets[0] == 0, every program length in [0, 2^30], offsets[n] ==
+// total_words.  A violation sets *bad.  The count and compact kernels given
+// `bad` then treat every program as empty (no word is read, no micro-op
+// written), so no access leaves the buffers the caller stated, and
+// poison_results_kernel turns every fitness and SSE of the call into NaN.
+// One thread per offset: grid ceil((n + 1) / 256) x 256.
+static __global__ void check_offsets_kernel(const int64_t* __restrict__ off, int64_t n, int64_t total_words,
+                                            unsigned long long* __restrict__ bad) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    bool ok;
+    if (i == n) {
+        ok = off[n] == total_words;
+    } else {
+        const int64_t l = off[i + 1] - off[i];
+        ok = l >= 0 && l <= ((int64_t)1 << 30) && (i != 0 || off[0] == 0);
+    }
+    if (!ok) atomicOr(bad, 1ull);
+}
+
+static __global__ void poison_results_kernel(const unsigned long long* __restrict__ bad, int64_t n,
+                                             float* __restrict__ fitness, double* __restrict__ sse) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || *bad == 0ull) return;
+    fitness[i] = __int_as_float(0x7fc00000);
+    if (sse) sse[i] = __longlong_as_double(0x7ff8000000000000ll);
+}
+
 template <class Src>
 __global__ void prepass_count_kernel(Src src, int64_t n, IsaParams isa, int strip,
                                      int32_t* __restrict__ eff_len,
-                                     unsigned long long* __restrict__ totals) {
+                                     unsigned long long* __restrict__ totals,
+                                     const unsigned long long* __restrict__ bad) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t raw = 0, cnt = 0;
-    if (i < n) {
+    if (i < n && bad != nullptr && *bad != 0ull) {
+        eff_len[i] = 0;
+    } else if (i < n) {
         const int64_t s = src.start(i);
         raw = src.length(i);
         if (!strip) {
@@ -191,9 +224,10 @@ template <class Src>
 __global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int strip,
                                        const int64_t* __restrict__ eff_off,
                                        uint32_t* __restrict__ uops,
-                                       uint32_t* __restrict__ raw_out, UopFormat fmt) {
+                                       uint32_t* __restrict__ raw_out, UopFormat fmt,
+                                       const unsigned long long* __restrict__ bad) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (bad != nullptr && *bad != 0ull)) return;
     const int64_t s = src.start(i);
     const int64_t raw = src.length(i);
     const int64_t o = eff_off[i];
@@ -224,20 +258,40 @@ __global__ void prepass_compact_kernel(Src src, int64_t n, IsaParams isa, int st
 // Longest-first order: histogram of bins (bin 0 = longest), scan, scatter.
 // A negative length (a copy left out by dedup.cuh) goes to the last bin,
 // after every program that is interpreted.
-__device__ __forceinline__ int order_bin(int l) {
+//
+// With per-program live-in words (fold.cuh), programs are also grouped by
+// register-file class: those whose values fit in split_slots slots come
+// first (bins [0, kClassBins)), the others after them (bins [kClassBins,
+// 2 kClassBins)), each group longest first; the scan reports the size of
+// the first group, where the interpreter's launches split the order.
+constexpr int kClassBins = 2047;
+
+__device__ __forceinline__ int order_bin(int l, int cls) {
     if (l < 0) return kOrderBins - 1;
-    if (l > kOrderBins - 2) l = kOrderBins - 2;
-    return kOrderBins - 2 - l;
+    if (cls < 0) {
+        if (l > kOrderBins - 2) l = kOrderBins - 2;
+        return kOrderBins - 2 - l;
+    }
+    if (l > kClassBins - 1) l = kClassBins - 1;
+    return cls * kClassBins + (kClassBins - 1 - l);
+}
+
+__device__ __forceinline__ int order_class(const uint32_t* livein, int64_t i, int split_slots) {
+    if (livein == nullptr) return -1;
+    return (int)livein_slots(livein[i]) > split_slots ? 1 : 0;
 }
 
 static __global__ void order_hist_kernel(const int32_t* __restrict__ len, int64_t n,
-                                  unsigned int* __restrict__ hist) {
+                                  unsigned int* __restrict__ hist, const uint32_t* __restrict__ livein,
+                                  int split_slots) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    atomicAdd(&hist[order_bin(len[i])], 1u);
+    atomicAdd(&hist[order_bin(len[i], order_class(livein, i, split_slots))], 1u);
 }
 
-static __global__ void order_scan_kernel(unsigned int* __restrict__ hist) {
+// split_out (may be null): programs in bins below kClassBins (the first
+// register-file class).
+static __global__ void order_scan_kernel(unsigned int* __restrict__ hist, unsigned long long* __restrict__ split_out) {
     // Single block of 1024 threads, 4 bins per thread, exclusive in place.
     __shared__ unsigned int buf[1024];
     const int t = threadIdx.x;
@@ -254,15 +308,20 @@ static __global__ void order_scan_kernel(unsigned int* __restrict__ hist) {
     }
     unsigned int run = buf[t] - s;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) { hist[t * 4 + j] = run; run += v[j]; }
+    for (int j = 0; j < 4; ++j) {
+        if (split_out != nullptr && t * 4 + j == kClassBins) *split_out = run;
+        hist[t * 4 + j] = run;
+        run += v[j];
+    }
 }
 
 static __global__ void order_scatter_kernel(const int32_t* __restrict__ len, int64_t n,
                                      unsigned int* __restrict__ cursor,
-                                     int32_t* __restrict__ order) {
+                                     int32_t* __restrict__ order, const uint32_t* __restrict__ livein,
+                                     int split_slots) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const unsigned int pos = atomicAdd(&cursor[order_bin(len[i])], 1u);
+    const unsigned int pos = atomicAdd(&cursor[order_bin(len[i], order_class(livein, i, split_slots))], 1u);
     order[pos] = (int32_t)i;
 }
 

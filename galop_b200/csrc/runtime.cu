@@ -48,8 +48,7 @@ int pick_wpb(const galop_ctx* ctx) {
 }
 
 int pick_dispatch(const galop_ctx* ctx) {
-    const int d = ctx->opt.dispatch;
-    return (d >= 0 && d <= 3) ? d : 3;
+    return ctx->opt.dispatch == 2 ? 2 : 3;
 }
 
 // Micro-op form the pre-pass writes for the chosen interpreter.
@@ -67,8 +66,7 @@ size_t interp_smem_bytes(const galop_ctx* ctx, int k, int wpb) {
     if (d == 3) return wide_smem_bytes(ctx->isa.num_registers, k, wpb);
     // Register file of every lane plus one block-shared copy of the constant
     // pool laid out the same way.
-    if (d == 2) return (size_t)(32 * wpb + 32) * ctx->isa.num_registers * k * sizeof(float);
-    return 0;
+    return (size_t)(32 * wpb + 32) * ctx->isa.num_registers * k * sizeof(float);
 }
 
 const void* kernel_for(const galop_ctx* ctx, int k, int mode) {
@@ -90,9 +88,16 @@ float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 }
 
 // Pre-pass over `src` into ctx->uops / eff_off (and order when sched).
+//
+// `bad` (device, may be null): the flag check_offsets_kernel sets for
+// caller-stated device offsets that are inconsistent; when it is set the
+// count and compact kernels treat every program as empty.  With `bad`, the
+// micro-op buffer is sized for raw_words_total instructions (the effective
+// total is not known on the host without waiting for the device).
 template <class Src>
 int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_total,
-                bool strip, bool sched, uint32_t* raw_out, bool reset_totals = true, bool fitness_mode = false) {
+                bool strip, bool sched, uint32_t* raw_out, bool reset_totals = true, bool fitness_mode = false,
+                const unsigned long long* bad = nullptr) {
     cudaStream_t s = ctx->stream;
     GALOP_CK(ctx->eff_len.ensure((size_t)std::max<int64_t>(n, 1)), "alloc eff_len");
     GALOP_CK(ctx->livein.ensure((size_t)std::max<int64_t>(n, 1)), "alloc livein");
@@ -101,10 +106,11 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
     GALOP_CK(ctx->tiles.ensure((size_t)n_tiles + 1), "alloc scan tiles");
     // counters: [0] work queue, [1] raw, [2] effective, [3] interpreted
     // instructions, [4] copies left out by dedup (this pre-pass), [5] their
-    // interpreted instructions
-    GALOP_CK(ctx->counters.ensure(6), "alloc counters");
+    // interpreted instructions, [6] bad device offsets (check_offsets_kernel),
+    // [7] register-file class split (order_scan_kernel)
+    GALOP_CK(ctx->counters.ensure(kCounters), "alloc counters");
     if (reset_totals)
-        GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 6 * sizeof(unsigned long long), s), "memset");
+        GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, kCounters * sizeof(unsigned long long), s), "memset");
     else
         GALOP_CK(cudaMemsetAsync(ctx->counters.p + 4, 0, sizeof(unsigned long long), s), "memset");
 
@@ -112,7 +118,7 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
     const unsigned blocks = (unsigned)((n + tpb - 1) / tpb);
     if (n > 0) {
         prepass_count_kernel<Src><<<blocks, tpb, 0, s>>>(src, n, ctx->isa, strip ? 1 : 0,
-                                                         ctx->eff_len.p, ctx->counters.p + 1);
+                                                         ctx->eff_len.p, ctx->counters.p + 1, bad);
         scan_tile_sums_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(ctx->eff_len.p, n, ctx->tiles.p);
         scan_tile_offsets_kernel<<<1, kScanThreads, 0, s>>>(ctx->tiles.p, n_tiles);
         scan_apply_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(ctx->eff_len.p, n, ctx->tiles.p,
@@ -129,17 +135,29 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
     const UopFormat fmt = uop_format(ctx);
     const size_t per = fmt.wide ? 4 : 1;
     if (ctx->uops.cap < (size_t)std::max<int64_t>(raw_words_total, 1) * per) {
-        int64_t eff_total = raw_words_total;
-        if (strip && n > 0) {
+        bool exact = strip && n > 0 && bad == nullptr;
+        if (!exact) {
+            // Sized for the raw total without waiting; only when that does
+            // not fit is the effective total read back after all.
+            const cudaError_t e = ctx->uops.ensure((size_t)std::max<int64_t>(raw_words_total, 1) * per);
+            if (e == cudaErrorMemoryAllocation && strip && n > 0) {
+                cudaGetLastError();
+                exact = true;
+            } else {
+                GALOP_CK(e, "alloc uops");
+            }
+        }
+        if (exact) {
+            int64_t eff_total = raw_words_total;
             GALOP_CK(cudaMemcpyAsync(&eff_total, ctx->eff_off.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s),
                      "D2H effective total");
             GALOP_CK(cudaStreamSynchronize(s), "effective total");
+            GALOP_CK(ctx->uops.ensure((size_t)std::max<int64_t>(eff_total, 1) * per), "alloc uops");
         }
-        GALOP_CK(ctx->uops.ensure((size_t)std::max<int64_t>(eff_total, 1) * per), "alloc uops");
     }
     if (n > 0) {
         prepass_compact_kernel<Src><<<blocks, tpb, 0, s>>>(src, n, ctx->isa, strip ? 1 : 0,
-                                                           ctx->eff_off.p, ctx->uops.p, raw_out, fmt);
+                                                           ctx->eff_off.p, ctx->uops.p, raw_out, fmt, bad);
         ctx->launches += 1;
     }
     // Constant folding (wide micro-ops of effective code only; the raw-word
@@ -191,9 +209,9 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
         GALOP_CK(ctx->order.ensure((size_t)n), "alloc order");
         GALOP_CK(ctx->hist.ensure(kOrderBins), "alloc hist");
         GALOP_CK(cudaMemsetAsync(ctx->hist.p, 0, kOrderBins * sizeof(unsigned int), s), "memset hist");
-        order_hist_kernel<<<blocks, tpb, 0, s>>>(ctx->eff_len.p, n, ctx->hist.p);
-        order_scan_kernel<<<1, 1024, 0, s>>>(ctx->hist.p);
-        order_scatter_kernel<<<blocks, tpb, 0, s>>>(ctx->eff_len.p, n, ctx->hist.p, ctx->order.p);
+        order_hist_kernel<<<blocks, tpb, 0, s>>>(ctx->eff_len.p, n, ctx->hist.p, nullptr, 0);
+        order_scan_kernel<<<1, 1024, 0, s>>>(ctx->hist.p, nullptr);
+        order_scatter_kernel<<<blocks, tpb, 0, s>>>(ctx->eff_len.p, n, ctx->hist.p, ctx->order.p, nullptr, 0);
         ctx->launches += 3;
         GALOP_CK(cudaGetLastError(), "order launch");
     }
@@ -328,7 +346,7 @@ int finish_stats(galop_ctx* ctx) {
     st.finalize_ms = ev_ms(ctx->ev[kEvInterp], ctx->ev[kEvFinalize]);
     st.d2h_ms = ev_ms(ctx->ev[kEvFinalize], ctx->ev[kEvD2H]);
     st.total_ms = ev_ms(ctx->ev[kEvStart], ctx->ev[kEvD2H]);
-    unsigned long long tot[5] = {0, 0, 0, 0, 0};
+    unsigned long long tot[kCounters - 1] = {};
     if (ctx->counters.p)
         GALOP_CK(cudaMemcpy(tot, ctx->counters.p + 1, sizeof tot, cudaMemcpyDeviceToHost), "stats D2H");
     st.raw_instructions = (int64_t)tot[0];
@@ -336,6 +354,10 @@ int finish_stats(galop_ctx* ctx) {
     st.interp_instructions = ctx->folded ? (int64_t)(tot[2] - tot[4]) : (int64_t)tot[1];
     st.kernels_launched = ctx->launches;
     ctx->stats_pending = false;
+    if (tot[kCounterBadOffsets - 1])
+        return ctx->fail(GALOP_E_INVALID, "device offsets disagree with total_words (offsets[0] != 0, a "
+                                          "decreasing offset or a program over 2^30 words, or offsets[n] != "
+                                          "total_words): nothing was read, every fitness is NaN");
     return GALOP_OK;
 }
 
@@ -446,6 +468,7 @@ int galop_create(const galop_options* opt, galop_ctx** out) {
     if (opt->profile != GALOP_PROFILE_REF && opt->profile != GALOP_PROFILE_BJ) return GALOP_E_INVALID;
     if (opt->reduce < GALOP_REDUCE_KAHAN32 || opt->reduce > GALOP_REDUCE_ORDERED) return GALOP_E_INVALID;
     if (opt->objective != GALOP_OBJECTIVE_MSE && opt->objective != GALOP_OBJECTIVE_R2) return GALOP_E_INVALID;
+    if (opt->dispatch != 2 && opt->dispatch != 3) return GALOP_E_INVALID;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -473,7 +496,7 @@ int galop_create(const galop_options* opt, galop_ctx** out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     for (int i = 0; e == cudaSuccess && i < kEvCount; ++i) e = cudaEventCreate(&ctx->ev[i]);
     for (int i = 0; e == cudaSuccess && i < 8; ++i) e = cudaEventCreate(&ctx->timers[i]);
-    if (e == cudaSuccess) e = ctx->counters.ensure(6);
+    if (e == cudaSuccess) e = ctx->counters.ensure(kCounters);
     if (e != cudaSuccess) {
         galop_destroy(ctx);
         return e == cudaErrorMemoryAllocation ? GALOP_E_NOMEM : GALOP_E_CUDA;
@@ -729,8 +752,8 @@ static int evaluate_csr_segmented(galop_ctx* ctx, const uint32_t* words, const i
         cudaStreamSynchronize(cs);   // the copies read the caller's buffers
         return rc;
     }
-    GALOP_CK(ctx->counters.ensure(6), "alloc counters");
-    GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, 6 * sizeof(unsigned long long), s), "memset");
+    GALOP_CK(ctx->counters.ensure(kCounters), "alloc counters");
+    GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, kCounters * sizeof(unsigned long long), s), "memset");
     for (int k = 0; k < segs; ++k) {
         const int64_t nk = b[k + 1] - b[k];
         GALOP_CK(cudaStreamWaitEvent(s, ctx->seg_ev[5 * k], 0), "stream wait");
@@ -822,11 +845,13 @@ int galop_evaluate_population(galop_ctx* ctx, const uint32_t* instructions, cons
 }
 
 int galop_evaluate_csr_device(galop_ctx* ctx, const uint32_t* d_words, const int64_t* d_offsets,
-                              int64_t n_programs, float* d_fitness, double* d_sse, void* stream) {
+                              int64_t n_programs, int64_t total_words, float* d_fitness, double* d_sse,
+                              void* stream) {
     if (int rc = check_ready(ctx)) return rc;
-    if (n_programs < 0 || !d_offsets) return ctx->fail(GALOP_E_INVALID, "bad arguments");
+    if (n_programs < 0 || total_words < 0 || !d_offsets) return ctx->fail(GALOP_E_INVALID, "bad arguments");
     if (n_programs > INT32_MAX) return ctx->fail(GALOP_E_CAPACITY, "n_programs > 2^31-1");
-    if (n_programs > 0 && (!d_words || !d_fitness)) return ctx->fail(GALOP_E_INVALID, "null pointer");
+    if (n_programs > 0 && (!d_fitness || (!d_words && total_words > 0)))
+        return ctx->fail(GALOP_E_INVALID, "null pointer");
     GALOP_CK(cudaSetDevice(ctx->device), "set device");
     begin_call(ctx, n_programs);
     cudaStream_t user = (cudaStream_t)stream;
@@ -837,14 +862,19 @@ int galop_evaluate_csr_device(galop_ctx* ctx, const uint32_t* d_words, const int
     } else {
         GALOP_CK(cudaEventRecord(ctx->ev[kEvStart], s), "event");
     }
-    // Total words from the device offsets (one 8-byte read).
-    int64_t total = 0;
-    GALOP_CK(cudaMemcpyAsync(&total, d_offsets + n_programs, sizeof(int64_t), cudaMemcpyDeviceToHost, s),
-             "read total");
-    GALOP_CK(cudaStreamSynchronize(s), "read total");
+    // The caller's offsets are checked on the device against total_words
+    // before any word is read (prepass.cuh); nothing waits for the device.
+    GALOP_CK(ctx->counters.ensure(kCounters), "alloc counters");
+    GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, kCounters * sizeof(unsigned long long), s), "memset");
+    unsigned long long* bad = ctx->counters.p + kCounterBadOffsets;
+    check_offsets_kernel<<<(unsigned)((n_programs + 256) / 256), 256, 0, s>>>(d_offsets, n_programs, total_words,
+                                                                            bad);
+    ctx->launches += 1;
+    GALOP_CK(cudaGetLastError(), "offset check launch");
     GALOP_CK(cudaEventRecord(ctx->ev[kEvH2D], s), "event");
     CsrSource src{d_words, d_offsets};
-    if (int rc = run_prepass(ctx, src, n_programs, total, ctx->opt.intron_prepass != 0, true, nullptr, true, true))
+    if (int rc = run_prepass(ctx, src, n_programs, total_words, ctx->opt.intron_prepass != 0, true, nullptr, false,
+                             true, bad))
         return rc;
     GALOP_CK(cudaEventRecord(ctx->ev[kEvPrepass], s), "event");
     int32_t chunks = 1;
@@ -852,6 +882,11 @@ int galop_evaluate_csr_device(galop_ctx* ctx, const uint32_t* d_words, const int
         return rc;
     GALOP_CK(cudaEventRecord(ctx->ev[kEvInterp], s), "event");
     if (int rc = finalize(ctx, n_programs, chunks, d_fitness, d_sse)) return rc;
+    if (n_programs > 0) {
+        poison_results_kernel<<<(unsigned)((n_programs + 255) / 256), 256, 0, s>>>(bad, n_programs, d_fitness, d_sse);
+        ctx->launches += 1;
+        GALOP_CK(cudaGetLastError(), "result check launch");
+    }
     GALOP_CK(cudaEventRecord(ctx->ev[kEvFinalize], s), "event");
     GALOP_CK(cudaEventRecord(ctx->ev[kEvD2H], s), "event");
     if (user && user != s) GALOP_CK(cudaStreamWaitEvent(user, ctx->ev[kEvD2H], 0), "stream wait");

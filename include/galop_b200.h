@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define GALOP_ABI_VERSION 1
+#define GALOP_ABI_VERSION 2
 
 typedef enum {
     GALOP_OK            = 0,
@@ -91,11 +91,12 @@ typedef struct {
     int32_t cases_per_lane;   /* 0 = tuned default; else 1, 2, 4 or 8          */
     int32_t warps_per_block;  /* 0 = tuned default; else 1..8                  */
     int32_t dispatch;         /* interpreter: 3 = shared-memory register file,
-                                 16-byte pre-decoded micro-ops (default);
+                                 16-byte pre-decoded micro-ops, constant
+                                 folding, operand forwarding (default);
                                  2 = shared-memory register file, 32-bit
-                                 micro-ops; 1 = lane registers behind PTX
-                                 jump tables; 0 = lane registers behind C++
-                                 switches.  All give identical results.     */
+                                 micro-ops, one instruction at a time.
+                                 Both give identical results; any other
+                                 value is GALOP_E_INVALID.                  */
     int32_t objective;        /* galop_objective (default MSE)                  */
     int32_t dedup;            /* 1: programs whose interpreted code is identical
                                  are interpreted once and share the fitness
@@ -302,11 +303,20 @@ GALOP_API int galop_evaluate_population(galop_ctx* ctx, const uint32_t* instruct
 GALOP_API int galop_evaluate_csr(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets,
                        int64_t n_programs, float* fitness_out, double* sse_out);
 
-/* Device-resident form: all pointers are device memory on the context's
- * device; work is ordered on `stream` (a cudaStream_t, or NULL for the
- * context's own stream) and the call returns without synchronizing. */
+/* Device-resident form of galop_evaluate_csr: all pointers are device memory
+ * on the context's device, total_words = d_offsets[n_programs] as the caller
+ * knows it (the size of d_words).  Work is ordered on `stream` (a
+ * cudaStream_t, or NULL for the context's own stream) and the call returns
+ * without waiting for the device; it only blocks when a working buffer must
+ * grow (the first call, or a larger population).  The offsets are checked on
+ * the device before any word is read: if d_offsets[0] != 0, an offset
+ * decreases, a program is longer than 2^30 words, or d_offsets[n_programs]
+ * != total_words, no word is read, every d_fitness (and d_sse) is NaN, and
+ * galop_last_stats returns GALOP_E_INVALID for the call.  Its result is read
+ * once the stream has reached it (galop_last_stats waits for that). */
 GALOP_API int galop_evaluate_csr_device(galop_ctx* ctx, const uint32_t* d_words, const int64_t* d_offsets,
-                              int64_t n_programs, float* d_fitness, double* d_sse, void* stream);
+                              int64_t n_programs, int64_t total_words, float* d_fitness, double* d_sse,
+                              void* stream);
 
 /* Per-case outputs r[OUTPUT_REG] (src/Interpreter.cpp:54-57), host pointers:
  * outputs[i*n_cases + c] for program i, case c. */
@@ -327,7 +337,8 @@ GALOP_API int galop_effective_csr(galop_ctx* ctx, const uint32_t* words, const i
                         int64_t n_programs, int64_t* eff_len, uint32_t* eff_words);
 
 /* Stats of the most recent evaluate call; after galop_evaluate_csr_device
- * this waits for that call's work to finish. */
+ * this waits for that call's work to finish, and returns GALOP_E_INVALID if
+ * the device found its offsets inconsistent. */
 GALOP_API int galop_last_stats(galop_ctx* ctx, galop_stats* out);
 
 /* Blocks until the context's stream is idle. */
@@ -481,28 +492,38 @@ GALOP_API int galop_server_stats(galop_server* sv, galop_server_totals* out);
 #define GALOP_NOALLOC_MAX_WORDS 2097152
 
 /* No counterpart in the reference.  For callers that cannot let a library
- * call cudaMalloc: code that evaluates while a stream is being captured
- * (cudaMalloc and cudaFree are not allowed there and would synchronise the
- * device), and hosts that hand the library a fixed device-memory budget and
- * cannot afford an out-of-memory failure in the middle of a run.  It needs no
+ * call cudaMalloc: hosts that own all device memory through their own pool
+ * allocator (a framework's caching allocator, a server with a fixed budget
+ * per model) and must never meet an out-of-memory failure or unaccounted
+ * memory in the middle of a run, and loops that must not stall, since
+ * cudaMalloc and cudaFree can synchronise the whole device.  It needs no
  * galop_ctx and allocates nothing -- no cudaMalloc, no cudaFree, no
  * allocating library routine; its scratch is the static array above.
  *
- * Same evaluation as galop_evaluate_csr_device: device pointers, CSR programs
- * (words, int64 offsets starting at 0, total_words = offsets[n_programs]), the
- * dataset already feature-major on the device -- d_inputs[f*padded_cases + c],
- * d_targets[c], padded_cases a multiple of 1024 and >= n_cases (padding values
- * are never counted) -- opt as for galop_create (device ignored: the current
- * device is used).  Work is queued on `stream` (NULL = default stream) and the
- * call returns without waiting.
+ * Same evaluation as galop_evaluate_csr_device, with the compact
+ * interpreter (dispatch 2; results are identical): device pointers, CSR
+ * programs (words, int64 offsets, total_words = offsets[n_programs]), the
+ * dataset already feature-major on the device -- d_inputs[f*padded_cases +
+ * c], d_targets[c], padded_cases a multiple of 1024 and >= n_cases (padding
+ * values are never counted) -- opt as for galop_create (device and dispatch
+ * ignored: the current device is used).  Work is queued on `stream` (NULL =
+ * default stream) and the call returns without waiting.
  *
  * Limits: n_programs <= GALOP_NOALLOC_MAX_PROGRAMS and total_words <=
- * GALOP_NOALLOC_MAX_WORDS, else GALOP_E_CAPACITY with nothing queued.
- * The first call on a device looks up the scratch's device address (and
- * loads this library's code on that device); make that first call before any
- * stream capture.  Every call uses the same scratch: calls whose work
- * overlaps on the GPU (different streams, or different host threads, without
- * ordering between them) race and corrupt each other's results. */
+ * GALOP_NOALLOC_MAX_WORDS, else GALOP_E_CAPACITY with nothing queued.  The
+ * offsets are checked on the device before any word is read: if offsets[0]
+ * != 0, an offset decreases or offsets[n_programs] != total_words, nothing
+ * beyond the stated sizes is read or written and every fitness (and SSE)
+ * is NaN.  A CUDA error left pending by an earlier call of the caller is
+ * not cleared: the call returns GALOP_E_CUDA and queues nothing.
+ *
+ * The first call on a device, with that device current, looks up the
+ * scratch's device address and loads this entry point's kernels on that
+ * device; make that first call before any stream capture.  Every call uses
+ * the same scratch, which keeps the last call's contents (each call clears
+ * what must start at zero): calls whose work overlaps on the GPU
+ * (different streams, or different host threads, without ordering between
+ * them) race and corrupt each other's results. */
 GALOP_API int galop_evaluate_csr_noalloc(const galop_options* opt, const uint32_t* d_words,
                                          const int64_t* d_offsets, int64_t n_programs,
                                          int64_t total_words, const float* d_inputs,

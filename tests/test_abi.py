@@ -62,7 +62,7 @@ def test_options_defaults_and_status_strings(native):
     assert native.galop_options_init(C.byref(o)) == 0
     assert (o.profile, o.num_registers, o.input_protect, o.reduce, o.device, o.intron_prepass) == \
         (g.PROFILE_REF, 8, 0, g.REDUCE_KAHAN32, 0, 1)
-    assert native.galop_abi_version() == 1
+    assert native.galop_abi_version() == 2
     for code in (0, -1, -2, -3, -4, -5, -6, -7, -8):
         assert native.galop_status_string(code)
     assert native.galop_options_init(None) == g.E_INVALID

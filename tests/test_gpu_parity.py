@@ -525,7 +525,7 @@ def test_large_host_call_in_segments_matches_device_call(native, reduce):
         try:
             ev.h2d(dw, words)
             ev.h2d(do, off)
-            ev.evaluate_csr_device(dw, do, len(lens), df)
+            ev.evaluate_csr_device(dw, do, len(lens), int(off[-1]), df)
             ev.synchronize()
             dev = np.empty(len(lens), np.float32)
             ev.d2h(dev, df)
