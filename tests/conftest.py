@@ -19,6 +19,21 @@ if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
 
+def reference_root():
+    """The reference checkout: $REF, else the path oracle/Makefile built the
+    checkers from (oracle/_ref/ref_path.txt); None when neither exists (the
+    tests that compile against the reference's sources then skip)."""
+    import os
+    cands = [os.environ.get("REF")]
+    rec = ROOT / "oracle" / "_ref" / "ref_path.txt"
+    if rec.exists():
+        cands.append(rec.read_text().strip())
+    for c in cands:
+        if c and (Path(c) / "src" / "EvalBackend.h").exists():
+            return Path(c)
+    return None
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: runs the CUDA path on a B200 (through the C ABI)")
 

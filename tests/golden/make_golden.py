@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures in tests/golden/ from the reference itself.
 
-Runs in a checkout that has the reference sources (REF, default
-/root/reference): builds oracle/_ref/ with ``make -C oracle`` (the reference's
+Runs in a checkout that has the reference sources (the REF environment
+variable names the checkout): builds oracle/_ref/ with ``make -C oracle`` (the reference's
 own src/*.cpp compiled where they lie) and records what the REFERENCE CODE
 computes:
 
@@ -26,6 +26,7 @@ import hashlib
 import os
 import subprocess
 import sys
+import tempfile
 from pathlib import Path
 
 import numpy as np
@@ -35,7 +36,9 @@ sys.path.insert(0, str(ROOT))
 from oracle.oracle import RefLib  # noqa: E402
 from galop_b200 import workloads as W  # noqa: E402
 
-REF = Path(os.environ.get("REF", "/root/reference"))
+if "REF" not in os.environ:
+    sys.exit("set REF to the reference checkout (the directory holding src/ and golden/)")
+REF = Path(os.environ["REF"])
 OUT = Path(__file__).resolve().parent
 
 
@@ -63,8 +66,7 @@ def datasets():
 def histories():
     h = OUT / "histories"
     h.mkdir(exist_ok=True)
-    tmp = ROOT / "_work" / "golden_regen"
-    tmp.mkdir(parents=True, exist_ok=True)
+    tmp = Path(tempfile.mkdtemp(prefix="golden_regen_"))
     exe = ROOT / "oracle" / "_ref" / "lgp_run_cpu"
     procs = []
     env = dict(os.environ, OMP_NUM_THREADS="1")

@@ -11,7 +11,7 @@ import sys
 
 import pytest
 
-from conftest import ROOT
+from conftest import ROOT, reference_root
 
 HEADER = ROOT / "include" / "galop_b200.h"
 
@@ -45,7 +45,7 @@ def test_header_compiles_as_c_and_cpp(tmp_path):
                     f"-I{ROOT / 'include'}", str(src)], check=True)
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/src/EvalBackend.h"),
+@pytest.mark.skipif(reference_root() is None,
                     reason="the EvalBackend adapter compiles inside the reference's build")
 def test_backend_adapter_compiles_against_reference_interface(tmp_path):
     src = tmp_path / "t.cpp"
@@ -53,7 +53,7 @@ def test_backend_adapter_compiles_against_reference_interface(tmp_path):
                    "int main(){ EvalBackend* b = nullptr; (void)b; "
                    "galop_options o = galop::B200Evaluator::options_from_config(); return o.num_registers; }\n")
     subprocess.run(["g++", "-std=c++20", "-fsyntax-only", f"-I{ROOT / 'include'}",
-                    "-I/root/reference/src", str(src)], check=True)
+                    f"-I{reference_root() / 'src'}", str(src)], check=True)
 
 
 def test_options_defaults_and_status_strings(native):

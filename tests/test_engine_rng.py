@@ -10,11 +10,13 @@ from pathlib import Path
 
 import pytest
 
-ROOT = Path(__file__).resolve().parents[1]
-REF_SRC = Path("/root/reference/src")
+from conftest import ROOT, reference_root
+
+REF = reference_root()
+REF_SRC = REF / "src" if REF else None
 
 
-@pytest.mark.skipif(not (REF_SRC / "LGPEngine.h").exists() or shutil.which("g++") is None,
+@pytest.mark.skipif(REF_SRC is None or shutil.which("g++") is None,
                     reason="needs the reference's sources and g++")
 def test_engine_streams_match_reference_and_libstdcxx(tmp_path):
     exe = tmp_path / "engine_rng_check"

@@ -26,7 +26,7 @@ def _worker(rank, world, port, out_path):
     sys.path.insert(0, str(ROOT))
     import torch.distributed as dist
     from galop_b200 import workloads as W
-    from galop_b200.sharding import evaluate_sharded
+    from sharding import evaluate_sharded
     from oracle.oracle import Oracle
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -44,7 +44,7 @@ def _worker(rank, world, port, out_path):
 
 
 def test_shard_bounds_cover_everything():
-    from galop_b200.sharding import shard_bounds
+    from sharding import shard_bounds
     for n in (0, 1, 7, 1000, 1023):
         for world in (1, 2, 3, 8):
             b = [shard_bounds(n, r, world) for r in range(world)]
