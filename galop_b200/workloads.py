@@ -72,7 +72,15 @@ def mask_random_words(raw: np.ndarray, num_registers: int) -> np.ndarray:
 
 
 def random_words(rng: np.random.Generator, n: int, num_registers: int) -> np.ndarray:
-    return mask_random_words(rng.integers(0, 2**32, size=n, dtype=np.uint64).astype(np.uint32), num_registers)
+    if n < (1 << 24):
+        return mask_random_words(rng.integers(0, 2**32, size=n, dtype=np.uint64).astype(np.uint32), num_registers)
+    # large populations: 32-bit draws in chunks, masked in place (bounded memory)
+    out = np.empty(n, dtype=np.uint32)
+    step = 1 << 26
+    for i in range(0, n, step):
+        m = min(step, n - i)
+        out[i:i + m] = mask_random_words(rng.integers(0, 2**32, size=m, dtype=np.uint32), num_registers)
+    return out
 
 
 def csr_offsets(lengths: np.ndarray) -> np.ndarray:
@@ -292,36 +300,47 @@ class Workload:
 
 def single_generation(seed: int = 2, n_programs: int = 1 << 20, n_cases: int = 4096, len_lo: int = 16,
                       len_hi: int = 256, eff_frac: float = 0.6, num_inputs: int = 5, x_lo: float = -3.0,
-                      x_hi: float = 3.0, target_eff: int = 16, noise: float = 0.01) -> Workload:
+                      x_hi: float = 3.0, target_eff: int = 16, noise: float = 0.01, ops=None) -> Workload:
     """One generation: 2^20 random programs, lengths U[16,256] with ~40%
     introns by construction, 5 features U[-3,3], 4096 cases, target = a
     random 16-effective-instruction program + N(0, 0.01^2).  REF ISA with 16
-    registers (5 inputs + 11 scratch) and the reference's 16-entry pool."""
+    registers (5 inputs + 11 scratch) and the reference's 16-entry pool.
+    ``ops`` restricts the opcodes of the population (not of the target)."""
     rng = np.random.default_rng(seed)
     isa = IsaSpec(PROFILE_REF, 16)
     X = rng.uniform(x_lo, x_hi, size=(n_cases, num_inputs)).astype(np.float32)
     y, tp = regression_target(rng, X, isa, target_eff, noise)
     lens = uniform_lengths(rng, n_programs, len_lo, len_hi)
-    words, off = structured_population(rng, lens, isa, eff_frac)
+    words, off = structured_population(rng, lens, isa, eff_frac, ops=ops)
     return Workload("single_generation", isa, words, off, X, y, tp,
                     f"{n_programs} programs, L~U[{len_lo},{len_hi}], {eff_frac:.0%} effective, "
                     f"{num_inputs} features U[{x_lo},{x_hi}], {n_cases} cases")
 
 
 def hbm_streaming(seed: int = 3, n_programs: int = 1 << 22, n_cases: int = 1 << 20, len_lo: int = 32,
-                  len_hi: int = 1024, num_inputs: int = 8, target_eff: int = 24) -> Workload:
+                  len_hi: int = 1024, num_inputs: int = 8, target_eff: int = 24,
+                  prefix_programs: Optional[int] = None) -> Workload:
     """2^22 programs, lengths log-uniform [32,1024] (uniform random words, so
-    the intron fraction is whatever random code has), 8 features U[-1,1],
-    2^20 cases, target = random 24-effective-instruction program."""
+    the intron fraction is whatever random code has, ~90%), 8 features
+    U[-1,1], 2^20 cases, target = random 24-effective-instruction program.
+    Words are drawn as 32-bit values in order, so ``prefix_programs`` = m
+    materialises exactly the first m programs of the full population."""
     rng = np.random.default_rng(seed)
     isa = IsaSpec(PROFILE_REF, 16)
     X = rng.uniform(-1.0, 1.0, size=(n_cases, num_inputs)).astype(np.float32)
     y, tp = regression_target(rng, X, isa, target_eff)
     lens = log_uniform_lengths(rng, n_programs, len_lo, len_hi)
-    words, off = random_population(rng, lens, isa.num_registers)
+    m = n_programs if prefix_programs is None else min(prefix_programs, n_programs)
+    off = csr_offsets(lens[:m])
+    n_words = int(off[-1])
+    words = np.empty(n_words, dtype=np.uint32)
+    step = 1 << 26
+    for i in range(0, n_words, step):
+        k = min(step, n_words - i)
+        words[i:i + k] = mask_random_words(rng.integers(0, 2**32, size=k, dtype=np.uint32), isa.num_registers)
     return Workload("hbm_streaming", isa, words, off, X, y, tp,
                     f"{n_programs} programs, L log-uniform [{len_lo},{len_hi}], {num_inputs} features, "
-                    f"{n_cases} cases")
+                    f"{n_cases} cases" + (f" (first {m} materialised)" if m < n_programs else ""))
 
 
 def plain_cpu(seed: int = 0, n_programs: int = 1000, n_cases: int = 64) -> Workload:

@@ -60,6 +60,8 @@ typedef struct {
     uint8_t op, dest, src1, src2, is_const, unary;
 } orc_ins_t;
 
+int64_t orc_extract_effective(const orc_isa_t* isa, const uint32_t* prog, int64_t len, uint32_t* out);
+
 /* Output register: r0, or the first scratch register NR/2 under
  * INPUT_PROTECT (src/LGPConfig.h:294-300). */
 int orc_output_reg(const orc_isa_t* isa) {
@@ -107,6 +109,11 @@ float orc_apply_op(int profile, int op, float a, float b) {
             if (profile == ORC_PROFILE_BJ) return (b != 0.0f) ? logf(fabsf(b)) : 0.0f;
             return (a > b) ? 1.0f : 0.0f;
     }
+}
+
+/* apply_op over n operand pairs (replaying long register traces). */
+void orc_apply_op_n(int profile, int op, const float* a, const float* b, int64_t n, float* out) {
+    for (int64_t i = 0; i < n; ++i) out[i] = orc_apply_op(profile, op, a[i], b[i]);
 }
 
 /* The same op semantics in double precision: the precision-stability probe
@@ -305,6 +312,68 @@ void orc_evaluate_population_csr(const orc_isa_t* isa, const uint32_t* words,
     (void)threads;
 }
 
+/* Per-case outputs of CSR programs: out[i*n_cases + c] = r[OUTPUT_REG] of
+ * program i on case c (src/Interpreter.cpp:36-59, one program after the
+ * other as src/EvaluatorCpu.cpp:7-15 walks them; OpenMP over programs, so
+ * results do not depend on the thread count).  effective_only != 0 runs
+ * each program's effective instructions only (src/Introns.h:50-57), whose
+ * outputs the reference's own intron test proves bit-identical to the full
+ * program's (tests/test_bed.cpp:1355-1381); it makes large case counts
+ * affordable. */
+void orc_case_outputs_csr(const orc_isa_t* isa, const uint32_t* words, const int64_t* offsets,
+                          int64_t n_programs, const float* inputs, int num_inputs, int64_t n_cases,
+                          float* out, int threads, int effective_only) {
+#ifdef _OPENMP
+    if (threads < 1) threads = omp_get_max_threads();
+    #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+#endif
+    for (int64_t i = 0; i < n_programs; ++i) {
+        const uint32_t* prog = words + offsets[i];
+        int64_t len = offsets[i + 1] - offsets[i];
+        uint32_t* eff = NULL;
+        if (effective_only) {
+            eff = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(len > 0 ? len : 1));
+            len = orc_extract_effective(isa, prog, len, eff);
+            prog = eff;
+        }
+        orc_ins_t* p = orc_decode_program(isa, prog, len);
+        float* o = out + i * n_cases;
+        for (int64_t c = 0; c < n_cases; ++c)
+            o[c] = orc_run_case(isa, p, len, inputs + c * num_inputs, num_inputs);
+        free(p);
+        free(eff);
+    }
+    (void)threads;
+}
+
+/* Fitness and double SSE of CSR programs as orc_evaluate_population_csr,
+ * with the effective-instructions-only option of orc_case_outputs_csr. */
+void orc_evaluate_population_csr_opt(const orc_isa_t* isa, const uint32_t* words,
+                                     const int64_t* offsets, int64_t n_programs,
+                                     const float* inputs, const float* targets, int num_inputs,
+                                     int64_t n_cases, float* fitness_out, double* sse_out,
+                                     int threads, int effective_only) {
+#ifdef _OPENMP
+    if (threads < 1) threads = omp_get_max_threads();
+    #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+#endif
+    for (int64_t i = 0; i < n_programs; ++i) {
+        const uint32_t* prog = words + offsets[i];
+        int64_t len = offsets[i + 1] - offsets[i];
+        uint32_t* eff = NULL;
+        if (effective_only) {
+            eff = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(len > 0 ? len : 1));
+            len = orc_extract_effective(isa, prog, len, eff);
+            prog = eff;
+        }
+        const double sse = orc_sse(isa, prog, len, inputs, targets, num_inputs, n_cases);
+        if (sse_out) sse_out[i] = sse;
+        fitness_out[i] = orc_mse_to_fitness((float)(sse / (double)n_cases));
+        free(eff);
+    }
+    (void)threads;
+}
+
 /* Dense layout of the EvalBackend boundary (src/EvalBackend.h:11-17):
  * program i at instructions + i*stride, lengths[i] instructions. */
 void orc_evaluate_population_dense(const orc_isa_t* isa, const uint32_t* instructions,
@@ -361,6 +430,24 @@ void orc_effective_lengths_csr(const orc_isa_t* isa, const uint32_t* words,
         eff_len[i] = orc_effective_mask(isa, words + offsets[i], len, mask);
         free(mask);
     }
+}
+
+/* Host intron strip of a CSR population into CSR effective code (the
+ * reference's PackedEffective layout, src/EvaluatorCuda.cu:374-422):
+ * eff_offsets[n+1] must hold the exclusive scan of the effective lengths
+ * (orc_effective_lengths_csr); out_words receives each program's effective
+ * instructions in program order (src/Introns.h:50-57).  OpenMP over
+ * programs. */
+void orc_extract_effective_csr(const orc_isa_t* isa, const uint32_t* words, const int64_t* offsets,
+                               int64_t n_programs, const int64_t* eff_offsets, uint32_t* out_words,
+                               int threads) {
+#ifdef _OPENMP
+    if (threads < 1) threads = omp_get_max_threads();
+    #pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+#endif
+    for (int64_t i = 0; i < n_programs; ++i)
+        orc_extract_effective(isa, words + offsets[i], offsets[i + 1] - offsets[i], out_words + eff_offsets[i]);
+    (void)threads;
 }
 
 int orc_max_threads(void) {

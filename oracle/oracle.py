@@ -69,6 +69,7 @@ class Oracle:
                 "orc_output_reg": (C.c_int, [P(OrcIsa)]),
                 "orc_decode": (C.c_int, [P(OrcIsa), C.c_uint32, P(C.c_int32)]),
                 "orc_apply_op": (C.c_float, [C.c_int, C.c_int, C.c_float, C.c_float]),
+                "orc_apply_op_n": (None, [C.c_int, C.c_int, P(_F32), P(_F32), _I64, P(_F32)]),
                 "orc_case_outputs": (None, [P(OrcIsa), P(_U32), _I64, P(_F32), C.c_int, _I64, P(_F32)]),
                 "orc_case_outputs_f64": (None, [P(OrcIsa), P(_U32), _I64, P(_F32), C.c_int, _I64, P(_F64)]),
                 "orc_trace_case": (None, [P(OrcIsa), P(_U32), _I64, P(_F32), C.c_int, P(_F32)]),
@@ -79,6 +80,12 @@ class Oracle:
                                                        C.c_int, _I64, P(_F32), P(_F64), C.c_int]),
                 "orc_evaluate_population_dense": (None, [P(OrcIsa), P(_U32), P(_U8), _I64, _I64, P(_F32),
                                                          P(_F32), C.c_int, _I64, P(_F32)]),
+                "orc_case_outputs_csr": (None, [P(OrcIsa), P(_U32), P(_I64), _I64, P(_F32), C.c_int, _I64,
+                                                P(_F32), C.c_int, C.c_int]),
+                "orc_evaluate_population_csr_opt": (None, [P(OrcIsa), P(_U32), P(_I64), _I64, P(_F32), P(_F32),
+                                                           C.c_int, _I64, P(_F32), P(_F64), C.c_int, C.c_int]),
+                "orc_extract_effective_csr": (None, [P(OrcIsa), P(_U32), P(_I64), _I64, P(_I64), P(_U32),
+                                                     C.c_int]),
                 "orc_effective_mask": (_I64, [P(OrcIsa), P(_U32), _I64, P(_U8)]),
                 "orc_extract_effective": (_I64, [P(OrcIsa), P(_U32), _I64, P(_U32)]),
                 "orc_effective_lengths_csr": (None, [P(OrcIsa), P(_U32), P(_I64), _I64, P(_I64)]),
@@ -104,6 +111,13 @@ class Oracle:
 
     def apply_op(self, op: int, a: float, b: float) -> float:
         return self.lib().orc_apply_op(self.profile, op, a, b)
+
+    def apply_op_n(self, op: int, a, b) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        b = np.ascontiguousarray(b, dtype=np.float32)
+        out = np.empty(a.shape[0], dtype=np.float32)
+        self.lib().orc_apply_op_n(self.profile, op, _p(a, _F32), _p(b, _F32), a.shape[0], _p(out, _F32))
+        return out
 
     def case_outputs(self, prog, inputs, n_cases=None) -> np.ndarray:
         prog = np.ascontiguousarray(prog, dtype=np.uint32)
@@ -159,6 +173,35 @@ class Oracle:
                                                inputs.shape[0], _p(fit, _F32), _p(sse, _F64), threads)
         return (fit, sse) if with_sse else fit
 
+    def case_outputs_csr(self, words, offsets, inputs, threads: int = 0, effective_only: bool = False,
+                         n_cases=None) -> np.ndarray:
+        """Per-case outputs of CSR programs, shape (n_programs, n_cases)."""
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        inputs = np.ascontiguousarray(inputs, dtype=np.float32)
+        k = inputs.shape[1] if inputs.ndim == 2 else 1
+        N = inputs.shape[0] if n_cases is None else n_cases
+        n = offsets.shape[0] - 1
+        out = np.empty((n, N), dtype=np.float32)
+        self.lib().orc_case_outputs_csr(C.byref(self.isa), _p(words, _U32), _p(offsets, _I64), n,
+                                        _p(inputs, _F32), k, N, _p(out, _F32), threads, int(effective_only))
+        return out
+
+    def evaluate_csr_opt(self, words, offsets, inputs, targets, threads: int = 0, effective_only: bool = False):
+        """(fitness, double SSE) of CSR programs; see orc_evaluate_population_csr_opt."""
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        inputs = np.ascontiguousarray(inputs, dtype=np.float32)
+        targets = np.ascontiguousarray(targets, dtype=np.float32)
+        n = offsets.shape[0] - 1
+        fit = np.empty(n, dtype=np.float32)
+        sse = np.empty(n, dtype=np.float64)
+        k = inputs.shape[1] if inputs.ndim == 2 else 1
+        self.lib().orc_evaluate_population_csr_opt(C.byref(self.isa), _p(words, _U32), _p(offsets, _I64), n,
+                                                   _p(inputs, _F32), _p(targets, _F32), k, inputs.shape[0],
+                                                   _p(fit, _F32), _p(sse, _F64), threads, int(effective_only))
+        return fit, sse
+
     def evaluate_csr_r2(self, words, offsets, inputs, targets, threads: int = 0):
         """R^2 fitness (src/Evaluator.cpp:49-97) of CSR programs."""
         words = np.ascontiguousarray(words, dtype=np.uint32)
@@ -185,6 +228,19 @@ class Oracle:
         self.lib().orc_effective_lengths_csr(C.byref(self.isa), _p(words, _U32), _p(offsets, _I64), n,
                                              _p(out, _I64))
         return out
+
+    def extract_effective_csr(self, words, offsets, threads: int = 0):
+        """(effective words, offsets) of every program, host-side: the
+        reference's PackedEffective layout."""
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        eff = self.effective_lengths(words, offsets)
+        eoff = np.zeros(eff.size + 1, dtype=np.int64)
+        np.cumsum(eff, out=eoff[1:])
+        out = np.empty(int(eoff[-1]), dtype=np.uint32)
+        self.lib().orc_extract_effective_csr(C.byref(self.isa), _p(words, _U32), _p(offsets, _I64), eff.size,
+                                             _p(eoff, _I64), _p(out, _U32), threads)
+        return out, eoff
 
     @staticmethod
     def mse_to_fitness(mse: float) -> float:

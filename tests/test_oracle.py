@@ -64,6 +64,18 @@ def test_case_outputs_and_fitness_bit_exact(oracle_lib, variant):
         assert same_bits(fit, v[f"{d}_fitness"]), d
         mse = (sse / X.shape[0]).astype(np.float32)
         assert same_bits(mse, v[f"{d}_mse"]), d
+        # the threaded population forms, full and effective-code-only, give
+        # the same bits (the config-sized GPU parity tests use them)
+        for eff in (False, True):
+            assert same_bits(o.case_outputs_csr(words, off, X, threads=4, effective_only=eff),
+                             v[f"{d}_outputs"]), (d, eff)
+            fit2, sse2 = o.evaluate_csr_opt(words, off, X, y, threads=4, effective_only=eff)
+            assert same_bits(fit2, v[f"{d}_fitness"]), (d, eff)
+            assert np.array_equal(sse2.view(np.uint64), sse.view(np.uint64)), (d, eff)
+        ew, eo = o.extract_effective_csr(words, off)
+        for i in range(0, len(off) - 1, 7):
+            p = words[off[i]:off[i + 1]]
+            assert np.array_equal(ew[eo[i]:eo[i + 1]], p[o.effective_mask(p)])
 
 
 @pytest.mark.parametrize("variant", list(VARIANTS))
