@@ -3,24 +3,36 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Workload (one step = one generation's evaluation of the whole population):
-2^20 seeded random LGP programs, lengths U[16,256] with ~40% introns by
-construction, 5 input features U[-3,3], 4,096 fitness cases, target = a
-seeded random 16-effective-instruction program + N(0, 0.01^2); reference ISA,
-16 registers.  Synthetic data of the reference's shapes (no datasets ship).
+Headline workload (the HBM-streaming configuration at full size): a
+population of 2^22 seeded random LGP programs, lengths log-uniform in
+[32,1024] (uniform random words, ~10% effective), resident in HBM; 8 input
+features U[-1,1] over 2^20 fitness cases (32 MiB + 4 MiB); target = a seeded
+random 24-effective-instruction program; reference ISA, 16 registers; the
+intron pre-pass on.  One step evaluates the next batch of 2^18 programs of
+the population (16 steps = one generation); one whole-population call (all
+2^22 programs) is timed beside the steps.  Synthetic data of the reference's
+shapes (no datasets ship).
 
 Metric: GPop/s = (effective instructions x fitness cases) / second, whole job.
 ``value``: population resident in HBM when the clock starts (intron pre-pass,
 interpreter and fitness reduction on the device).  ``e2e``: the same through
-the host-pointer C call (galop_evaluate_csr): H2D of the raw population from
-pinned memory, pre-pass, interpretation, D2H of fitness, every step.
+the host-pointer C call (galop_evaluate_csr): H2D of the step's raw programs
+from pinned memory, pre-pass, interpretation, D2H of fitness, every step.
+
+Beside the headline the line carries: the single-generation configuration
+(2^20 programs, 4,096 cases) measured the same way, the reference's own GPU
+kernel on that configuration's whole population (raw words and host-stripped
+effective words, as its Packed and PackedEffective layouts), the batching
+configuration at a stated scale with all 2^22 cases (persistent batched
+launch against one plain launch per population), and the reference's CPU
+evaluator timed on the host's cores.
 
 Multi-GPU (torchrun, one rank per GPU): every rank evaluates its own
 population of the same size on the shared dataset (programs are independent,
 so there is no collective on the data path; torch.distributed is used only for
 the barrier and the max-over-ranks of the timings).  ``--impl reference``
 times the reference's own CPU evaluator (Evaluator::evaluate_sr_mse built from
-its sources, OpenMP over programs on every host core) on a bounded sample of
+its sources, OpenMP over programs on every host core) on bounded samples of
 the same workload.
 """
 from __future__ import annotations
@@ -43,9 +55,13 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "GPop/s (eff. instr x cases/s) vs FP32-issue roofline; p50/p99 eval latency"
 UNIT = "GPop/s"
-WORKLOAD = ("single generation: 2^20 random programs, L~U[16,256] (~40% introns by construction), "
-            "5 features U[-3,3], 4096 cases, target = random 16-effective-instruction program + N(0,0.01^2), "
-            "reference ISA with 16 registers")
+WORKLOAD = ("HBM-streaming configuration at full size: population of 2^22 random programs resident in HBM, "
+            "L log-uniform [32,1024], 8 features U[-1,1], 2^20 cases (32 MiB + 4 MiB), target = random "
+            "24-effective-instruction program, reference ISA with 16 registers, intron pre-pass on; one step "
+            "evaluates the next 2^18-program batch of the population (16 steps = one generation)")
+SINGLE_WORKLOAD = ("single generation: 2^20 random programs, L~U[16,256] (~40% introns by construction), "
+                   "5 features U[-3,3], 4096 cases, target = random 16-effective-instruction program + "
+                   "N(0,0.01^2), reference ISA with 16 registers")
 
 
 def parse():
@@ -54,25 +70,31 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--programs", type=int, default=1 << 20)
-    ap.add_argument("--cases", type=int, default=4096)
+    ap.add_argument("--programs", type=int, default=1 << 22, help="population of the headline workload")
+    ap.add_argument("--batch-programs", type=int, default=1 << 18, help="programs evaluated per step")
+    ap.add_argument("--cases", type=int, default=1 << 20)
     ap.add_argument("--cases-per-lane", type=int, default=0)
     ap.add_argument("--warps-per-block", type=int, default=0)
     ap.add_argument("--reduce", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline only: skip the single-generation, batching and reference-GPU keys")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "stream", "evo", "capacity"],
-                    help="single: the headline single-generation workload; batch: many populations in one "
+    ap.add_argument("--workload", default="generation",
+                    choices=["generation", "single", "batch", "serve", "evo", "capacity"],
+                    help="generation: the headline (HBM-streaming configuration at full size); single: "
+                         "the single-generation configuration alone; batch: many populations in one "
                          "persistent launch per generation (graph replay) vs one plain launch per population; "
-                         "serve: continuous batching of Poisson-arriving GP runs; stream: 2^20-case dataset; "
-                         "evo: a whole 100-generation run of the reference engine with this backend, beside "
-                         "the reference's own whole-run benchmark on the same GPU; capacity: the largest "
-                         "device-resident population that evaluates, and its footprint per program")
+                         "serve: continuous batching of Poisson-arriving GP runs; evo: a whole 100-generation "
+                         "run of the reference engine with this backend, beside the reference's own whole-run "
+                         "benchmark on the same GPU; capacity: the largest device-resident population that "
+                         "evaluates, and its footprint per program")
     ap.add_argument("--evo-pop", type=int, default=100000, choices=[10000, 100000, 1000000])
     ap.add_argument("--evo-cases", type=int, default=1024)
     ap.add_argument("--evo-seed", type=int, default=70)
-    ap.add_argument("--scale", type=float, default=1.0 / 32,
-                    help="population-size scale of the batch/serve/stream workloads")
+    ap.add_argument("--scale", type=float, default=1.0 / 64,
+                    help="population-size scale of the batch workload (the serve workload runs at full size)")
+    ap.add_argument("--batch-generations", type=int, default=3)
     return ap.parse_args()
 
 
@@ -159,11 +181,6 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def load_workload(n_programs: int, n_cases: int, seed: int):
-    from galop_b200 import workloads as W
-    return W.single_generation(seed=seed, n_programs=n_programs, n_cases=n_cases)
-
-
 def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -171,10 +188,9 @@ def measured_peaks() -> dict:
     return {}
 
 
-def profile_summary() -> dict:
-    """Kernel name and DRAM bytes per interpreter launch from the committed
-    ncu summary."""
-    p = ROOT / "profiles" / "interp_single_generation.json"
+def profile_summary(name: str) -> dict:
+    """Figures of a committed ncu summary (profiles/<name>.json)."""
+    p = ROOT / "profiles" / f"{name}.json"
     if p.exists():
         try:
             return json.loads(p.read_text())
@@ -187,7 +203,6 @@ def fp32_issue_peak(device: int, peaks: dict):
     """SMs x 128 FP32 lanes x the measured maximum SM clock, in G lane-ops/s."""
     sm_count = 148
     try:
-        import ctypes
         cudart = ctypes.CDLL("libcudart.so")
         v = ctypes.c_int()
         if cudart.cudaDeviceGetAttribute(ctypes.byref(v), 16, device) == 0:
@@ -195,7 +210,8 @@ def fp32_issue_peak(device: int, peaks: dict):
     except OSError:
         pass
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
-    return sm_count * 128 * sm_max * 1e6 / 1e9, sm_count, sm_max
+    src = "sm_max_mhz of MEASURED_PEAKS.json" if "sm_max_mhz" in peaks else "fallback clock 1965 MHz"
+    return sm_count * 128 * sm_max * 1e6 / 1e9, sm_count, sm_max, src
 
 
 def hbm_view(traffic, kernel_ms: float, peaks: dict):
@@ -206,14 +222,37 @@ def hbm_view(traffic, kernel_ms: float, peaks: dict):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = traffic / (kernel_ms / 1e3) / 1e9
     return {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": "hbm_gbs of MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback"}
+            "peak_source": "hbm_gbs of MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
 
 
-def profile_traffic():
-    return profile_summary().get("dram_bytes_per_launch_full")
+def roofline(eff_instr: float, interp_instr: float, n_cases: int, kernel_ms: float, device: int, prof: dict,
+             programs_per_launch: int) -> dict:
+    """The interpreter against the FP32-issue roofline (1 op = 1 effective
+    instruction x 1 case); DRAM traffic from the committed ncu capture,
+    scaled from its program count to this launch's."""
+    peaks = measured_peaks()
+    peak, sm_count, sm_max, src = fp32_issue_peak(device, peaks)
+    achieved = eff_instr * n_cases / (kernel_ms / 1e3) / 1e9
+    traffic = None
+    if prof.get("dram_bytes") and prof.get("programs"):
+        traffic = float(prof["dram_bytes"]) * programs_per_launch / float(prof["programs"])
+    return {"bound": "fp32_issue", "achieved": achieved, "peak": peak, "unit": UNIT, "frac": achieved / peak,
+            "traffic": traffic, "kernel": prof.get("kernel", "interp_wide_kernel"), "kernel_ms": kernel_ms,
+            "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {sm_max:.0f} MHz ({src})",
+            "ops_per_launch": float(eff_instr) * n_cases,
+            # instructions the interpreter actually runs per case: the effective ones minus
+            # those evaluated once per program (every operand case-independent) and the copies
+            # of programs interpreted once
+            "interpreted_ops_per_launch": float(interp_instr) * n_cases,
+            "interpreted_achieved": interp_instr * n_cases / (kernel_ms / 1e3) / 1e9,
+            "hbm_view": hbm_view(traffic, kernel_ms, peaks),
+            "issue_slots_active": prof.get("issue_slots_active"),
+            "achieved_occupancy": prof.get("achieved_occupancy"),
+            "traffic_source": (f"ncu capture of {prof.get('programs')} programs x {prof.get('cases')} cases, "
+                               f"scaled to {programs_per_launch} programs") if traffic else None}
 
 
-def cpu_reference_rate(wl, seconds: float, threads: int):
+def cpu_reference_rate(wl, seconds: float, threads: int, batch: int = 0):
     """The reference's CPU evaluator (libref_nr16: Evaluator::evaluate_sr_mse
     + mse_to_fitness, OpenMP over programs) on successive batches of the
     workload until `seconds` of wall time; effective-instruction GPop/s."""
@@ -227,7 +266,10 @@ def cpu_reference_rate(wl, seconds: float, threads: int):
         orc = Oracle(0, 16)
         evaluate = lambda w, o: orc.evaluate_csr(w, o, wl.X, wl.y, threads=threads)  # noqa: E731
     orc = Oracle(0, 16)
-    batch = 256
+    if batch <= 0:
+        # about a second of work per batch on these threads
+        raw_per_prog = float(wl.offsets[-1]) / max(wl.n_programs, 1)
+        batch = int(max(threads, min(4096, 4e8 * threads / max(raw_per_prog * wl.n_cases, 1.0))))
     done_progs, ops, t_total = 0, 0.0, 0.0
     start = 0
     while t_total < seconds:
@@ -246,11 +288,22 @@ def cpu_reference_rate(wl, seconds: float, threads: int):
     return rate, kind, done_progs, t_total
 
 
+def headline_workload(args, seed: int, prefix=None):
+    from galop_b200 import workloads as W
+    return W.hbm_streaming(seed=seed, n_programs=args.programs, n_cases=args.cases, prefix_programs=prefix)
+
+
 def run_reference(args, dist: Dist):
     if dist.rank != 0:
         return
     threads = os.cpu_count() or 1
-    wl = load_workload(min(args.programs, 16384), args.cases, 2)
+    if args.workload == "single":
+        from galop_b200 import workloads as W
+        wl = W.single_generation(seed=2, n_programs=16384, n_cases=4096)
+        workload, cases = SINGLE_WORKLOAD, 4096
+    else:
+        wl = headline_workload(args, 3, prefix=4096)
+        workload, cases = WORKLOAD, args.cases
     per_step = max(2.0, args.cpu_seconds / max(args.steps, 1))
     for _ in range(max(args.warmup, 0)):
         cpu_reference_rate(wl, 0.5, threads)
@@ -267,183 +320,272 @@ def run_reference(args, dist: Dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(secs)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "programs_per_step": progs, "cases": args.cases,
-                   "sample": f"first {progs} programs of the same workload per step"},
+        "config": {"workload": workload, "programs_per_step": progs, "cases": cases,
+                   "sample": f"the first {progs} programs of the same population per step"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": f"{progs} programs x {args.cases} cases per step, ~{per_step:.0f} s each"},
+                         "sample": f"{progs} programs x {cases} cases per step, ~{per_step:.0f} s each"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def run_b200(args, dist: Dist):
+def batches_of(offsets: np.ndarray, batch: int):
+    """[(lo, hi, offsets rebased to 0)] program ranges of `batch` programs."""
+    n = offsets.shape[0] - 1
+    out = []
+    for lo in range(0, n, batch):
+        hi = min(n, lo + batch)
+        out.append((lo, hi, np.ascontiguousarray(offsets[lo:hi + 1] - offsets[lo])))
+    return out
+
+
+def cpu_baseline_leg(wl, args) -> dict:
+    threads = os.cpu_count() or 1
+    rate, kind, progs, secs = cpu_reference_rate(wl, args.cpu_seconds, threads)
+    # the reference's CpuEvaluator as shipped is serial (src/EvaluatorCpu.cpp:7-15)
+    rate1, _, progs1, secs1 = cpu_reference_rate(wl, 3.0, 1)
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"the first {progs} programs of the population x {wl.n_cases} cases ({secs:.1f} s wall, "
+                      f"OpenMP over programs)",
+            "one_core": {"value": rate1, "unit": UNIT, "cores": 1,
+                         "sample": f"the first {progs1} programs x {wl.n_cases} cases ({secs1:.1f} s)"}}
+
+
+def run_generation(args, dist: Dist):
+    """The headline: the HBM-streaming configuration at full size."""
     import galop_b200 as g
 
-    wl = load_workload(args.programs, args.cases, 2 + dist.rank)
-    ds = g.Dataset(wl.X, wl.y)
-    ev = g.Evaluator(num_registers=16, device=dist.local if dist.world > 1 else 0, reduce=args.reduce,
-                     cases_per_lane=args.cases_per_lane, warps_per_block=args.warps_per_block)
-    ev.set_dataset(ds)
+    dev = dist.local if dist.world > 1 else 0
+    wl = headline_workload(args, 3 + dist.rank)
     n = wl.n_programs
-    words = np.ascontiguousarray(wl.words)
-    offsets = np.ascontiguousarray(wl.offsets)
+    words, offsets = wl.words, wl.offsets
+    pop_bytes = words.nbytes
+    B = min(args.batch_programs, n)
+    bats = batches_of(offsets, B)
+    ev = g.Evaluator(num_registers=16, device=dev, reduce=args.reduce, cases_per_lane=args.cases_per_lane,
+                     warps_per_block=args.warps_per_block)
+    ev.set_dataset(g.Dataset(wl.X, wl.y))
 
     # ---- device-resident population: the `value` leg -------------------------
     d_words = ev.device_alloc(words.nbytes)
-    d_off = ev.device_alloc(offsets.nbytes)
+    ev.h2d(d_words, words)
+    d_off_all = ev.device_alloc(offsets.nbytes)
+    ev.h2d(d_off_all, offsets)
+    d_boff = []
+    for lo, hi, o in bats:
+        d = ev.device_alloc(o.nbytes)
+        ev.h2d(d, o)
+        d_boff.append(d)
     d_fit = ev.device_alloc(4 * n)
     d_sse = ev.device_alloc(8 * n)
-    ev.h2d(d_words, words)
-    ev.h2d(d_off, offsets)
 
-    def step_device():
-        ev.evaluate_csr_device(d_words, d_off, n, int(offsets[-1]), d_fit, d_sse)
-        ev.synchronize()
-        st = ev.stats
-        return st
+    def step_device(i):
+        b = i % len(bats)
+        lo, hi, o = bats[b]
+        ev.evaluate_csr_device(d_words + 4 * int(offsets[lo]), d_boff[b], hi - lo, int(o[-1]), d_fit + 4 * lo,
+                               d_sse + 8 * lo)
+        return ev.stats
 
-    for _ in range(args.warmup):
-        step_device()
-    # counts of one evaluation (identical every step)
-    fit_check = ev.evaluate_csr(words, offsets)
-    st0 = ev.stats
-    eff_instr, raw_instr = st0.eff_instructions, st0.raw_instructions
-    interp_instr = st0.interp_instructions
-
-    clocks = ClockSampler(dist.local)
+    for i in range(args.warmup):
+        step_device(i)
+    clocks = ClockSampler(dev)
     dist.barrier()
     ev.synchronize()
     clocks.start()
     ev.timer_record(0)
-    interp_ms, launches = [], 0
-    for _ in range(args.steps):
-        st = step_device()
-        interp_ms.append(st.interp_ms)
-        launches += st.kernels_launched
+    per_step = []
+    for i in range(args.steps):
+        st = step_device(args.warmup + i)
+        per_step.append((st.eff_instructions, st.interp_instructions, st.raw_instructions, st.interp_ms,
+                         st.total_ms, st.kernels_launched, st.n_programs))
     ev.timer_record(1)
     ms_total = ev.timer_elapsed(0, 1)
     clock = clocks.stop()
     dist.barrier()
     ms_total_max = dist.max(ms_total)
-    ops_rank = float(eff_instr) * wl.n_cases * args.steps
-    ops_all = dist.sum(ops_rank)
+    eff_sum = float(sum(r[0] for r in per_step))
+    ops_all = dist.sum(eff_sum * wl.n_cases)
     value = ops_all / (ms_total_max / 1e3) / 1e9
+    launches = int(sum(r[5] for r in per_step))
+
+    # ---- one whole generation: all programs in one call ----------------------
+    ev.evaluate_csr_device(d_words, d_off_all, n, int(offsets[-1]), d_fit, d_sse)
+    stg = ev.stats
+    full_fit = np.empty(n, np.float32)
+    ev.d2h(full_fit, d_fit)
+    generation = {"programs": n, "ms": stg.total_ms,
+                  "value": stg.eff_instructions * wl.n_cases / (stg.total_ms / 1e3) / 1e9, "unit": UNIT,
+                  "interp_ms": stg.interp_ms, "raw_instructions": stg.raw_instructions,
+                  "effective_instructions": stg.eff_instructions,
+                  "interpreted_instructions": stg.interp_instructions}
 
     # ---- end to end through the host-pointer C call ---------------------------
     pin_w = g.PinnedArray(words.shape, np.uint32)
-    pin_o = g.PinnedArray(offsets.shape, np.int64)
-    pin_f = g.PinnedArray((n,), np.float32)
     pin_w.array[:] = words
-    pin_o.array[:] = offsets
-    ev.evaluate_csr(pin_w.array, pin_o.array, fitness_out=pin_f.array)   # warm the host path
+    pin_o = [g.PinnedArray(o.shape, np.int64) for _, _, o in bats]
+    for p_, (_, _, o) in zip(pin_o, bats):
+        p_.array[:] = o
+    pin_f = g.PinnedArray((B,), np.float32)
+
+    def step_host(i):
+        b = i % len(bats)
+        lo, hi, o = bats[b]
+        ev.evaluate_csr(pin_w.array[offsets[lo]:offsets[hi]], pin_o[b].array, fitness_out=pin_f.array[:hi - lo])
+        return b, hi - lo, int(o[-1])
+
+    step_host(0)   # warm the host path (and its copy stream)
     dist.barrier()
     ev.synchronize()
     ev.timer_record(2)
-    e2e_launches = 0
-    for _ in range(args.steps):
-        ev.evaluate_csr(pin_w.array, pin_o.array, fitness_out=pin_f.array)
-        e2e_launches += ev.stats.kernels_launched
+    e2e_wall, h2d_bytes, d2h_bytes = [], 0, 0
+    check = None
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        b, m, nw = step_host(args.warmup + i)
+        e2e_wall.append((time.perf_counter() - t0) * 1e3)
+        h2d_bytes += 4 * nw + 8 * (m + 1)
+        d2h_bytes += 4 * m
+        if check is None:
+            lo = bats[b][0]
+            check = bool(np.array_equal(pin_f.array[:m].view(np.uint32), full_fit[lo:lo + m].view(np.uint32)))
     ev.timer_record(3)
     e2e_ms = dist.max(ev.timer_elapsed(2, 3))
     e2e_value = ops_all / (e2e_ms / 1e3) / 1e9
-    assert np.array_equal(pin_f.array.view(np.uint32), fit_check.view(np.uint32))
+    assert check, "host-pointer fitness differs from the device-resident call's"
 
-    # ---- roofline of the interpreter (FP32 issue) -------------------------------
-    peaks = measured_peaks()
-    peak_gops, sm_count, sm_max = fp32_issue_peak(dist.local if dist.world > 1 else 0, peaks)
-    interp_avg_ms = float(np.mean(interp_ms))
-    achieved = eff_instr * wl.n_cases / (interp_avg_ms / 1e3) / 1e9
-
-    # ---- the reference's own GPU kernel on the same B200 (a sample) ------------
-    ref_gpu = None
-    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        try:
-            from oracle.oracle import Oracle, RefCuda
-            m = min(n, 4096)
-            sub = wl.subsample(np.arange(m))
-            _, kms = RefCuda().evaluate_packed(sub.words, sub.offsets, wl.X, wl.y, reps=1)
-            eff = float(Oracle(0, 16).effective_lengths(sub.words, sub.offsets).sum())
-            ref_gpu = {"value": eff * wl.n_cases / (kms / 1e3) / 1e9, "unit": UNIT,
-                       "raw_gpops": float(sub.offsets[-1]) * wl.n_cases / (kms / 1e3) / 1e9,
-                       "kernel_ms": kms, "sample": f"first {m} programs x {wl.n_cases} cases",
-                       "kernel": "evaluate_kernel_packed from the reference's src/EvaluatorCuda.cu, sm_100a"}
-        except (FileNotFoundError, OSError, RuntimeError) as e:
-            ref_gpu = {"unavailable": str(e)}
-
+    kernel_ms = float(sum(r[3] for r in per_step))
+    interp_sum = float(sum(r[1] for r in per_step))
+    raw_sum = float(sum(r[2] for r in per_step))
+    roof = roofline(eff_sum / args.steps, interp_sum / args.steps, wl.n_cases, kernel_ms / args.steps, dev,
+                    profile_summary("interp_hbm_streaming"), B)
     cpu = None
+    extras = {}
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        rate, kind, progs, secs = cpu_reference_rate(wl, args.cpu_seconds, threads)
-        # the reference's CpuEvaluator as shipped is serial (src/EvaluatorCpu.cpp:7-15)
-        rate1, _, progs1, secs1 = cpu_reference_rate(wl, 3.0, 1)
-        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
-               "sample": f"first {progs} programs of the workload x {wl.n_cases} cases ({secs:.1f} s wall, "
-                         f"OpenMP over programs)",
-               "one_core": {"value": rate1, "unit": UNIT, "cores": 1,
-                            "sample": f"first {progs1} programs x {wl.n_cases} cases ({secs1:.1f} s)"}}
+        cpu = cpu_baseline_leg(wl, args)
+    for d in [d_words, d_off_all, d_fit, d_sse] + d_boff:
+        ev.device_free(d)
+    for p_ in [pin_w, pin_f] + pin_o:
+        p_.free()
+    ev.close()
+    n_cases = wl.n_cases
+    del wl, words, offsets
+    if dist.rank == 0 and dist.world == 1 and not args.no_extras:
+        extras["single_generation"] = single_generation_leg(args)
+        extras["batching"] = batching_leg(args)
 
     if dist.rank == 0:
+        total_ms = [r[4] for r in per_step]
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_total_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "programs_per_gpu": n, "cases": wl.n_cases,
-                       "raw_instructions_per_gpu": raw_instr, "effective_instructions_per_gpu": eff_instr,
-                       "interpreted_instructions_per_gpu": interp_instr,
-                       "cases_per_lane": st0.cases_per_lane, "warps_per_block": st0.warps_per_block,
+            "config": {"workload": WORKLOAD, "population_per_gpu": n, "programs_per_step": B,
+                       "steps_per_generation": len(bats), "cases": n_cases,
+                       "raw_instructions_per_step": raw_sum / args.steps,
+                       "effective_instructions_per_step": eff_sum / args.steps,
+                       "interpreted_instructions_per_step": interp_sum / args.steps,
                        "reduce": ["kahan32", "fp64", "ordered"][args.reduce],
-                       "l2": "inputs larger than L2 (raw population %.2f GB per GPU)" % (words.nbytes / 1e9),
+                       "l2": "inputs larger than L2 (the population's raw words are %.2f GB per GPU, each "
+                             "step's batch %.2f GB); the 36 MB dataset itself fits in L2" %
+                             (pop_bytes / 1e9, 4.0 * raw_sum / args.steps / 1e9),
                        "parallelism": f"programs sharded, {dist.world} rank(s), no data-path collective"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(words.nbytes + offsets.nbytes),
-                    "d2h_bytes_per_step": int(4 * n), "ms_per_step": e2e_ms / args.steps},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d_bytes / args.steps),
+                    "d2h_bytes_per_step": int(d2h_bytes / args.steps), "ms_per_step": e2e_ms / args.steps,
+                    "latency_ms": {"p50": float(np.percentile(e2e_wall, 50)),
+                                   "p99": float(np.percentile(e2e_wall, 99))}},
             "gpu_launches": launches,
-            "raw_gpops": value * raw_instr / max(eff_instr, 1),
-            "roofline": {"bound": "fp32_issue", "achieved": achieved, "peak": peak_gops, "unit": UNIT,
-                         "frac": achieved / peak_gops, "traffic": profile_traffic(),
-                         "kernel": profile_summary().get("kernel", "interp_wide_kernel"), "kernel_ms": interp_avg_ms,
-                         "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {sm_max:.0f} MHz "
-                                        f"(sm_max_mhz of MEASURED_PEAKS.json)",
-                         "ops_per_launch": float(eff_instr) * wl.n_cases,
-                         # instructions the interpreter actually runs per case: the effective ones
-                         # minus those evaluated once per program (every operand case-independent)
-                         "interpreted_ops_per_launch": float(interp_instr) * wl.n_cases,
-                         "interpreted_achieved": interp_instr * wl.n_cases / (interp_avg_ms / 1e3) / 1e9,
-                         # the same kernel read against HBM (it streams each program once)
-                         "hbm_view": hbm_view(profile_traffic(), interp_avg_ms, peaks),
-                         "issue_slots_active": profile_summary().get("issue_slots_active")},
+            "raw_gpops": value * raw_sum / max(eff_sum, 1.0),
+            "roofline": roof,
             "clocks": clock,
-            "latency_ms": {"p50": float(np.percentile(interp_ms, 50)), "p99": float(np.percentile(interp_ms, 99))},
+            # one evaluation call (pre-pass through finalize) on the device, per step
+            "latency_ms": {"p50": float(np.percentile(total_ms, 50)), "p99": float(np.percentile(total_ms, 99)),
+                           "scope": "device time of one evaluate call of 2^18 programs x 2^20 cases"},
+            "generation": generation,
         }
         if cpu:
             line["cpu_baseline"] = cpu
-        if ref_gpu:
-            line["reference_gpu_same_b200"] = ref_gpu
+        line.update(extras)
         print(json.dumps(line), flush=True)
-    for d in (d_words, d_off, d_fit, d_sse):
-        ev.device_free(d)
-    pin_w.free()
-    pin_o.free()
-    pin_f.free()
-    ev.close()
 
 
-def run_batch(args):
-    """Many populations of uneven sizes and lengths on one shared dataset,
-    one persistent launch per generation replayed from a CUDA graph; the
-    plain form (one launch per population, no intron pass) timed beside it,
-    and the compensated-FP32 fitness compared with the FP64 case-order sum."""
+def single_generation_leg(args) -> dict:
+    """The single-generation configuration (2^20 programs x 4,096 cases),
+    device-resident, beside the reference's own GPU kernel on the same whole
+    population."""
     import galop_b200 as g
     from galop_b200 import workloads as W
-    n_cases = args.cases if args.cases != 4096 else 1 << 16
+    wl = W.single_generation(seed=2, n_programs=1 << 20, n_cases=4096)
+    n = wl.n_programs
+    out = {"workload": SINGLE_WORKLOAD}
+    with g.Evaluator(num_registers=16) as ev:
+        ev.set_dataset(g.Dataset(wl.X, wl.y))
+        d_w, d_o = ev.device_alloc(wl.words.nbytes), ev.device_alloc(wl.offsets.nbytes)
+        d_f = ev.device_alloc(4 * n)
+        ev.h2d(d_w, wl.words)
+        ev.h2d(d_o, wl.offsets)
+        for _ in range(2):
+            ev.evaluate_csr_device(d_w, d_o, n, int(wl.offsets[-1]), d_f)
+            ev.stats
+        ms, interp = [], []
+        for _ in range(5):
+            ev.evaluate_csr_device(d_w, d_o, n, int(wl.offsets[-1]), d_f)
+            st = ev.stats
+            ms.append(st.total_ms)
+            interp.append(st.interp_ms)
+        for d in (d_w, d_o, d_f):
+            ev.device_free(d)
+    out.update({"value": st.eff_instructions * 4096 / (np.mean(ms) / 1e3) / 1e9, "unit": UNIT,
+                "ms_per_generation": float(np.mean(ms)),
+                "roofline": roofline(st.eff_instructions, st.interp_instructions, 4096, float(np.mean(interp)), 0,
+                                     profile_summary("interp_single_generation"), n),
+                "effective_instructions": st.eff_instructions, "interpreted_instructions": st.interp_instructions,
+                "raw_instructions": st.raw_instructions})
+    try:
+        from oracle.oracle import Oracle, RefCuda
+        ref = RefCuda()
+        _, kms_raw = ref.evaluate_packed(wl.words, wl.offsets, wl.X, wl.y, reps=3)
+        ew, eo = Oracle(0, 16).extract_effective_csr(wl.words, wl.offsets)
+        _, kms_eff = ref.evaluate_packed(ew, eo, wl.X, wl.y, reps=3)
+        eff = float(eo[-1]) * 4096
+        out["reference_gpu_same_b200"] = {
+            "kernel": "evaluate_kernel_packed from the reference's src/EvaluatorCuda.cu, sm_100a, launched as "
+                      "tests/cuda_capacity.cu:119-132 does (grid ceil(n/8) x 256)",
+            "sample": f"the whole population ({n} programs x 4096 cases), mean of 3 launches after one warm-up",
+            "packed_raw_words": {"kernel_ms": kms_raw, "value": eff / (kms_raw / 1e3) / 1e9, "unit": UNIT,
+                                 "raw_gpops": float(wl.offsets[-1]) * 4096 / (kms_raw / 1e3) / 1e9},
+            "packed_effective_words": {"kernel_ms": kms_eff, "value": eff / (kms_eff / 1e3) / 1e9, "unit": UNIT,
+                                       "note": "introns stripped on the host first, as its PackedEffective "
+                                               "layout (src/EvaluatorCuda.cu:374-422)"},
+            "ours_over_best_reference": out["value"] / (eff / (min(kms_raw, kms_eff) / 1e3) / 1e9)}
+    except (FileNotFoundError, OSError, RuntimeError) as e:
+        out["reference_gpu_same_b200"] = {"unavailable": str(e)}
+    return out
+
+
+def batching_leg(args) -> dict:
+    """The batching configuration: 64 populations of uneven sizes (log-uniform
+    [1k, 2^20] x scale) and lengths (log-uniform [8,2048]) on one shared
+    dataset of 2^22 cases x 4 features N(0, 10^2) with targets ~1e4 + N(0,1).
+    The batched form evaluates every population in one persistent launch per
+    generation, replayed from a CUDA graph; the plain form launches one
+    warp-per-individual grid per population (one warp per program over all
+    cases, program order, no work queue, no case chunking) with the same
+    intron pass, folding and dedup.  KAHAN32 fitness is compared with the
+    FP64 case-order sum of the same outputs."""
+    import galop_b200 as g
+    from galop_b200 import workloads as W
+    n_cases = 1 << 22
     lo, hi = max(8, int(1000 * args.scale)), max(64, int((1 << 20) * args.scale))
     isa, X, y, pops = W.many_populations(n_cases=n_cases, size_lo=lo, size_hi=hi)
     ds = g.Dataset(X, y)
+    gens = max(1, args.batch_generations)
     ev = g.Evaluator(num_registers=16)
-    # Tile from the autotuner, measured on a sample of all populations together.
     all_words = np.concatenate([w for w, _ in pops])
     all_off = np.concatenate([[0]] + [o[1:] + base for (_, o), base in
                                       zip(pops, np.cumsum([0] + [int(o[-1]) for _, o in pops[:-1]]))])
-    tune = ev.autotune(all_words, all_off.astype(np.int64), ds, cache=os.environ.get("GALOP_TUNE_CACHE"))
+    # tile from the autotuner, on a sample of all populations together
+    tune = ev.autotune(all_words, all_off.astype(np.int64), ds, cache=os.environ.get("GALOP_TUNE_CACHE"),
+                       sample=2048)
     rd = g.ResidentDataset(ev, ds)
     caps = [(rd, o.shape[0] - 1, int(o[-1])) for _, o in pops]
     b = g.Batch(ev, caps)
@@ -455,12 +597,11 @@ def run_batch(args):
         b.synchronize()
         return b.stats
 
-    for _ in range(args.warmup):
-        generation(True)
-    dev_ms, wall = [], time.perf_counter()
-    for _ in range(args.steps):
+    generation(True)
+    dev_ms, t0 = [], time.perf_counter()
+    for _ in range(gens):
         dev_ms.append(generation(True).total_ms)
-    wall = (time.perf_counter() - wall) * 1e3 / args.steps
+    wall = (time.perf_counter() - t0) * 1e3 / gens
     st = b.stats
     eff_total = 0
     for p_ in range(len(pops)):
@@ -471,7 +612,8 @@ def run_batch(args):
     batched = ops / (np.mean(dev_ms) / 1e3) / 1e9
     fit_k = [b.fitness(p_) for p_ in range(len(pops))]
     b.close()
-    # FP64 case-order reference of the same outputs
+    rd.close()
+    # FP64 case-order sum of the same outputs
     ev_o = g.Evaluator(num_registers=16, reduce=g.REDUCE_ORDERED)
     rd_o = g.ResidentDataset(ev_o, ds)
     bo = g.Batch(ev_o, [(rd_o, c[1], c[2]) for c in caps])
@@ -481,82 +623,107 @@ def run_batch(args):
     bo.synchronize()
     fit_o = [bo.fitness(p_) for p_ in range(len(pops))]
     bo.close()
+    rd_o.close()
     ev_o.close()
     fk = np.concatenate(fit_k).astype(np.float64)
     fo = np.concatenate(fit_o).astype(np.float64)
     nz = fo > 0
     rel = float(np.max(np.abs(fk[nz] - fo[nz]) / fo[nz])) if nz.any() else 0.0
     zero_mismatch = int(np.sum((fo > 0) != (fk > 0)))
-    # plain: one launch per population, raw programs (no intron pass), per generation
-    ev_p = g.Evaluator(num_registers=16, intron_prepass=False)
+    # plain: one warp-per-individual launch per population, same pre-pass
+    ev_p = g.Evaluator(num_registers=16, schedule=g.SCHEDULE_PLAIN, cases_per_lane=tune.cases_per_lane,
+                       warps_per_block=tune.warps_per_block)
     ev_p.set_dataset(ds)
     plain_ms = 0.0
+    fit_p = []
     for w, o in pops:
-        ev_p.evaluate_csr(w, o)
+        fit_p.append(ev_p.evaluate_csr(w, o))
         plain_ms += ev_p.stats.prepass_ms + ev_p.stats.interp_ms + ev_p.stats.finalize_ms
     ev_p.close()
+    ev.close()
+    fp = np.concatenate(fit_p).astype(np.float64)
+    nzk = fk > 0
     plain = ops / (plain_ms / 1e3) / 1e9
-    line = {
-        "metric": METRIC, "value": batched, "unit": UNIT, "workload": "batch", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(dev_ms)),
-        "wall_ms_per_generation": wall, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": f"{len(pops)} populations, sizes log-uniform [{lo},{hi}] (x{args.scale:g} of "
-                               f"[1000, 2^20]), lengths log-uniform [8,2048], one shared dataset of {n_cases} cases "
-                               "x 4 features N(0,10^2), targets ~1e4 + N(0,1); generations replayed from a CUDA graph",
-                   "programs": int(sum(c[1] for c in caps)), "raw_instructions": int(sum(c[2] for c in caps)),
-                   "effective_instructions": int(eff_total)},
-        "plain_per_population_gpops": plain, "speedup_vs_plain": batched / plain,
+    peak, sm_count, sm_max, src = fp32_issue_peak(0, measured_peaks())
+    return {
+        "workload": f"batching configuration at population scale {args.scale:g}: {len(pops)} populations, sizes "
+                    f"log-uniform [{lo},{hi}] (x{args.scale:g} of [1000, 2^20]), lengths log-uniform [8,2048], "
+                    f"one shared dataset of {n_cases} cases x 4 features N(0,10^2), targets ~1e4 + N(0,1); "
+                    f"{gens} generations replayed from a CUDA graph",
+        "value": batched, "unit": UNIT, "ms_per_generation": float(np.mean(dev_ms)),
+        "wall_ms_per_generation": wall, "generations": gens,
+        "programs": int(sum(c[1] for c in caps)), "raw_instructions": int(sum(c[2] for c in caps)),
+        "effective_instructions": int(eff_total),
+        "plain_per_population": {"value": plain, "unit": UNIT, "ms_per_generation": plain_ms,
+                                 "launch": "one grid per population: one warp per program over all cases, "
+                                           "program order, no work queue, no case chunking; intron pass, "
+                                           "folding and dedup as the batched form"},
+        "speedup_vs_plain": batched / plain,
+        "plain_fitness_rel_err_vs_batched": float(np.max(np.abs(fp[nzk] - fk[nzk]) / fk[nzk])) if nzk.any() else 0.0,
         "fitness_rel_err_kahan32_vs_fp64_case_order": rel,
         "fitness_zero_mismatches": zero_mismatch,
         "kernels_per_generation": st.kernels_launched,
         "autotune": {k: v for k, v in tune.as_dict().items() if k != "key"},
+        "roofline": {"bound": "fp32_issue", "achieved": batched, "peak": peak, "unit": UNIT,
+                     "frac": batched / peak, "scope": "whole generation (pre-pass, interpreter, finalize), device time",
+                     "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {sm_max:.0f} MHz ({src})"},
     }
-    peak_gops, sm_count, sm_max = fp32_issue_peak(0, measured_peaks())
-    line["roofline"] = {"bound": "fp32_issue", "achieved": batched, "peak": peak_gops, "unit": UNIT,
-                        "frac": batched / peak_gops, "traffic": None,
-                        "scope": "whole generation (pre-pass, interpreter, finalize), device time",
-                        "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {sm_max:.0f} MHz "
-                                       f"(sm_max_mhz of MEASURED_PEAKS.json)"}
-    rd.close()
-    ev.close()
+
+
+def run_batch(args):
+    out = batching_leg(args)
+    line = {"metric": METRIC, "value": out["value"], "unit": UNIT, "workload": "batch", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": out["workload"]}, **{k: v for k, v in out.items() if k not in ("value", "unit")}}
     print(json.dumps(line), flush=True)
 
 
 def run_serve(args):
-    """256 independent GP runs arriving as a Poisson process (mean 2 ms),
-    each with its own dataset; every run submits its generations one after
-    the other through the continuous-batching server."""
+    """The serving configuration at its stated distributions: 256
+    independent GP runs arriving as a Poisson process (mean 2 ms), each with
+    its own seeded dataset (cases log-uniform [256, 2^20], 1-8 features) and
+    population (log-uniform [1k, 2^18] programs, lengths U[8,512]); every run
+    submits two generations one after the other (the second a variation of
+    the first: 10% of its words redrawn) through the continuous-batching
+    server, admission capped at 150 GB of HBM.  A run's data are generated
+    when it arrives and dropped when it finishes."""
     import threading
     import galop_b200 as g
     from galop_b200 import workloads as W
-    cases_hi = max(1024, int((1 << 20) * args.scale * 2))
-    pop_hi = max(1024, int((1 << 18) * args.scale * 2))
-    isa, runs = W.serving_runs(n_runs=256, cases_hi=cases_hi, pop_hi=pop_hi, generations=3)
+    specs = W.serving_run_specs(n_runs=256)
     ev = g.Evaluator(num_registers=16)
     sv = g.Server(ev, hbm_budget_bytes=int(150e9), slots=4, slot_programs=1 << 20, slot_words=1 << 27,
-                  slot_items=1 << 23)
+                  slot_items=1 << 25, pinned_bytes=4 << 30)
     rng = np.random.default_rng(9)
-    arrivals = np.cumsum(rng.exponential(2e-3, size=len(runs)))
-    lat, queued, sizes = [], [], []
+    arrivals = np.cumsum(rng.exponential(2e-3, size=len(specs)))
+    lat, queued, sizes, peak = [], [], [], [0]
     lock = threading.Lock()
+    errors = []
     t0 = time.perf_counter()
 
     def client(i):
-        X, y, gens = runs[i]
-        delay = t0 + arrivals[i] - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        rid = sv.open_run(g.Dataset(X, y))
-        for w, o in gens:
-            rq = sv.submit(rid, w, o)
-            _, info = sv.wait(rq)
+        try:
+            delay = t0 + arrivals[i] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            X, y, (w, o) = W.serving_run_data(specs[i])
+            rid = sv.open_run(g.Dataset(X, y))
+            for gen in range(2):
+                if gen:
+                    W.vary_words(np.random.default_rng(specs[i]["seed"] + gen), w, 0.1, 16)
+                rq = sv.submit(rid, w, o)
+                _, info = sv.wait(rq)
+                with lock:
+                    lat.append(info.latency_ms)
+                    queued.append(info.queued_ms)
+                    sizes.append(info.batch_requests)
+                    peak[0] = max(peak[0], sv.totals.resident_bytes)
+            sv.close_run(rid)
+        except Exception as e:  # reported in the line
             with lock:
-                lat.append(info.latency_ms)
-                queued.append(info.queued_ms)
-                sizes.append(info.batch_requests)
-        sv.close_run(rid)
+                errors.append(f"run {i}: {e}")
 
-    threads = [threading.Thread(target=client, args=(i,)) for i in range(len(runs))]
+    threads = [threading.Thread(target=client, args=(i,)) for i in range(len(specs))]
     for t in threads:
         t.start()
     for t in threads:
@@ -569,43 +736,19 @@ def run_serve(args):
         "metric": METRIC, "value": tot.case_ops / wall / 1e9, "unit": UNIT, "workload": "serve",
         "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                       "mean": float(np.mean(lat))},
+                       "mean": float(np.mean(lat)),
+                       "scope": "submit -> fitness in the caller's buffer, per generation of one run"},
         "queued_ms": {"p50": float(np.percentile(queued, 50)), "p99": float(np.percentile(queued, 99))},
         "requests": len(lat), "batches": int(tot.batches), "mean_batch_requests": float(np.mean(sizes)),
         # sum of the batches' own device times over wall time: above 1 when
         # batches in different slots overlap on the device
         "batch_device_time_over_wall": tot.device_ms / 1e3 / wall, "wall_s": wall,
-        "config": {"workload": f"256 GP runs, Poisson arrivals (mean 2 ms), 3 generations each; cases "
-                               f"log-uniform [256,{cases_hi}], 1-8 features; populations log-uniform "
-                               f"[1000,{pop_hi}], lengths U[8,512]; HBM admission cap 150 GB; 4 batches in flight"},
+        "device_busy_s": tot.device_ms / 1e3, "peak_resident_gb": peak[0] / 1e9,
+        "errors": errors[:5],
+        "config": {"workload": "256 GP runs, Poisson arrivals (mean 2 ms), 2 generations each; cases "
+                               "log-uniform [256, 2^20], 1-8 features U[-1,1]; populations log-uniform "
+                               "[1000, 2^18], lengths U[8,512]; HBM admission cap 150 GB; 4 batches in flight"},
     }
-    print(json.dumps(line), flush=True)
-
-
-def run_stream(args):
-    """2^20 fitness cases x 8 features (32 MiB + 4 MiB resident), programs
-    log-uniform [32,1024], the intron pre-pass on; a sample of the 2^22
-    programs."""
-    import galop_b200 as g
-    from galop_b200 import workloads as W
-    n = max(1024, int((1 << 22) * args.scale / 8))
-    wl = W.hbm_streaming(n_programs=n, n_cases=1 << 20)
-    ev = g.Evaluator(num_registers=16)
-    ev.set_dataset(g.Dataset(wl.X, wl.y))
-    for _ in range(args.warmup):
-        ev.evaluate_csr(wl.words, wl.offsets)
-    ms = []
-    for _ in range(args.steps):
-        ev.evaluate_csr(wl.words, wl.offsets)
-        ms.append(ev.stats.interp_ms + ev.stats.prepass_ms + ev.stats.finalize_ms)
-    st = ev.stats
-    ev.close()
-    ops = float(st.eff_instructions) * wl.n_cases
-    line = {"metric": METRIC, "value": ops / (np.mean(ms) / 1e3) / 1e9, "unit": UNIT, "workload": "stream",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(ms)),
-            "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": wl.description, "programs": n, "raw_instructions": st.raw_instructions,
-                       "effective_instructions": st.eff_instructions, "case_chunks": st.case_chunks}}
     print(json.dumps(line), flush=True)
 
 
@@ -793,14 +936,16 @@ def main():
             run_batch(args)
         elif args.workload == "serve":
             run_serve(args)
-        elif args.workload == "stream":
-            run_stream(args)
         elif args.workload == "evo":
             run_evo(args)
         elif args.workload == "capacity":
             run_capacity(args)
+        elif args.workload == "single":
+            line = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+                    "data": "synthetic (seeded)", **single_generation_leg(args)}
+            print(json.dumps(line), flush=True)
         else:
-            run_b200(args, dist)
+            run_generation(args, dist)
     finally:
         dist.close()
 

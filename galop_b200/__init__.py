@@ -33,6 +33,7 @@ LIB_PATH = _PKG / "libgalop_b200.so"
 PROFILE_REF, PROFILE_BJ = 0, 1
 REDUCE_KAHAN32, REDUCE_FP64, REDUCE_ORDERED = 0, 1, 2
 OBJECTIVE_MSE, OBJECTIVE_R2 = 0, 1
+SCHEDULE_PERSISTENT, SCHEDULE_PLAIN = 0, 1
 
 OK = 0
 E_INVALID, E_CUDA, E_NOMEM, E_NO_DATASET, E_TIMEOUT, E_CAPACITY, E_NO_DEVICE, E_STATE = (
@@ -70,7 +71,7 @@ class _Options(C.Structure):
         ("reduce", C.c_int32), ("constants", C.POINTER(C.c_float)), ("device", C.c_int32),
         ("intron_prepass", C.c_int32), ("cases_per_lane", C.c_int32),
         ("warps_per_block", C.c_int32), ("dispatch", C.c_int32), ("objective", C.c_int32),
-        ("dedup", C.c_int32), ("reserved", C.c_int32 * 1),
+        ("dedup", C.c_int32), ("schedule", C.c_int32),
     ]
 
 
@@ -319,7 +320,7 @@ class Evaluator:
                  reduce: int = REDUCE_KAHAN32, constants: Optional[Sequence[float]] = None,
                  device: int = 0, intron_prepass: bool = True, cases_per_lane: int = 0,
                  warps_per_block: int = 0, dispatch: Optional[int] = None, objective: int = OBJECTIVE_MSE,
-                 dedup: Optional[bool] = None):
+                 dedup: Optional[bool] = None, schedule: int = SCHEDULE_PERSISTENT):
         self._lib = load_library()
         opt = _Options()
         self._lib.galop_options_init(C.byref(opt))
@@ -336,6 +337,7 @@ class Evaluator:
         opt.objective = objective
         if dedup is not None:
             opt.dedup = int(bool(dedup))
+        opt.schedule = schedule
         self.constants = None
         if constants is not None:
             self.constants = np.ascontiguousarray(constants, dtype=np.float32)

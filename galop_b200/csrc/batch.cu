@@ -205,7 +205,7 @@ int enqueue(galop_batch* b) {
         // (intron pass on), forwarding flags on every wide stream
         FoldParams fp{ctx->isa.profile, ctx->isa.num_registers, ctx->isa.output_reg,
                       7u + (uint32_t)__builtin_ctz(b->fmt.stride / 128u), 0, b->descs.p, b->prog_pop.p,
-                      fold ? 1 : 0};
+                      fold ? 1 : 0, 1};
         fold_kernel<<<blocks, tpb, 0, s>>>(reinterpret_cast<uint4*>(b->uops.p), b->eff_off.p, G, fp, b->eff_len.p,
                                            b->livein.p,
                                            b->counters.p + 3);
@@ -217,7 +217,7 @@ int enqueue(galop_batch* b) {
         const uint4* u4 = reinterpret_cast<const uint4*>(b->uops.p);
         size_t tmp = b->dtmp.cap;
         dedup_hash_kernel<<<blocks, tpb, 0, s>>>(u4, b->eff_off.p, b->eff_len.p, G, b->dkeys.p, b->dvals.p, b->rep.p,
-                                                 b->prog_pop.p);
+                                                 b->prog_pop.p, b->livein.p);
         B_CK(cub::DeviceRadixSort::SortPairs(b->dtmp.p, tmp, b->dkeys.p, b->dkeys_sorted.p, b->dvals.p,
                                              b->dvals_sorted.p, (int)G, 0, 64, s), "dedup sort");
         dedup_run_start_kernel<<<blocks, tpb, 0, s>>>(b->dkeys_sorted.p, G, b->dhead.p);
@@ -225,7 +225,7 @@ int enqueue(galop_batch* b) {
         B_CK(cub::DeviceScan::InclusiveScan(b->dtmp.p, tmp, b->dhead.p, b->dvals.p, cub::Max(), (int)G, s),
              "dedup scan");
         dedup_rep_kernel<<<blocks, tpb, 0, s>>>(b->dvals.p, b->dvals_sorted.p, G, u4, b->eff_off.p, b->eff_len.p,
-                                                b->rep.p, b->counters.p + 4, b->prog_pop.p);
+                                                b->rep.p, b->counters.p + 4, b->prog_pop.p, b->livein.p);
         b->launches += 5;
     }
     batch_key_kernel<<<blocks, tpb, 0, s>>>(b->layout.p, b->prog_pop.p, b->eff_len.p, G, b->key.p);

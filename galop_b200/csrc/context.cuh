@@ -67,6 +67,8 @@ inline double targets_ss_tot(const float* y, int64_t n) {
 // [7] size of the first register-file class in the order.
 constexpr int kCounters = 8;
 constexpr int kCounterBadOffsets = 6;
+constexpr int kCounterClassSplit = 7;   // programs of the 8-slot class at the head of the order
+constexpr int kSplitSlots = 8;          // register-file slots of the smaller interpreter
 
 struct galop_ctx {
     galop_options opt{};
@@ -106,6 +108,7 @@ struct galop_ctx {
     bool flagged = false;         // the last pre-pass marked forwarding and live-in registers
     bool folded = false;          // the last pre-pass folded constants (interp lengths in eff_len)
     bool deduped = false;         // ... and left identical programs out (representatives in rep)
+    bool class_split = false;     // ... and ordered the programs by register-file class
     DevBuf<unsigned long long> dkeys, dkeys_sorted;
     DevBuf<int32_t> dvals, dvals_sorted, rep, dhead;
     DevBuf<unsigned char> dsort_tmp;
@@ -138,6 +141,7 @@ namespace galop {
 int pick_k(const galop_ctx* ctx);
 int pick_wpb(const galop_ctx* ctx);
 const void* kernel_for(const galop_ctx* ctx, int k, int mode);
+const void* kernel_for_slots(const galop_ctx* ctx, int k, int mode, int nslot);
 int pick_dispatch(const galop_ctx* ctx);
 UopFormat uop_format(const galop_ctx* ctx);
 size_t interp_smem_bytes(const galop_ctx* ctx, int k, int wpb);

@@ -24,10 +24,14 @@ namespace galop {
 // 64-bit FNV-1a over the length and the micro-op words.
 // group (may be null): programs of different groups (populations of a
 // batch, each on its own dataset) are never merged.
+// livein (may be null): the per-program live-in words of the folding pass,
+// part of what makes two programs equal (renamed micro-ops do not say which
+// registers their slots start from).
 static __global__ void dedup_hash_kernel(const uint4* __restrict__ uops, const int64_t* __restrict__ eff_off,
                                          const int32_t* __restrict__ len, int64_t n,
                                          unsigned long long* __restrict__ keys, int32_t* __restrict__ vals,
-                                         int32_t* __restrict__ rep, const int32_t* __restrict__ group) {
+                                         int32_t* __restrict__ rep, const int32_t* __restrict__ group,
+                                         const uint32_t* __restrict__ livein) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int32_t L = len[i];
@@ -39,6 +43,7 @@ static __global__ void dedup_hash_kernel(const uint4* __restrict__ uops, const i
     };
     mix((uint32_t)L);
     if (group) mix((uint32_t)group[i]);
+    if (livein) mix(livein[i]);
     for (int32_t j = 0; j < L; ++j) {
         const uint4 u = p[j];
         mix(u.x);
@@ -68,7 +73,7 @@ static __global__ void dedup_rep_kernel(const int32_t* __restrict__ head_pos, co
                                         int64_t n, const uint4* __restrict__ uops,
                                         const int64_t* __restrict__ eff_off, int32_t* __restrict__ len,
                                         int32_t* __restrict__ rep, unsigned long long* __restrict__ dup_count,
-                                        const int32_t* __restrict__ group) {
+                                        const int32_t* __restrict__ group, const uint32_t* __restrict__ livein) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool copy = false;
     int32_t L = 0;
@@ -77,7 +82,7 @@ static __global__ void dedup_rep_kernel(const int32_t* __restrict__ head_pos, co
         if (h != j) {
             const int32_t head = vals[h], i = vals[j];
             L = len[head];
-            if (len[i] == L && (!group || group[i] == group[head])) {
+            if (len[i] == L && (!group || group[i] == group[head]) && (!livein || livein[i] == livein[head])) {
                 const uint4* hp = uops + eff_off[head + 1] - L;
                 const uint4* ip = uops + eff_off[i + 1] - L;
                 copy = true;

@@ -49,6 +49,8 @@ struct FoldParams {
     const PopDesc* pops;
     const int32_t* prog_pop;
     int fold;                    // 0: forwarding flags only (no folding, no dead-code removal)
+    int rename;                  // 1: values renamed into register-file slots (rename_slots);
+                                 // 0: the ISA's register layout (register traces)
 };
 
 // Operand swap that keeps the result bits: ADD, MUL, and LT <-> GT of REF.
@@ -223,6 +225,91 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
     return kept;
 }
 
+// ---- register renaming ------------------------------------------------------
+//
+// The interpreter's register file is per warp in shared memory, so the
+// registers a program needs -- not the ISA's NR -- set how many warps fit on
+// an SM.  rename_slots assigns every value of the program's final micro-op
+// order u[0, n) a slot of the file: each register the program reads before
+// writing it gets one of slots 0..m-1 (in register order: the interpreter
+// loads the i-th set bit of the live-in mask into slot i), each result gets
+// the lowest free slot, and a slot is free again after the last instruction
+// that reads its value, or when its register is overwritten.  On
+// straight-line code this linear scan uses as many slots as there are
+// values live at once.  An instruction's operands whose values end there
+// are freed before its result is placed, so the result may take an
+// operand's slot: the interpreter loads every operand of an instruction
+// before that instruction's result is stored (results are stored, if at
+// all, at the start of the next instruction, before it loads anything).
+// The forwarding flags, set on registers before renaming, stay valid: they
+// name the previous instruction's value, whatever slot it gets.
+constexpr uint32_t kDies1 = 1u << 8;    // src1's value is not read after this instruction
+constexpr uint32_t kDies2 = 1u << 9;    // the same for a register src2
+
+__device__ __forceinline__ uint32_t rename_slots(uint4* __restrict__ u, int64_t n, uint32_t sh, int output_reg,
+                                                 uint32_t livein) {
+    // backward: mark the reads whose values end at their instruction
+    uint32_t live = 1u << output_reg;   // registers live after instruction j
+    for (int64_t j = n - 1; j >= 0; --j) {
+        uint4 w = u[j];
+        const uint32_t d = w.z >> sh;
+        const bool bcast = (w.w & ~kWideFlags) == kWideBcast;
+        const uint32_t reads = uop_reads(w, sh);
+        if (!bcast && !(w.w & kWideSpecial)) {
+            const uint32_t r = w.x >> sh;
+            if (r == d || !((live >> r) & 1u)) w.w |= kDies1;
+        }
+        if (!bcast && !(w.w & 8u)) {
+            const uint32_t r = w.y >> sh;
+            if (r == d || !((live >> r) & 1u)) w.w |= kDies2;
+        }
+        u[j] = w;
+        live = (live & ~(1u << d)) | reads;
+    }
+    // forward: linear-scan slot assignment
+    int8_t slot_of[kMaxRegisters];
+    for (int r = 0; r < kMaxRegisters; ++r) slot_of[r] = -1;
+    uint32_t used = 0u, top = 0u;
+    for (uint32_t m = livein & 0xFFFFu; m != 0u; m &= m - 1u) {
+        const int r = __ffs(m) - 1;
+        slot_of[r] = (int8_t)top;
+        used |= 1u << top;
+        ++top;
+    }
+    for (int64_t j = 0; j < n; ++j) {
+        uint4 w = u[j];
+        const uint32_t d = w.z >> sh;
+        const bool bcast = (w.w & ~(kWideFlags | kDies1 | kDies2)) == kWideBcast;
+        const bool reads1 = !bcast && !(w.w & kWideSpecial);
+        const bool reads2 = !bcast && !(w.w & 8u);
+        const uint32_t r1 = w.x >> sh, r2 = w.y >> sh;
+        if (reads1) w.x = (uint32_t)slot_of[r1] << sh;
+        if (reads2) w.y = (uint32_t)slot_of[r2] << sh;
+        if (reads1 && (w.w & kDies1) && slot_of[r1] >= 0) {
+            used &= ~(1u << slot_of[r1]);
+            slot_of[r1] = -1;
+        }
+        if (reads2 && (w.w & kDies2) && slot_of[r2] >= 0) {
+            used &= ~(1u << slot_of[r2]);
+            slot_of[r2] = -1;
+        }
+        if (slot_of[d] >= 0) {           // the register's old value, never read again
+            used &= ~(1u << slot_of[d]);
+            slot_of[d] = -1;
+        }
+        const uint32_t p = (uint32_t)(__ffs(~used) - 1);
+        used |= 1u << p;
+        slot_of[d] = (int8_t)p;
+        if (p + 1u > top) top = p + 1u;
+        w.z = p << sh;
+        w.w &= ~(kDies1 | kDies2);
+        u[j] = w;
+    }
+    const uint32_t out = slot_of[output_reg] >= 0 ? (uint32_t)slot_of[output_reg] : 0u;
+    if (top < 1u) top = 1u;
+    return pack_livein(livein, top, out);
+}
+
 static __global__ void fold_kernel(uint4* __restrict__ uops, const int64_t* __restrict__ eff_off, int64_t n,
                                    FoldParams fp, int32_t* __restrict__ interp_len,
                                    uint32_t* __restrict__ livein, unsigned long long* __restrict__ total) {
@@ -234,15 +321,17 @@ static __global__ void fold_kernel(uint4* __restrict__ uops, const int64_t* __re
         uint4* __restrict__ u = uops + p0;
         const uint32_t sh = fp.stride_shift;
         const int k_in = fp.pops ? fp.pops[fp.prog_pop[i]].num_inputs : fp.num_inputs;
+        uint32_t in = 0u;
         if (!fp.fold) {
-            livein[i] = mark_forwarding(u, L, sh, fp.output_reg, fp.profile);
-            interp_len[i] = (int32_t)L;
+            in = mark_forwarding(u, L, sh, fp.output_reg, fp.profile);
+            kept = L;
         } else {
-            uint32_t in = 0u;
             kept = fold_program(u, L, fp, k_in, in);
-            livein[i] = in;
-            interp_len[i] = (int32_t)kept;
         }
+        livein[i] = fp.rename ? rename_slots(u + (L - kept), kept, sh, fp.output_reg, in)
+                              : pack_livein(in, (uint32_t)fp.num_registers, (uint32_t)fp.output_reg);
+        interp_len[i] = (int32_t)kept;
+        if (!fp.fold) kept = 0;
     }
     __shared__ unsigned long long sk;
     if (threadIdx.x == 0) sk = 0;

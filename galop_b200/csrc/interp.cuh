@@ -83,6 +83,16 @@ struct InterpArgs {
     const unsigned long long* items;
     int64_t n_items;
     const int64_t* n_items_dev;    // the item count computed on the device (dedup), or null
+    // Plain schedule (single population): warp w of the grid evaluates
+    // program w over all its cases (n_chunks 1, no order, no queue), and a
+    // dedup copy (interp_len < 0) is skipped.
+    int32_t plain;
+    // Register-file classes (single population, wide kernel): the order
+    // lists the programs whose values fit in 8 slots first; *class_split is
+    // their count.  class_part 0 covers those slots of the order, 1 the rest.
+    // class_split null: one launch covers the whole order.
+    const unsigned long long* class_split;
+    int32_t class_part;
 };
 
 template <int K>
@@ -209,13 +219,19 @@ interp_smem_kernel(InterpArgs args) {
         reinterpret_cast<float*>(galop_smem4)[i] = args.consts.c[i / RS];
     __syncthreads();
     const bool batched = args.pops != nullptr;
+    const bool plain = args.plain != 0;
     const int64_t total_items = batched ? args.n_items : args.n_programs * (int64_t)args.n_chunks;
     constexpr int kPass = 32 * K;
 
-    for (;;) {
+    for (int round = 0;; ++round) {
         unsigned long long item = 0;
-        if (lane == 0) item = atomicAdd(args.counter, 1ull);
-        item = __shfl_sync(0xffffffffu, item, 0);
+        if (plain) {
+            if (round > 0) break;
+            item = (unsigned long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        } else {
+            if (lane == 0) item = atomicAdd(args.counter, 1ull);
+            item = __shfl_sync(0xffffffffu, item, 0);
+        }
         if ((int64_t)item >= total_items) break;
 
         // Resolve the work item: program, case range, dataset, output slot.

@@ -1,14 +1,19 @@
 // interp_wide.cuh -- the wide-micro-op interpreter (dispatch 3).
 //
 // Same work decomposition as the shared-memory interpreter of interp.cuh
-// (one warp per program or case chunk, K cases per lane, the lane's NR x K
+// (one warp per program or case chunk, K cases per lane, the lane's
 // register file in shared memory), but every instruction is a 16-byte
 // micro-op whose operand fields are already byte offsets into the register
 // file (encode_wide in isa.cuh), and a constant operand carries its value.
-// Runs of binary instructions execute inside one PTX loop (WideLoop); per
-// instruction the warp does:
-//   one broadcast 16-byte shared load of the micro-op (the 32-instruction
-//     window is staged in shared memory; the next micro-op is prefetched
+// The register file has NSLOT slots per lane, not the ISA's NR registers:
+// the folding pass renames each program's values into as few slots as it
+// keeps live at once (fold.cuh), and the runtime runs the programs that fit
+// in 8 slots on the 8-slot instance, which needs half the shared memory per
+// warp.  Runs of binary instructions execute inside one PTX loop (WideLoop);
+// per instruction the warp does:
+//   one broadcast 16-byte shared load of the micro-op (32-instruction
+//     windows are staged in shared memory with cp.async, the next window
+//     copied while the current one runs; the next micro-op is prefetched
 //     into a second register set, the loop body existing twice),
 //   a sign test (unary ops and the window end leave the loop),
 //   one jump table (16 arms: 8 ops x register/constant src2, each with
@@ -22,9 +27,9 @@
 // profile), which run in C++ on the slow branch with the CUDA math library,
 // read and write them too.  The last result is never stored: the output
 // is taken from it when the last instruction wrote the output register.
-// Each pass initialises only the registers the program reads before
-// writing them (args.livein).  The folding pass sets the flags and the
-// masks (isa.cuh, fold.cuh).
+// Each pass initialises only the values the program reads before writing
+// them (args.livein: registers, slots used, output slot).  The folding pass
+// sets the flags and these words (isa.cuh, fold.cuh).
 //
 // Semantics are those of interp.cuh (src/Interpreter.cpp:36-59,
 // src/ISA.h:219-231, src/Evaluator.cpp:11-45 and :88-91).
@@ -92,17 +97,17 @@ __device__ __forceinline__ void sts_u4(uint32_t addr, uint4 u) {
                  : "memory");
 }
 
-// Shared memory per warp: NR registers x stride, then a 33-entry micro-op
-// stage (32 instructions + a permanent end marker).
+// Shared memory per warp: NSLOT register slots x stride, then two 33-entry
+// micro-op stages (32 instructions + a permanent end marker each).
 constexpr uint32_t kWideStageBytes = 33u * 16u;
 
-template <int NR, int K>
+template <int NSLOT, int K>
 __host__ __device__ constexpr uint32_t wide_warp_bytes() {
-    return (uint32_t)NR * 128u * K + kWideStageBytes;
+    return (uint32_t)NSLOT * 128u * K + 2u * kWideStageBytes;
 }
 
-inline size_t wide_smem_bytes(int nr, int k, int warps) {
-    return (size_t)warps * ((size_t)nr * 128u * (size_t)k + kWideStageBytes);
+inline size_t wide_smem_bytes(int nslot, int k, int warps) {
+    return (size_t)warps * ((size_t)nslot * 128u * (size_t)k + 2u * kWideStageBytes);
 }
 
 // One work item of the persistent queue: which program, which cases, which
@@ -117,7 +122,8 @@ struct WideItem {
     Objective obj;
 };
 
-__device__ __forceinline__ WideItem resolve_item(const InterpArgs& args, unsigned long long item) {
+__device__ __forceinline__ WideItem resolve_item(const InterpArgs& args, unsigned long long item,
+                                                int64_t slot_lo) {
     WideItem w;
     w.partial_index = -1;
     if (args.pops != nullptr) {
@@ -138,7 +144,7 @@ __device__ __forceinline__ WideItem resolve_item(const InterpArgs& args, unsigne
         w.out_index = w.prog - d->prog_base;
         if (d->n_chunks > 1) w.partial_index = (int64_t)item;
     } else {
-        const int64_t slot = (int64_t)item / args.n_chunks;
+        const int64_t slot = slot_lo + (int64_t)item / args.n_chunks;
         const int chunk = (int)((int64_t)item % args.n_chunks);
         w.prog = args.order ? (int64_t)args.order[slot] : slot;
         w.X = args.X;
@@ -193,8 +199,49 @@ __device__ __forceinline__ void unary_op(uint32_t op, const float (&b)[K], float
     }
 }
 
-template <int NR, int K, int PROFILE, int REDUCE, int MODE>
-__global__ void __launch_bounds__(256, 3)
+// Launch bounds: at most GALOP_WIDE_MAX_THREADS threads per block and at
+// least GALOP_WIDE_MIN_BLOCKS blocks per SM, which caps the registers per
+// thread.
+#ifndef GALOP_WIDE_MAX_THREADS
+#define GALOP_WIDE_MAX_THREADS 256
+#endif
+#ifndef GALOP_WIDE_MIN_BLOCKS
+#define GALOP_WIDE_MIN_BLOCKS 3
+#endif
+
+// Asynchronous copy of one 16-byte micro-op into shared memory (cached in
+// L2 only), and the waits.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Stage window w of a program (micro-ops [32w, min(32w + 32, L))) into the
+// stage at st: lane l copies micro-op 32w + l asynchronously; in a partial
+// window the first slot past the program gets the end marker (a full
+// window ends at the stage's permanent marker, slot 32).
+__device__ __forceinline__ void stage_window(uint32_t st, const uint4* __restrict__ pw, int64_t L, int64_t w,
+                                             int lane) {
+    const int64_t j = w * 32 + lane;
+    if (j < L) cp_async16(st + (uint32_t)lane * 16u, pw + j);
+    else if (j == L) sts_u4(st + (uint32_t)lane * 16u, make_uint4(0u, 0u, 0u, kWideEnd));
+    cp_async_commit();
+}
+
+// NSLOT: register-file slots per warp.  The folding pass renames each
+// program's values into slots (rename_slots in fold.cuh); a program whose
+// values need at most NSLOT slots runs here.  Trace mode interprets the raw
+// program in the ISA's own register layout (NSLOT = NR).
+//
+// Micro-op staging: each warp has two 33-entry stages.  A program of at
+// most two 32-instruction windows is staged once per work item and stays in
+// shared memory for all its passes over the cases; a longer one is streamed
+// window by window, the next window (the first one again at the end of a
+// pass) copied with cp.async into the other stage while the current one
+// runs.
+template <int NSLOT, int K, int PROFILE, int REDUCE, int MODE>
+__global__ void __launch_bounds__(GALOP_WIDE_MAX_THREADS, GALOP_WIDE_MIN_BLOCKS)
 interp_wide_kernel(InterpArgs args) {
     extern __shared__ float4 galop_smem4[];
     using WR = WideRegs<K>;
@@ -203,31 +250,61 @@ interp_wide_kernel(InterpArgs args) {
     constexpr int kPass = 32 * K;
     const int lane = threadIdx.x & 31;
     const uint32_t warp_base = (uint32_t)__cvta_generic_to_shared(galop_smem4) +
-                               (threadIdx.x >> 5) * wide_warp_bytes<NR, K>();
-    const uint32_t base = warp_base + (uint32_t)lane * V * 4u;   // this lane's register 0
-    const uint32_t stage = warp_base + NR * S;
+                               (threadIdx.x >> 5) * wide_warp_bytes<NSLOT, K>();
+    const uint32_t base = warp_base + (uint32_t)lane * V * 4u;   // this lane's slot 0
+    const uint32_t stage0 = warp_base + NSLOT * S;
+    const uint32_t stage1 = stage0 + kWideStageBytes;
     const uint4 kEnd4 = make_uint4(0u, 0u, 0u, kWideEnd);
-    if (lane == 0) sts_u4(stage + 32u * 16u, kEnd4);
+    if (lane == 0) {
+        sts_u4(stage0 + 32u * 16u, kEnd4);
+        sts_u4(stage1 + 32u * 16u, kEnd4);
+    }
     __syncwarp();
 
+    const bool plain = args.plain != 0;
     const int64_t n_work = args.n_skipped ? args.n_programs - (int64_t)*args.n_skipped : args.n_programs;
+    // the slots of the order this launch covers (one register-file class)
+    int64_t slot_lo = 0, slot_hi = n_work;
+    if (args.class_split != nullptr) {
+        const int64_t n0 = (int64_t)*args.class_split;
+        if (args.class_part == 0) slot_hi = n0 < n_work ? n0 : n_work;
+        else slot_lo = n0 < n_work ? n0 : n_work;
+    }
     const int64_t total_items = args.pops != nullptr ? (args.n_items_dev ? *args.n_items_dev : args.n_items)
-                                                     : n_work * (int64_t)args.n_chunks;
+                              : plain ? args.n_programs : (slot_hi - slot_lo) * (int64_t)args.n_chunks;
     const uint4* __restrict__ uops4 = reinterpret_cast<const uint4*>(args.uops);
 
-    for (;;) {
+    for (int round = 0;; ++round) {
         unsigned long long item = 0;
-        if (lane == 0) item = atomicAdd(args.counter, 1ull);
-        item = __shfl_sync(0xffffffffu, item, 0);
+        if (plain) {
+            if (round > 0) break;
+            item = (unsigned long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        } else {
+            if (lane == 0) item = atomicAdd(args.counter, 1ull);
+            item = __shfl_sync(0xffffffffu, item, 0);
+        }
         if ((int64_t)item >= total_items) break;
-        const WideItem w = resolve_item(args, item);
+        const WideItem w = resolve_item(args, item, slot_lo);
+        if (plain && args.interp_len != nullptr && args.interp_len[w.prog] < 0) continue;   // a dedup copy
         // folded programs are packed against the end of their slot (fold.cuh)
         const int64_t L = args.interp_len ? (int64_t)args.interp_len[w.prog]
                                           : args.eff_off[w.prog + 1] - args.eff_off[w.prog];
         const int64_t p0 = args.eff_off[w.prog + 1] - L;
         const uint4* __restrict__ pw = uops4 + p0;
-        const uint32_t livein = (MODE == kModeTrace || args.livein == nullptr) ? (1u << NR) - 1u
-                                                                              : args.livein[w.prog];
+        // live-in registers (loaded into slots 0..m-1 in register order) and
+        // the output value's slot; a trace uses the ISA's layout
+        const bool arch = MODE == kModeTrace || args.livein == nullptr;
+        const uint32_t lv = arch ? (1u << NSLOT) - 1u : args.livein[w.prog];
+        const uint32_t live_regs = arch ? lv : livein_regs(lv);
+        const uint32_t out_addr = base + (arch ? (uint32_t)args.output_reg : livein_out_slot(lv)) * S;
+        const int64_t nwin = (L + 31) / 32;
+        const bool resident = nwin <= 2;
+        if (resident) {
+            for (int64_t wi = 0; wi < nwin; ++wi) stage_window(wi == 0 ? stage0 : stage1, pw, L, wi, lane);
+        } else {
+            stage_window(stage0, pw, L, 0, lane);
+        }
+        int64_t gw = 0;   // windows of this item streamed so far (stage = gw & 1)
 
         float ks = 0.0f, kc = 0.0f;
         double big = 0.0;
@@ -236,9 +313,10 @@ interp_wide_kernel(InterpArgs args) {
         for (int64_t cb = w.cbeg; cb < w.cend; cb += kPass) {
             // Case of element q*V+e of this lane: cb + (q*32 + lane)*V + e.
             const int64_t c0 = cb + (int64_t)lane * V;
-            // Only the registers the program reads before writing them are
-            // initialised (all of them for a register trace).
-            for (uint32_t m = livein; m != 0u; m &= m - 1u) {
+            // Only the values the program reads before writing them are
+            // initialised (all registers for a register trace).
+            uint32_t slot_addr = base;
+            for (uint32_t m = live_regs; m != 0u; m &= m - 1u) {
                 const int f = __ffs(m) - 1;
                 float v[K];
                 if (f < w.num_inputs) {
@@ -253,19 +331,29 @@ interp_wide_kernel(InterpArgs args) {
 #pragma unroll
                     for (int k = 0; k < K; ++k) v[k] = 0.0f;
                 }
-                WR::store(base + f * S, v);
+                WR::store(slot_addr, v);
+                slot_addr += S;
             }
-            if constexpr (MODE == kModeTrace) wide_trace<NR, K>(args.trace, 0, base, lane);
+            if constexpr (MODE == kModeTrace) wide_trace<NSLOT, K>(args.trace, 0, base, lane);
 
             float a[K];       // result of the last instruction executed
-            uint32_t pt = 0;  // its register's address
+            uint32_t pt = 0;  // its slot's address
 #pragma unroll
             for (int k = 0; k < K; ++k) a[k] = 0.0f;
-            for (int64_t wb = 0; wb < L; wb += 32) {
-                const int64_t n = (L - wb < 32) ? L - wb : 32;
-                const uint4 mine = (lane < n) ? __ldg(pw + wb + lane) : kEnd4;
-                sts_u4(stage + (uint32_t)lane * 16u, mine);
-                __syncwarp();
+            for (int64_t wi = 0; wi < nwin; ++wi) {
+                cp_async_wait_all();
+                __syncwarp();   // the window has landed, and every lane is done with the other stage
+                uint32_t stage;
+                if (resident) {
+                    stage = wi == 0 ? stage0 : stage1;
+                } else {
+                    stage = (gw & 1) ? stage1 : stage0;
+                    const bool last = wi + 1 == nwin;
+                    if (!last || cb + kPass < w.cend)
+                        stage_window((gw & 1) ? stage0 : stage1, pw, L, last ? 0 : wi + 1, lane);
+                    ++gw;
+                }
+                const int64_t wb = wi * 32;
                 uint32_t sp = stage;
                 if constexpr (MODE == kModeTrace) {
                     // One instruction at a time, the register file dumped after
@@ -274,7 +362,7 @@ interp_wide_kernel(InterpArgs args) {
                         uint4 u = lds_u4(sp);
                         while ((int32_t)u.w >= 0) {
                             WideOps<K, PROFILE>::run(u.w & 15u, base + u.x, base + u.y, base + u.z, u.y);
-                            wide_trace<NR, K>(args.trace, wb + (sp - stage) / 16u + 1, base, lane);
+                            wide_trace<NSLOT, K>(args.trace, wb + (sp - stage) / 16u + 1, base, lane);
                             sp += 16u;
                             u = lds_u4(sp);
                         }
@@ -289,7 +377,7 @@ interp_wide_kernel(InterpArgs args) {
                         }
                         slow_op<K, PROFILE>(u.w & 7u, b, b, a);
                         WR::store(base + u.z, a);
-                        wide_trace<NR, K>(args.trace, wb + (sp - stage) / 16u + 1, base, lane);
+                        wide_trace<NSLOT, K>(args.trace, wb + (sp - stage) / 16u + 1, base, lane);
                         sp += 16u;
                     }
                 } else {
@@ -320,12 +408,10 @@ interp_wide_kernel(InterpArgs args) {
                         cur = next;
                     }
                 }
-                __syncwarp();
             }
-            // The output register: the last result when the last instruction
-            // wrote it (never stored), else the register file.
+            // The output: the last result when the last instruction wrote the
+            // output's slot (never stored), else the register file.
             float o[K];
-            const uint32_t out_addr = base + (uint32_t)args.output_reg * S;
             if (MODE != kModeTrace && L > 0 && pt == out_addr) {
 #pragma unroll
                 for (int k = 0; k < K; ++k) o[k] = a[k];
@@ -392,6 +478,8 @@ interp_wide_kernel(InterpArgs args) {
             }
             if constexpr (MODE == kModeTrace) break;
         }
+        cp_async_wait_all();   // nothing of this item may still be landing in a stage
+        __syncwarp();
 
         if constexpr (MODE == kModeFitness) {
             double sse;

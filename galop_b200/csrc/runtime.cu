@@ -69,6 +69,13 @@ size_t interp_smem_bytes(const galop_ctx* ctx, int k, int wpb) {
     return (size_t)(32 * wpb + 32) * ctx->isa.num_registers * k * sizeof(float);
 }
 
+// The wide interpreter with an NSLOT-slot register file (8 or 16): the
+// same kernels serve both ISAs, since renamed micro-ops address slots.
+const void* kernel_for_slots(const galop_ctx* ctx, int k, int mode, int nslot) {
+    if (nslot == 8) return interp_kernel_nr8(k, 3, ctx->isa.profile, ctx->opt.reduce, mode);
+    return interp_kernel_nr16(k, 3, ctx->isa.profile, ctx->opt.reduce, mode);
+}
+
 const void* kernel_for(const galop_ctx* ctx, int k, int mode) {
     const int reduce = ctx->opt.reduce;
     const int dispatch = pick_dispatch(ctx);
@@ -168,7 +175,7 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
     if (ctx->flagged) {
         FoldParams fp{ctx->isa.profile, ctx->isa.num_registers, ctx->isa.output_reg,
                       7u + (uint32_t)__builtin_ctz((unsigned)pick_k(ctx)), ctx->num_inputs, nullptr, nullptr,
-                      ctx->folded ? 1 : 0};
+                      ctx->folded ? 1 : 0, sched ? 1 : 0};
         fold_kernel<<<blocks, tpb, 0, s>>>(reinterpret_cast<uint4*>(ctx->uops.p), ctx->eff_off.p, n, fp,
                                            ctx->eff_len.p, ctx->livein.p, ctx->counters.p + 3);
         ctx->launches += 1;
@@ -192,7 +199,7 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
         size_t tmp = ctx->dsort_tmp.cap;
         const uint4* u4 = reinterpret_cast<const uint4*>(ctx->uops.p);
         dedup_hash_kernel<<<blocks, tpb, 0, s>>>(u4, ctx->eff_off.p, ctx->eff_len.p, n, ctx->dkeys.p, ctx->dvals.p,
-                                                 ctx->rep.p, nullptr);
+                                                 ctx->rep.p, nullptr, ctx->livein.p);
         GALOP_CK(cub::DeviceRadixSort::SortPairs(ctx->dsort_tmp.p, tmp, ctx->dkeys.p, ctx->dkeys_sorted.p,
                                                  ctx->dvals.p, ctx->dvals_sorted.p, (int)n, 0, 64, s), "dedup sort");
         dedup_run_start_kernel<<<blocks, tpb, 0, s>>>(ctx->dkeys_sorted.p, n, ctx->dhead.p);
@@ -200,18 +207,26 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
         GALOP_CK(cub::DeviceScan::InclusiveScan(ctx->dsort_tmp.p, tmp, ctx->dhead.p, ctx->dvals.p, cub::Max(), (int)n,
                                                 s), "dedup scan");
         dedup_rep_kernel<<<blocks, tpb, 0, s>>>(ctx->dvals.p, ctx->dvals_sorted.p, n, u4, ctx->eff_off.p,
-                                                ctx->eff_len.p, ctx->rep.p, ctx->counters.p + 4, nullptr);
+                                                ctx->eff_len.p, ctx->rep.p, ctx->counters.p + 4, nullptr,
+                                                ctx->livein.p);
         ctx->launches += 5;
         GALOP_CK(cudaGetLastError(), "dedup launch");
     }
     GALOP_CK(cudaGetLastError(), "pre-pass compact launch");
+    // Register-file classes: with a 16-register ISA, programs whose values
+    // fit in 8 slots lead the order and run on the 8-slot interpreter (half
+    // the shared memory per warp), the rest after them on the 16-slot one.
+    ctx->class_split = sched && n > 1 && ctx->flagged && ctx->isa.num_registers > kSplitSlots &&
+                       ctx->opt.schedule == GALOP_SCHEDULE_PERSISTENT;
     if (sched && n > 1) {
+        const uint32_t* lv = ctx->class_split ? ctx->livein.p : nullptr;
         GALOP_CK(ctx->order.ensure((size_t)n), "alloc order");
         GALOP_CK(ctx->hist.ensure(kOrderBins), "alloc hist");
         GALOP_CK(cudaMemsetAsync(ctx->hist.p, 0, kOrderBins * sizeof(unsigned int), s), "memset hist");
-        order_hist_kernel<<<blocks, tpb, 0, s>>>(ctx->eff_len.p, n, ctx->hist.p, nullptr, 0);
-        order_scan_kernel<<<1, 1024, 0, s>>>(ctx->hist.p, nullptr);
-        order_scatter_kernel<<<blocks, tpb, 0, s>>>(ctx->eff_len.p, n, ctx->hist.p, ctx->order.p, nullptr, 0);
+        order_hist_kernel<<<blocks, tpb, 0, s>>>(ctx->eff_len.p, n, ctx->hist.p, lv, kSplitSlots);
+        order_scan_kernel<<<1, 1024, 0, s>>>(ctx->hist.p, ctx->class_split ? ctx->counters.p + kCounterClassSplit
+                                                                           : nullptr);
+        order_scatter_kernel<<<blocks, tpb, 0, s>>>(ctx->eff_len.p, n, ctx->hist.p, ctx->order.p, lv, kSplitSlots);
         ctx->launches += 3;
         GALOP_CK(cudaGetLastError(), "order launch");
     }
@@ -252,7 +267,8 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
         if (pn < 4 * resident_warps) n_chunks = std::min<int64_t>(passes, (4 * resident_warps + pn - 1) / pn);
         n_chunks = std::max<int64_t>(n_chunks, std::min<int64_t>(passes, (ctx->N + kMaxItemCases - 1) / kMaxItemCases));
     }
-    if (mode != kModeFitness) n_chunks = 1;
+    const bool plain = ctx->opt.schedule == GALOP_SCHEDULE_PLAIN && mode != kModeTrace;
+    if (mode != kModeFitness || plain) n_chunks = 1;
     const int64_t chunk_passes = (passes + n_chunks - 1) / n_chunks;
     const int64_t chunk_cases = chunk_passes * pass;
     n_chunks = std::max<int64_t>(1, (std::max<int64_t>(ctx->N, 1) + chunk_cases - 1) / chunk_cases);
@@ -263,7 +279,8 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
     a.interp_len = ctx->folded ? ctx->eff_len.p : nullptr;
     a.livein = ctx->flagged ? ctx->livein.p : nullptr;
     a.n_skipped = ctx->deduped ? ctx->counters.p + 4 : nullptr;
-    a.order = (sched && n > 1) ? ctx->order.p : nullptr;
+    a.order = (sched && n > 1 && !plain) ? ctx->order.p : nullptr;
+    a.plain = plain ? 1 : 0;
     a.n_programs = n;
     a.n_chunks = (int32_t)n_chunks;
     a.chunk_cases = chunk_cases;
@@ -285,15 +302,34 @@ int run_interp(galop_ctx* ctx, int64_t n, int mode, bool sched, float* d_fitness
         a.partial = ctx->partial.p;
     }
     const int64_t items = n * n_chunks;
-    int64_t blocks = (int64_t)ctx->sm_count * per_sm;
     const int64_t need = (items + wpb - 1) / wpb;
-    if (blocks > need) blocks = std::max<int64_t>(need, 1);
-    GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned long long), s), "memset queue");
-    if (n > 0) {
+    // One launch per register-file class (the 8-slot programs first, then
+    // the rest), or one launch over the whole order.
+    const bool split = ctx->class_split && sched && n > 1 && mode != kModeTrace && pick_dispatch(ctx) == 3;
+    const int parts = split ? 2 : 1;
+    int64_t blocks = 0;
+    for (int part = 0; part < parts && n > 0; ++part) {
+        const void* f = fn;
+        size_t sm = smem;
+        int psm = per_sm;
+        if (split && part == 0) {
+            f = kernel_for_slots(ctx, k, mode, kSplitSlots);
+            sm = wide_smem_bytes(kSplitSlots, k, wpb);
+            GALOP_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "smem attribute");
+            GALOP_CK(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared), "smem carveout");
+            GALOP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&psm, f, threads, sm), "occupancy");
+            if (psm < 1) psm = 1;
+        }
+        a.class_split = split ? ctx->counters.p + kCounterClassSplit : nullptr;
+        a.class_part = part;
+        int64_t b = (int64_t)ctx->sm_count * psm;
+        if (b > need || plain) b = std::max<int64_t>(need, 1);   // plain: one warp per program
+        GALOP_CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned long long), s), "memset queue");
         void* params[] = {&a};
-        GALOP_CK(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(threads), params, smem, s),
-                 "interpreter launch");
+        GALOP_CK(cudaLaunchKernel(f, dim3((unsigned)b), dim3(threads), params, sm, s), "interpreter launch");
         ctx->launches += 1;
+        blocks = std::max(blocks, b);
     }
     ctx->stats.cases_per_lane = k;
     ctx->stats.warps_per_block = wpb;
@@ -469,6 +505,7 @@ int galop_create(const galop_options* opt, galop_ctx** out) {
     if (opt->reduce < GALOP_REDUCE_KAHAN32 || opt->reduce > GALOP_REDUCE_ORDERED) return GALOP_E_INVALID;
     if (opt->objective != GALOP_OBJECTIVE_MSE && opt->objective != GALOP_OBJECTIVE_R2) return GALOP_E_INVALID;
     if (opt->dispatch != 2 && opt->dispatch != 3) return GALOP_E_INVALID;
+    if (opt->schedule != GALOP_SCHEDULE_PERSISTENT && opt->schedule != GALOP_SCHEDULE_PLAIN) return GALOP_E_INVALID;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();

@@ -378,6 +378,42 @@ def many_populations(seed: int = 4, n_pops: int = 64, size_lo: int = 1000, size_
     return isa, X, y, pops
 
 
+def serving_run_specs(seed: int = 5, n_runs: int = 256, cases_lo: int = 256, cases_hi: int = 1 << 20,
+                      pop_lo: int = 1000, pop_hi: int = 1 << 18, len_lo: int = 8, len_hi: int = 512):
+    """Shapes of independent GP runs for the serving loop (cases log-uniform,
+    1-8 features, population log-uniform, lengths U[len_lo, len_hi]) and a
+    seed for each; serving_run_data materialises one."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_runs):
+        specs.append({"n_cases": int(log_uniform_lengths(rng, 1, cases_lo, cases_hi)[0]),
+                      "num_inputs": int(rng.integers(1, 9)),
+                      "programs": int(log_uniform_lengths(rng, 1, pop_lo, pop_hi)[0]),
+                      "len_lo": len_lo, "len_hi": len_hi, "seed": seed * 100003 + i})
+    return specs
+
+
+def serving_run_data(spec: dict):
+    """(X, y, (words, offsets)) of one serving run: X U[-1,1], y a random
+    12-effective-instruction program, uniform random words (REF ISA, 16
+    registers)."""
+    rng = np.random.default_rng(spec["seed"])
+    isa = IsaSpec(PROFILE_REF, 16)
+    X = rng.uniform(-1.0, 1.0, (spec["n_cases"], spec["num_inputs"])).astype(np.float32)
+    y, _ = regression_target(rng, X, isa, 12)
+    lens = uniform_lengths(rng, spec["programs"], spec["len_lo"], spec["len_hi"])
+    return X, y, random_population(rng, lens, isa.num_registers)
+
+
+def vary_words(rng, words: np.ndarray, frac: float, num_registers: int) -> None:
+    """Redraw a fraction of the words in place (a next generation's
+    variation, for serving workloads)."""
+    k = int(words.size * frac)
+    if k:
+        idx = rng.integers(0, words.size, size=k)
+        words[idx] = random_words(rng, k, num_registers)
+
+
 def serving_runs(seed: int = 5, n_runs: int = 256, cases_lo: int = 256, cases_hi: int = 1 << 20,
                  pop_lo: int = 1000, pop_hi: int = 1 << 18, len_lo: int = 8, len_hi: int = 512,
                  generations: int = 1):

@@ -77,6 +77,18 @@ typedef enum {
  *         (Fitness::r2_to_fitness :93-97).                                  */
 typedef enum { GALOP_OBJECTIVE_MSE = 0, GALOP_OBJECTIVE_R2 = 1 } galop_objective;
 
+/* How the interpreter's work is scheduled on the GPU.
+ *   PERSISTENT : one grid of resident warps pulls (program, case chunk)
+ *                items from a device queue, longest interpreted program
+ *                first; long case ranges are split into chunks (default).
+ *   PLAIN      : the reference's launch shape (src/EvaluatorCuda.cu:433-441):
+ *                one warp per program over all its cases, programs in
+ *                population order, no queue and no case chunking.  Same
+ *                pre-pass, folding and dedup; results equal PERSISTENT's
+ *                within the reduction mode's tolerance (bit for bit in
+ *                ORDERED mode).                                             */
+typedef enum { GALOP_SCHEDULE_PERSISTENT = 0, GALOP_SCHEDULE_PLAIN = 1 } galop_schedule;
+
 typedef struct {
     int32_t profile;          /* galop_profile                                  */
     int32_t num_registers;    /* 8 or 16 (src/LGPConfig.h:132-140)              */
@@ -101,7 +113,7 @@ typedef struct {
     int32_t dedup;            /* 1: programs whose interpreted code is identical
                                  are interpreted once and share the fitness
                                  (dispatch 3, intron pass on; default 1)     */
-    int32_t reserved[1];
+    int32_t schedule;         /* galop_schedule (default PERSISTENT)            */
 } galop_options;
 
 typedef struct galop_ctx galop_ctx;
