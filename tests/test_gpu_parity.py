@@ -225,7 +225,7 @@ def test_prepass_on_off_and_tile_shapes_bitwise(native):
     for pre in (True, False):
         for k in (1, 2, 4, 8):
             for wpb in (1, 4, 8):
-                for disp in (0, 1, 2, 3):
+                for disp in (2, 3):
                     with g.Evaluator(num_registers=16, intron_prepass=pre, cases_per_lane=k, warps_per_block=wpb,
                                      reduce=g.REDUCE_ORDERED, dispatch=disp) as ev:
                         outs = ev.case_outputs(wl.words, wl.offsets, ds)
