@@ -199,15 +199,18 @@ __device__ __forceinline__ void unary_op(uint32_t op, const float (&b)[K], float
     }
 }
 
-// Launch bounds: at most GALOP_WIDE_MAX_THREADS threads per block and at
-// least GALOP_WIDE_MIN_BLOCKS blocks per SM, which caps the registers per
-// thread.
-#ifndef GALOP_WIDE_MAX_THREADS
-#define GALOP_WIDE_MAX_THREADS 256
-#endif
-#ifndef GALOP_WIDE_MIN_BLOCKS
-#define GALOP_WIDE_MIN_BLOCKS 3
-#endif
+// Launch bounds: at most 256 threads per block and at least kMinBlocks
+// blocks of 256 threads per SM, which caps the registers per thread.  The
+// 8-slot instance needs 5,152 bytes of shared memory per warp at K = 4, so
+// 40 warps fit on an SM; 5 blocks of 8 warps cap it at 48 registers per
+// thread, which those 40 warps need (65,536 / (40 x 32) = 51).  The 16-slot
+// instance fits 24 warps by shared memory, which its uncapped register use
+// already allows.
+template <int NSLOT>
+struct WideBounds {
+    static constexpr int kMaxThreads = 256;
+    static constexpr int kMinBlocks = NSLOT <= 8 ? 5 : 3;
+};
 
 // Asynchronous copy of one 16-byte micro-op into shared memory (cached in
 // L2 only), and the waits.
@@ -241,7 +244,7 @@ __device__ __forceinline__ void stage_window(uint32_t st, const uint4* __restric
 // pass) copied with cp.async into the other stage while the current one
 // runs.
 template <int NSLOT, int K, int PROFILE, int REDUCE, int MODE>
-__global__ void __launch_bounds__(GALOP_WIDE_MAX_THREADS, GALOP_WIDE_MIN_BLOCKS)
+__global__ void __launch_bounds__(WideBounds<NSLOT>::kMaxThreads, WideBounds<NSLOT>::kMinBlocks)
 interp_wide_kernel(InterpArgs args) {
     extern __shared__ float4 galop_smem4[];
     using WR = WideRegs<K>;
