@@ -267,9 +267,9 @@ def cpu_reference_rate(wl, seconds: float, threads: int, batch: int = 0):
         evaluate = lambda w, o: orc.evaluate_csr(w, o, wl.X, wl.y, threads=threads)  # noqa: E731
     orc = Oracle(0, 16)
     if batch <= 0:
-        # about a second of work per batch on these threads
+        # a few programs per thread and about a second of work per call
         raw_per_prog = float(wl.offsets[-1]) / max(wl.n_programs, 1)
-        batch = int(max(threads, min(4096, 4e8 * threads / max(raw_per_prog * wl.n_cases, 1.0))))
+        batch = int(threads * max(4, min(256, 4e8 / max(raw_per_prog * wl.n_cases, 1.0))))
     done_progs, ops, t_total = 0, 0.0, 0.0
     start = 0
     while t_total < seconds:

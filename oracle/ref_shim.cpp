@@ -104,7 +104,7 @@ void ref_evaluate_csr(const uint32_t* words, const int64_t* offsets, int64_t n, 
     Dataset d = make_dataset(inputs, targets, n_cases, num_inputs);
 #ifdef _OPENMP
     if (threads < 1) threads = omp_get_max_threads();
-    #pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
+    #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
 #endif
     for (int64_t i = 0; i < n; ++i) {
         ProgramView pv{words + offsets[i], (int)(offsets[i + 1] - offsets[i])};
