@@ -143,6 +143,16 @@ int run_prepass(galop_ctx* ctx, const Src& src, int64_t n, int64_t raw_words_tot
     const size_t per = fmt.wide ? 4 : 1;
     if (ctx->uops.cap < (size_t)std::max<int64_t>(raw_words_total, 1) * per) {
         bool exact = strip && n > 0 && bad == nullptr;
+        if (!exact && strip && n > 0) {
+            // A buffer for the raw total that would take more than half the
+            // free device memory is sized exactly instead (one wait), so
+            // that very large populations still fit.
+            size_t free_b = 0, total_b = 0;
+            if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+                (size_t)raw_words_total * per * sizeof(uint32_t) > free_b / 2)
+                exact = true;
+            cudaGetLastError();
+        }
         if (!exact) {
             // Sized for the raw total without waiting; only when that does
             // not fit is the effective total read back after all.

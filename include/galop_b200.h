@@ -320,7 +320,9 @@ GALOP_API int galop_evaluate_csr(galop_ctx* ctx, const uint32_t* words, const in
  * knows it (the size of d_words).  Work is ordered on `stream` (a
  * cudaStream_t, or NULL for the context's own stream) and the call returns
  * without waiting for the device; it only blocks when a working buffer must
- * grow (the first call, or a larger population).  The offsets are checked on
+ * grow (the first call, or a larger population), and waits once for the
+ * effective instruction count when a buffer sized for total_words would take
+ * more than half the free device memory.  The offsets are checked on
  * the device before any word is read: if d_offsets[0] != 0, an offset
  * decreases, a program is longer than 2^30 words, or d_offsets[n_programs]
  * != total_words, no word is read, every d_fitness (and d_sse) is NaN, and
