@@ -873,8 +873,14 @@ def run_capacity(args):
         ev.set_dataset(ds)
         w, off, fit = population(P0)
         ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P0, P0 * L, fit.data_ptr())
-        ev.synchronize()
+        st0 = ev.stats
         used = before - torch.cuda.mem_get_info(dev)[0]
+        # At this size the device call sizes its micro-op buffer for the raw
+        # words (no wait); at the largest population it sizes it exactly
+        # (the raw-sized buffer would exceed half the free memory), so the
+        # footprint is extrapolated with the exact size.
+        per_uop = 16 if dispatch == 3 else 4
+        used += (st0.eff_instructions - P0 * L) * per_uop
         per_prog = used / P0
         del w, off, fit
         ev.close()
