@@ -203,13 +203,14 @@ __device__ __forceinline__ void unary_op(uint32_t op, const float (&b)[K], float
 // blocks of 256 threads per SM, which caps the registers per thread.  The
 // 8-slot instance needs 5,152 bytes of shared memory per warp at K = 4, so
 // 40 warps fit on an SM; 5 blocks of 8 warps cap it at 48 registers per
-// thread, which those 40 warps need (65,536 / (40 x 32) = 51).  The 16-slot
-// instance fits 24 warps by shared memory, which its uncapped register use
-// already allows.
-template <int NSLOT>
+// thread, which those 40 warps need (65,536 / (40 x 32) = 51).  At K = 8 it
+// needs 9,248 bytes per warp (24 warps), and the 16-slot instance fits at
+// most 24 warps by shared memory at any K, which 3 blocks' cap of 85
+// registers per thread allows.
+template <int NSLOT, int K>
 struct WideBounds {
     static constexpr int kMaxThreads = 256;
-    static constexpr int kMinBlocks = NSLOT <= 8 ? 5 : 3;
+    static constexpr int kMinBlocks = (NSLOT <= 8 && K <= 4) ? 5 : 3;
 };
 
 // Asynchronous copy of one 16-byte micro-op into shared memory (cached in
@@ -244,7 +245,7 @@ __device__ __forceinline__ void stage_window(uint32_t st, const uint4* __restric
 // pass) copied with cp.async into the other stage while the current one
 // runs.
 template <int NSLOT, int K, int PROFILE, int REDUCE, int MODE>
-__global__ void __launch_bounds__(WideBounds<NSLOT>::kMaxThreads, WideBounds<NSLOT>::kMinBlocks)
+__global__ void __launch_bounds__(WideBounds<NSLOT, K>::kMaxThreads, WideBounds<NSLOT, K>::kMinBlocks)
 interp_wide_kernel(InterpArgs args) {
     extern __shared__ float4 galop_smem4[];
     using WR = WideRegs<K>;
