@@ -96,6 +96,12 @@ struct galop_batch {
     const void* interp_fn = nullptr;
     int threads = 0, grid = 0;
     size_t smem = 0;
+    // register-file classes: programs whose renamed values fit kSplitSlots
+    // slots run first in the smaller-footprint interpreter, the rest after
+    bool split = false;
+    const void* interp_fn8 = nullptr;
+    int grid8 = 0;
+    size_t smem8 = 0;
     UopFormat fmt{};                  // micro-op form of the chosen interpreter
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -103,6 +109,11 @@ struct galop_batch {
     int launches = 0;
     bool pending = false;
 };
+
+// Batch counters: [0] work queue, [1..5] the pre-pass totals the
+// statistics read, [6] programs of the first register-file class, [7] the
+// first work item of the second class.
+constexpr int kBatchCounters = 8;
 
 #define B_CK(call, what)                                              \
     do {                                                              \
@@ -166,6 +177,21 @@ int plan(galop_batch* b) {
     per_sm = std::max(per_sm, 1);
     const int64_t need = (b->n_items + wpb - 1) / wpb;
     b->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->sm_count * per_sm, need));
+    b->split = dispatch == 3 && b->fmt.wide && ctx->opt.intron_prepass && ctx->isa.num_registers > kSplitSlots;
+    if (b->split) {
+        b->interp_fn8 = kernel_for_slots(ctx, k, kModeFitness, kSplitSlots);
+        if (!b->interp_fn8) return ctx->fail(GALOP_E_INVALID, "no batched interpreter for this configuration");
+        b->smem8 = wide_smem_bytes(kSplitSlots, k, wpb);
+        B_CK(cudaFuncSetAttribute(b->interp_fn8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem8),
+             "smem attr");
+        B_CK(cudaFuncSetAttribute(b->interp_fn8, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared), "carveout");
+        int per_sm8 = 0;
+        B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm8, b->interp_fn8, b->threads, b->smem8),
+             "occupancy");
+        per_sm8 = std::max(per_sm8, 1);
+        b->grid8 = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->sm_count * per_sm8, need));
+    }
     b->planned_n.resize(n_pops);
     for (int p = 0; p < n_pops; ++p) b->planned_n[p] = b->pops[p].n;
     b->stats.cases_per_lane = k;
@@ -181,7 +207,7 @@ int enqueue(galop_batch* b) {
     cudaStream_t s = b->stream;
     const int64_t G = b->G;
     b->launches = 0;
-    B_CK(cudaMemsetAsync(b->counters.p, 0, 6 * sizeof(unsigned long long), s), "memset counters");
+    B_CK(cudaMemsetAsync(b->counters.p, 0, kBatchCounters * sizeof(unsigned long long), s), "memset counters");
     B_CK(cudaMemsetAsync(b->hist.p, 0, kOrderBins * sizeof(unsigned int), s), "memset hist");
     if (G == 0) return GALOP_OK;
     const int tpb = 256;
@@ -229,9 +255,12 @@ int enqueue(galop_batch* b) {
         b->launches += 5;
     }
     batch_key_kernel<<<blocks, tpb, 0, s>>>(b->layout.p, b->prog_pop.p, b->eff_len.p, G, b->key.p);
-    order_hist_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p, nullptr, 0);
-    order_scan_kernel<<<1, 1024, 0, s>>>(b->hist.p, nullptr);
-    order_scatter_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p, b->order.p, nullptr, 0);
+    // longest first; with the class split, the first register-file class
+    // before the second (counters[6] = its program count)
+    const uint32_t* cls = b->split ? b->livein.p : nullptr;
+    order_hist_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p, cls, kSplitSlots);
+    order_scan_kernel<<<1, 1024, 0, s>>>(b->hist.p, b->split ? b->counters.p + 6 : nullptr);
+    order_scatter_kernel<<<blocks, tpb, 0, s>>>(b->key.p, G, b->hist.p, b->order.p, cls, kSplitSlots);
     batch_item_count_kernel<<<blocks, tpb, 0, s>>>(b->order.p, b->prog_pop.p, b->chunks_of_pop.p, b->key.p, G,
                                                    b->cnt.p);
     scan_tile_sums_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s>>>(b->cnt.p, G, b->tiles.p);
@@ -240,6 +269,10 @@ int enqueue(galop_batch* b) {
     batch_item_fill_kernel<<<blocks, tpb, 0, s>>>(b->order.p, b->cnt.p, b->item_off.p, G, b->items.p,
                                                   b->first_item.p);
     b->launches += 16;
+    if (b->split) {
+        batch_split_items_kernel<<<1, 1, 0, s>>>(b->counters.p + 6, b->item_off.p, b->counters.p + 7);
+        b->launches += 1;
+    }
     B_CK(cudaGetLastError(), "batch pre-pass launch");
 
     InterpArgs a{};
@@ -259,6 +292,17 @@ int enqueue(galop_batch* b) {
     a.n_items = b->n_items;
     a.n_items_dev = dedup ? b->item_off.p + G : nullptr;
     void* params[] = {&a};
+    if (b->split) {
+        // items [0, counters[7]) in the kSplitSlots-slot interpreter, then the
+        // rest, each launch with its own work-queue counter reset
+        a.class_split = b->counters.p + 7;
+        a.class_part = 0;
+        B_CK(cudaLaunchKernel(b->interp_fn8, dim3((unsigned)b->grid8), dim3(b->threads), params, b->smem8, s),
+             "batched interpreter launch");
+        B_CK(cudaMemsetAsync(b->counters.p, 0, sizeof(unsigned long long), s), "memset queue");
+        a.class_part = 1;
+        b->launches += 1;
+    }
     B_CK(cudaLaunchKernel(b->interp_fn, dim3((unsigned)b->grid), dim3(b->threads), params, b->smem, s),
          "batched interpreter launch");
     batch_finalize_kernel<<<blocks, tpb, 0, s>>>(b->descs.p, b->prog_pop.p, b->first_item.p, b->partial.p, G);
@@ -388,7 +432,7 @@ int allocate(galop_batch* b, int64_t words, int64_t offs, int64_t progs, int64_t
     if (e == cudaSuccess) e = b->tiles.ensure(T1);
     if (e == cudaSuccess) e = b->items.ensure(I1);
     if (e == cudaSuccess) e = b->partial.ensure(I1);
-    if (e == cudaSuccess) e = b->counters.ensure(6);
+    if (e == cudaSuccess) e = b->counters.ensure(kBatchCounters);
     b->dedup = ctx->opt.dedup && b->fmt.wide && ctx->opt.intron_prepass && progs > 1;
     if (b->dedup) {
         if (e == cudaSuccess) e = b->dkeys.ensure(G1);

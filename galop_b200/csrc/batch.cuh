@@ -59,7 +59,8 @@ static __global__ void batch_rebase_kernel(const PopLayout* __restrict__ pops, i
 }
 
 // Sort key: log-scale bin of interpreted work (effective length x cases),
-// larger key = more work.  Bins of width 2^(1/64) over [1, 2^63].
+// larger key = more work.  Bins of width 2^(1/48): keys up to 2046 cover
+// work below 2^42, and each register-file class of the order holds 2047.
 static __global__ void batch_key_kernel(const PopLayout* __restrict__ pops, const int32_t* __restrict__ prog_pop,
                                         const int32_t* __restrict__ eff_len, int64_t n_total,
                                         int32_t* __restrict__ key) {
@@ -70,8 +71,8 @@ static __global__ void batch_key_kernel(const PopLayout* __restrict__ pops, cons
         return;
     }
     const double work = (double)eff_len[g] * (double)pops[prog_pop[g]].n_cases;
-    int k = work >= 1.0 ? (int)(log2(work) * 64.0) + 1 : 0;
-    key[g] = k < 4094 ? k : 4094;
+    int k = work >= 1.0 ? (int)(log2(work) * 48.0) + 1 : 0;
+    key[g] = k < 2046 ? k : 2046;
 }
 
 // Work items per program, by position in the order.
@@ -97,6 +98,15 @@ static __global__ void batch_item_fill_kernel(const int32_t* __restrict__ order,
     const int64_t o = item_off[i];
     for (int c = 0; c < cnt[i]; ++c) items[o + c] = ((unsigned long long)g << 20) | (unsigned long long)c;
     first_item[g] = o;
+}
+
+// The first work item of the second register-file class: the order holds
+// the n0 = *class0 programs of the first class first, so their items are
+// items [0, item_off[n0]).  One thread.
+static __global__ void batch_split_items_kernel(const unsigned long long* __restrict__ class0,
+                                                const int64_t* __restrict__ item_off,
+                                                unsigned long long* __restrict__ split_item) {
+    *split_item = (unsigned long long)item_off[*class0];
 }
 
 // Copies left out by dedup take their representative's results (same

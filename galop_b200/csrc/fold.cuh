@@ -7,7 +7,7 @@
 // operands are constants.  An instruction all of whose operands are such
 // known values computes the same number for every case, so it is evaluated
 // once here -- with the very operations the interpreter would use (apply_op:
-// __fadd_rn, IEEE division, sinf, ... on this device), hence the same bits --
+// __fadd_rn, IEEE division, galop_sinf, ... on this device), hence the same bits --
 // and becomes a broadcast micro-op (dest = that constant).  A second,
 // backward liveness pass then drops instructions whose results no remaining
 // instruction reads (broadcasts read nothing) and packs the survivors

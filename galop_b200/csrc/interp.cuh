@@ -87,10 +87,12 @@ struct InterpArgs {
     // program w over all its cases (n_chunks 1, no order, no queue), and a
     // dedup copy (interp_len < 0) is skipped.
     int32_t plain;
-    // Register-file classes (single population, wide kernel): the order
-    // lists the programs whose values fit in 8 slots first; *class_split is
-    // their count.  class_part 0 covers those slots of the order, 1 the rest.
-    // class_split null: one launch covers the whole order.
+    // Register-file classes (wide kernel): the order lists the programs
+    // whose values fit in 8 slots first.  Single population: *class_split is
+    // their count, class_part 0 covers those slots of the order, 1 the rest.
+    // Batched: their work items come first in `items`, *class_split is the
+    // first item of the others, class_part 0 covers the items before it, 1
+    // the rest.  class_split null: one launch covers everything.
     const unsigned long long* class_split;
     int32_t class_part;
 };
@@ -181,12 +183,10 @@ __device__ __forceinline__ void slow_op(uint32_t op, const float (&a)[K], const 
             for (int k = 0; k < K; ++k) t[k] = (b[k] != 0.0f) ? __fdiv_rn(a[k], b[k]) : 1.0f;
             break;
         case kSin:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = sinf(b[k]);
+            galop_trig_k<K>(b, t, 0u);
             break;
         case kCos:
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = cosf(b[k]);
+            galop_trig_k<K>(b, t, 1u);
             break;
         case kOp6:
 #pragma unroll

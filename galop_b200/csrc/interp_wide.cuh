@@ -183,17 +183,12 @@ __device__ __forceinline__ void wide_trace(float* __restrict__ trace, int64_t ro
 }
 
 // The unary ops of the profile on K cases: SIN/COS (REF), SIN/COS/EXP/LOG
-// (BJ), with the CUDA math library as everywhere else.
+// (BJ); sine and cosine from trig.cuh, EXP/LOG from the CUDA math library.
 template <int K, int PROFILE>
 __device__ __forceinline__ void unary_op(uint32_t op, const float (&b)[K], float (&t)[K]) {
     if constexpr (PROFILE == kProfileRef) {
-        if (op == kSin) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = sinf(b[k]);
-        } else {
-#pragma unroll
-            for (int k = 0; k < K; ++k) t[k] = cosf(b[k]);
-        }
+        if (op == kSin) galop_trig_k<K>(b, t, 0u);
+        else galop_trig_k<K>(b, t, 1u);
     } else {
         slow_op<K, PROFILE>(op, b, b, t);
     }
@@ -269,13 +264,21 @@ interp_wide_kernel(InterpArgs args) {
     const int64_t n_work = args.n_skipped ? args.n_programs - (int64_t)*args.n_skipped : args.n_programs;
     // the slots of the order this launch covers (one register-file class)
     int64_t slot_lo = 0, slot_hi = n_work;
-    if (args.class_split != nullptr) {
+    if (args.class_split != nullptr && args.pops == nullptr) {
         const int64_t n0 = (int64_t)*args.class_split;
         if (args.class_part == 0) slot_hi = n0 < n_work ? n0 : n_work;
         else slot_lo = n0 < n_work ? n0 : n_work;
     }
-    const int64_t total_items = args.pops != nullptr ? (args.n_items_dev ? *args.n_items_dev : args.n_items)
-                              : plain ? args.n_programs : (slot_hi - slot_lo) * (int64_t)args.n_chunks;
+    int64_t total_items = args.pops != nullptr ? (args.n_items_dev ? *args.n_items_dev : args.n_items)
+                        : plain ? args.n_programs : (slot_hi - slot_lo) * (int64_t)args.n_chunks;
+    // batched items: the first class's items come first in the item list,
+    // the split is the first item of the second class
+    int64_t item_lo = 0;
+    if (args.pops != nullptr && args.class_split != nullptr) {
+        const int64_t b = (int64_t)*args.class_split < total_items ? (int64_t)*args.class_split : total_items;
+        if (args.class_part == 0) total_items = b;
+        else item_lo = b;
+    }
     const uint4* __restrict__ uops4 = reinterpret_cast<const uint4*>(args.uops);
 
     for (int round = 0;; ++round) {
@@ -284,7 +287,7 @@ interp_wide_kernel(InterpArgs args) {
             if (round > 0) break;
             item = (unsigned long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
         } else {
-            if (lane == 0) item = atomicAdd(args.counter, 1ull);
+            if (lane == 0) item = (unsigned long long)item_lo + atomicAdd(args.counter, 1ull);
             item = __shfl_sync(0xffffffffu, item, 0);
         }
         if ((int64_t)item >= total_items) break;

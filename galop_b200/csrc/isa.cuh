@@ -14,6 +14,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "trig.cuh"
+
 namespace galop {
 
 constexpr int kMaxRegisters = 16;
@@ -127,7 +129,9 @@ __device__ __forceinline__ bool uop_is_const(uint32_t u) { return (u >> 31) != 0
 
 // Op semantics, src/ISA.h:219-231 (REF) and the BJ profile's EXP/LOG.
 // Explicit round-to-nearest intrinsics: no FMA contraction, IEEE division,
-// matching the CPU build (ISO C++, no contraction, SSE2 arithmetic).
+// matching the CPU build (ISO C++, no contraction, SSE2 arithmetic).  SIN
+// and COS are trig.cuh's (within 1.56 ulp of the exact value, as the C
+// library's are within 1 ulp); EXP and LOG are CUDA's.
 template <int PROFILE>
 __device__ __forceinline__ float apply_op(uint32_t op, float a, float b) {
     switch (op) {
@@ -135,8 +139,8 @@ __device__ __forceinline__ float apply_op(uint32_t op, float a, float b) {
         case kSub: return __fsub_rn(a, b);
         case kMul: return __fmul_rn(a, b);
         case kDiv: return (b != 0.0f) ? __fdiv_rn(a, b) : 1.0f;
-        case kSin: return sinf(b);
-        case kCos: return cosf(b);
+        case kSin: return galop_sinf(b);
+        case kCos: return galop_cosf(b);
         case kOp6:
             if constexpr (PROFILE == kProfileBj) return expf(b);
             else return (a < b) ? 1.0f : 0.0f;

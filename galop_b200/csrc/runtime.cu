@@ -36,10 +36,13 @@ using namespace galop;
 
 namespace galop {
 
+// Cases per lane: the option, else 8 for the 16-byte micro-op interpreter
+// (its loop's dispatch work spread over 8 cases) and 4 for the 32-bit one,
+// whose register file holds all NR registers per lane in shared memory.
 int pick_k(const galop_ctx* ctx) {
     const int k = ctx->opt.cases_per_lane;
     if (k == 1 || k == 2 || k == 4 || k == 8) return k;
-    return 4;
+    return ctx->opt.dispatch == 2 ? 4 : 8;
 }
 
 int pick_wpb(const galop_ctx* ctx) {

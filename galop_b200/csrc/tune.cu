@@ -160,12 +160,12 @@ int galop_autotune(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets
     };
 
     double def_gops = 0.0;
-    if (int rc = time_tile(3, 4, 4, &def_gops)) {
+    if (int rc = time_tile(3, 8, 4, &def_gops)) {
         ctx->opt = saved;
         return rc;
     }
     out->default_gpops = def_gops;
-    int best_d = 3, best_k = 4, best_w = 4;
+    int best_d = 3, best_k = 8, best_w = 4;
     double best = def_gops;
     int measured = 1;
     const int dispatches[] = {3, 2};
@@ -174,7 +174,7 @@ int galop_autotune(galop_ctx* ctx, const uint32_t* words, const int64_t* offsets
     for (int d : dispatches)
         for (int k : ks)
             for (int w : ws) {
-                if (d == 3 && k == 4 && w == 4) continue;
+                if (d == 3 && k == 8 && w == 4) continue;
                 double g = 0.0;
                 if (time_tile(d, k, w, &g) != GALOP_OK) {
                     ctx->err.clear();   // a tile this device cannot run is skipped

@@ -100,7 +100,8 @@ typedef struct {
     int32_t device;           /* CUDA device ordinal                            */
     int32_t intron_prepass;   /* 1: interpret only effective instructions
                                  (src/Introns.h:28-57); outputs unchanged       */
-    int32_t cases_per_lane;   /* 0 = tuned default; else 1, 2, 4 or 8          */
+    int32_t cases_per_lane;   /* 0 = default (8; 4 for dispatch 2); else 1, 2,
+                                 4 or 8                                         */
     int32_t warps_per_block;  /* 0 = tuned default; else 1..8                  */
     int32_t dispatch;         /* interpreter: 3 = shared-memory register file,
                                  16-byte pre-decoded micro-ops, constant
@@ -278,7 +279,7 @@ typedef struct {
     int32_t reserved0;
     int64_t sample_programs;       /* programs in the timed sample            */
     double gpops;                  /* effective GPop/s of the choice (sample) */
-    double default_gpops;          /* the default tile (3, 4, 4) on the sample */
+    double default_gpops;          /* the default tile (3, 8, 4) on the sample */
     char key[320];
 } galop_tune_result;
 

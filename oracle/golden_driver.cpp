@@ -57,7 +57,7 @@ static std::vector<float> driver_constants() {
 #elif defined(GOLDEN_BACKEND_ORACLE)
 extern "C" {
 typedef struct {
-    int32_t profile, num_registers, input_protect, reserved;
+    int32_t profile, num_registers, input_protect, trig;  // trig 0: the C library's sinf/cosf
     const float* constants;
 } orc_isa_t;
 void orc_evaluate_population_dense(const orc_isa_t* isa, const uint32_t* instructions,

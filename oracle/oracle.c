@@ -33,6 +33,15 @@
  *        LOG(b) = (b != 0) ? logf(|b|) : 0.  No reference test covers EXP/LOG:
  *        parity for those two opcodes is unpinned.
  *
+ * Transcendentals: SIN and COS use the C library's sinf/cosf, as the
+ * reference does (orc_isa_t.trig = ORC_TRIG_LIBM).  With ORC_TRIG_DEVICE
+ * they use the device's own functions instead.  Those come from
+ * galop_b200/csrc/trig.cuh, compiled here for the host, where it gives the
+ * same bits as on the GPU.  Every other op is unchanged, so GPU outputs can
+ * be checked bit for bit on programs that use SIN/COS.  How far those
+ * functions are from the exact values is pinned separately, against
+ * correctly rounded results and glibc.
+ *
  * Build: see oracle/Makefile.  Compiled with -O2 -ffp-contract=off and no
  * fast-math so that float arithmetic rounds exactly like the reference's
  * g++ -std=c++20 -O2 build (ISO mode, no FMA contraction, SSE2 arithmetic).
@@ -45,14 +54,20 @@
 #include <omp.h>
 #endif
 
+#include "../galop_b200/csrc/trig.cuh"
+
 enum { ORC_PROFILE_REF = 0, ORC_PROFILE_BJ = 1 };
+enum { ORC_TRIG_LIBM = 0, ORC_TRIG_DEVICE = 1 };
+/* orc_apply_op's `profile` argument: the profile, plus this flag for the
+ * device's sine and cosine. */
+#define ORC_OP_DEVICE_TRIG 0x100
 enum { OP_ADD = 0, OP_SUB, OP_MUL, OP_DIV, OP_SIN, OP_COS, OP_6, OP_7 };
 
 typedef struct {
     int32_t profile;        /* ORC_PROFILE_REF or ORC_PROFILE_BJ             */
     int32_t num_registers;  /* power of two, 2..128                          */
     int32_t input_protect;  /* 1: dest folded into the upper register half   */
-    int32_t reserved;
+    int32_t trig;           /* ORC_TRIG_LIBM or ORC_TRIG_DEVICE (SIN/COS)     */
     const float* constants; /* num_registers entries (pool size == NR)       */
 } orc_isa_t;
 
@@ -64,6 +79,11 @@ int64_t orc_extract_effective(const orc_isa_t* isa, const uint32_t* prog, int64_
 
 /* Output register: r0, or the first scratch register NR/2 under
  * INPUT_PROTECT (src/LGPConfig.h:294-300). */
+/* orc_apply_op's mode word for this configuration. */
+static inline int orc_op_mode(const orc_isa_t* isa) {
+    return isa->profile | (isa->trig == ORC_TRIG_DEVICE ? ORC_OP_DEVICE_TRIG : 0);
+}
+
 int orc_output_reg(const orc_isa_t* isa) {
     return isa->input_protect ? isa->num_registers / 2 : 0;
 }
@@ -93,15 +113,18 @@ int orc_decode(const orc_isa_t* isa, uint32_t w, int32_t* out5) {
     return d.unary;
 }
 
-/* Op semantics, src/ISA.h:219-231 for REF; BJ swaps LT/GT for EXP/LOG. */
+/* Op semantics, src/ISA.h:219-231 for REF; BJ swaps LT/GT for EXP/LOG.
+ * `profile` may carry ORC_OP_DEVICE_TRIG (SIN/COS as on the device). */
 float orc_apply_op(int profile, int op, float a, float b) {
+    const int device_trig = (profile & ORC_OP_DEVICE_TRIG) != 0;
+    profile &= 0xff;
     switch (op) {
         case OP_ADD: return a + b;
         case OP_SUB: return a - b;
         case OP_MUL: return a * b;
         case OP_DIV: return (b != 0.0f) ? a / b : 1.0f;
-        case OP_SIN: return sinf(b);
-        case OP_COS: return cosf(b);
+        case OP_SIN: return device_trig ? galop_sinf(b) : sinf(b);
+        case OP_COS: return device_trig ? galop_cosf(b) : cosf(b);
         case OP_6:
             if (profile == ORC_PROFILE_BJ) return expf(b);
             return (a < b) ? 1.0f : 0.0f;
@@ -154,7 +177,7 @@ static inline float orc_run_case(const orc_isa_t* isa, const orc_ins_t* p, int64
         const orc_ins_t in = p[pc];
         const float a = r[in.src1];
         const float b = in.is_const ? isa->constants[in.src2] : r[in.src2];
-        r[in.dest] = orc_apply_op(isa->profile, in.op, a, b);
+        r[in.dest] = orc_apply_op(orc_op_mode(isa), in.op, a, b);
     }
     return r[orc_output_reg(isa)];
 }
@@ -206,7 +229,7 @@ void orc_trace_case(const orc_isa_t* isa, const uint32_t* prog, int64_t len,
         const orc_ins_t in = orc_decode_word(isa, prog[pc]);
         const float a = r[in.src1];
         const float b = in.is_const ? isa->constants[in.src2] : r[in.src2];
-        r[in.dest] = orc_apply_op(isa->profile, in.op, a, b);
+        r[in.dest] = orc_apply_op(orc_op_mode(isa), in.op, a, b);
         memcpy(state + (size_t)(pc + 1) * nr, r, sizeof(float) * (size_t)nr);
     }
 }
@@ -448,6 +471,52 @@ void orc_extract_effective_csr(const orc_isa_t* isa, const uint32_t* words, cons
     for (int64_t i = 0; i < n_programs; ++i)
         orc_extract_effective(isa, words + offsets[i], offsets[i + 1] - offsets[i], out_words + eff_offsets[i]);
     (void)threads;
+}
+
+/* Accuracy of the device's sine (cosine = 0) or cosine (trig.cuh) over the
+ * floats with bit patterns lo, lo + stride, ... <= hi, against sinl/cosl
+ * rounded to float (the correctly rounded value, up to rare double roundings
+ * in long double) and against the C library's sinf/cosf.  Also checks
+ * sin(-x) = -sin(x) and cos(-x) = cos(x) bit for bit.  out[0..6]: values
+ * checked, largest error in ulps of the exact value, the argument where it
+ * occurs, correctly rounded count, count equal to the C library's, count
+ * above 1 ulp, symmetry violations. */
+static double orc_ulp_error(float y, long double t) {
+    if (isnan(y) || isnan((double)t)) return (isnan(y) && isnan((double)t)) ? 0.0 : 1e30;
+    int e;
+    frexpl(fabsl(t), &e);
+    int ue = e - 24;
+    if (ue < -149) ue = -149;
+    return (double)(fabsl((long double)y - t) / ldexpl(1.0L, ue));
+}
+
+void orc_trig_accuracy(int cosine, uint32_t lo, uint32_t hi, uint32_t stride, double* out) {
+    if (stride == 0) stride = 1;
+    const int64_t n = ((int64_t)hi - (int64_t)lo) / stride + 1;
+    double maxe = 0.0, arg = 0.0;
+    int64_t cr = 0, libm = 0, over1 = 0, asym = 0;
+#pragma omp parallel
+    {
+        double lmax = 0.0, larg = 0.0;
+#pragma omp for schedule(dynamic, 4096) reduction(+ : cr, libm, over1, asym)
+        for (int64_t i = 0; i < n; ++i) {
+            const float x = gt_float((uint32_t)((int64_t)lo + i * (int64_t)stride));
+            const float y = cosine ? galop_cosf(x) : galop_sinf(x);
+            const float yn = cosine ? galop_cosf(-x) : galop_sinf(-x);
+            const long double t = cosine ? cosl((long double)x) : sinl((long double)x);
+            const float g = cosine ? cosf(x) : sinf(x);
+            const double e = orc_ulp_error(y, t);
+            if (!isnan(y)) asym += gt_bits(yn) != (cosine ? gt_bits(y) : (gt_bits(y) ^ 0x80000000u));
+            cr += gt_bits(y) == gt_bits((float)t) || (isnan(y) && isnan((double)t));
+            libm += gt_bits(y) == gt_bits(g) || (isnan(y) && isnan(g));
+            over1 += e > 1.0;
+            if (e > lmax) { lmax = e; larg = x; }
+        }
+#pragma omp critical
+        if (lmax > maxe) { maxe = lmax; arg = larg; }
+    }
+    out[0] = (double)n; out[1] = maxe; out[2] = arg; out[3] = (double)cr; out[4] = (double)libm;
+    out[5] = (double)over1; out[6] = (double)asym;
 }
 
 int orc_max_threads(void) {

@@ -19,11 +19,13 @@ LIB = HERE / "liboracle.so"
 REF_DIR = HERE / "_ref"
 
 PROFILE_REF, PROFILE_BJ = 0, 1
+TRIG_LIBM, TRIG_DEVICE = 0, 1
+_OP_DEVICE_TRIG = 0x100   # orc_apply_op mode flag (oracle.c ORC_OP_DEVICE_TRIG)
 
 
 class OrcIsa(C.Structure):
     _fields_ = [("profile", C.c_int32), ("num_registers", C.c_int32), ("input_protect", C.c_int32),
-                ("reserved", C.c_int32), ("constants", C.POINTER(C.c_float))]
+                ("trig", C.c_int32), ("constants", C.POINTER(C.c_float))]
 
 
 def build(quiet: bool = True) -> None:
@@ -45,14 +47,18 @@ class Oracle:
     _lib: Optional[C.CDLL] = None
 
     def __init__(self, profile: int = PROFILE_REF, num_registers: int = 8, input_protect: bool = False,
-                 constants: Optional[Sequence[float]] = None):
+                 constants: Optional[Sequence[float]] = None, trig: int = TRIG_LIBM):
+        """trig: TRIG_LIBM (SIN/COS by the C library, as the reference) or
+        TRIG_DEVICE (the device's own sine and cosine, galop_b200/csrc/trig.cuh,
+        for bit-for-bit checks of GPU outputs on programs using them)."""
         lib = self.lib()
         if constants is None:
             from galop_b200 import REF_CONSTANTS_8, REF_CONSTANTS_16
             constants = REF_CONSTANTS_16 if num_registers == 16 else REF_CONSTANTS_8
         self.constants = np.ascontiguousarray(constants, dtype=np.float32)
         assert self.constants.shape == (num_registers,)
-        self.isa = OrcIsa(profile, num_registers, int(bool(input_protect)), 0, _p(self.constants, _F32))
+        self.isa = OrcIsa(profile, num_registers, int(bool(input_protect)), int(trig), _p(self.constants, _F32))
+        self.trig = int(trig)
         self.num_registers = num_registers
         self.profile = profile
         self.input_protect = bool(input_protect)
@@ -76,6 +82,7 @@ class Oracle:
                 "orc_sse": (C.c_double, [P(OrcIsa), P(_U32), _I64, P(_F32), P(_F32), C.c_int, _I64]),
                 "orc_evaluate_sr_mse": (C.c_float, [P(OrcIsa), P(_U32), _I64, P(_F32), P(_F32), C.c_int, _I64]),
                 "orc_mse_to_fitness": (C.c_float, [C.c_float]),
+                "orc_trig_accuracy": (None, [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, P(_F64)]),
                 "orc_evaluate_population_csr": (None, [P(OrcIsa), P(_U32), P(_I64), _I64, P(_F32), P(_F32),
                                                        C.c_int, _I64, P(_F32), P(_F64), C.c_int]),
                 "orc_evaluate_population_dense": (None, [P(OrcIsa), P(_U32), P(_U8), _I64, _I64, P(_F32),
@@ -109,14 +116,30 @@ class Oracle:
         unary = self.lib().orc_decode(C.byref(self.isa), word, out)
         return tuple(out) + (unary,)
 
+    @classmethod
+    def trig_accuracy(cls, cosine: bool, lo: float, hi: float, stride: int = 1) -> dict:
+        """The device's sine or cosine (galop_b200/csrc/trig.cuh, host build)
+        over the non-negative floats lo <= x <= hi with bit-pattern stride
+        `stride`, against the correctly rounded value and the C library."""
+        out = np.zeros(7, np.float64)
+        lo_b = int(np.float32(lo).view(np.uint32))
+        hi_b = int(np.float32(hi).view(np.uint32))
+        cls.lib().orc_trig_accuracy(int(bool(cosine)), lo_b, hi_b, stride, _p(out, _F64))
+        n = int(out[0])
+        return {"values": n, "max_ulp": float(out[1]), "at": float(out[2]), "correctly_rounded": int(out[3]) / n,
+                "equal_to_libm": int(out[4]) / n, "over_1ulp": int(out[5]), "asymmetric": int(out[6])}
+
+    def _op_mode(self) -> int:
+        return self.profile | (_OP_DEVICE_TRIG if self.trig == TRIG_DEVICE else 0)
+
     def apply_op(self, op: int, a: float, b: float) -> float:
-        return self.lib().orc_apply_op(self.profile, op, a, b)
+        return self.lib().orc_apply_op(self._op_mode(), op, a, b)
 
     def apply_op_n(self, op: int, a, b) -> np.ndarray:
         a = np.ascontiguousarray(a, dtype=np.float32)
         b = np.ascontiguousarray(b, dtype=np.float32)
         out = np.empty(a.shape[0], dtype=np.float32)
-        self.lib().orc_apply_op_n(self.profile, op, _p(a, _F32), _p(b, _F32), a.shape[0], _p(out, _F32))
+        self.lib().orc_apply_op_n(self._op_mode(), op, _p(a, _F32), _p(b, _F32), a.shape[0], _p(out, _F32))
         return out
 
     def case_outputs(self, prog, inputs, n_cases=None) -> np.ndarray:

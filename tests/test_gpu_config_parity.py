@@ -16,6 +16,10 @@ own vectors and golden histories by tests/test_oracle.py).  Bars:
   be bit-identical wherever all of a program's outputs are, and the
   fitness is held to the reference's own GPU gate (tests/cuda_diff.cu:82:
   |d fitness| < 1e-4, at most 1% of programs over);
+* the same programs against the oracle with the device's own sine and
+  cosine (trig.cuh built for the host, Oracle(trig=TRIG_DEVICE)): every
+  per-case output and every ORDERED fitness bit-identical, so the only
+  difference from the reference is in the SIN/COS results themselves;
 * the production path (intron pass, constant folding, operand forwarding,
   register renaming, 16-byte micro-ops) gives the same bits as the plain
   one-instruction-at-a-time interpreter on the raw programs (dispatch 2,
@@ -166,14 +170,20 @@ def test_config2_sample_ulp_histogram_and_fitness(native, oracle_lib):
     fo, _ = gpu_fitness(wl.words, wl.offsets, ds, g.REDUCE_ORDERED)
     want = o.case_outputs_csr(wl.words, wl.offsets, wl.X)
     wfit, _ = o.evaluate_csr_opt(wl.words, wl.offsets, wl.X, wl.y)
+    od = oracle_lib.Oracle(oracle_lib.PROFILE_REF, 16, trig=oracle_lib.TRIG_DEVICE)
+    dev_ok = same_or_nan(outs, od.case_outputs_csr(wl.words, wl.offsets, wl.X))
+    dfit, dsse = od.evaluate_csr_opt(wl.words, wl.offsets, wl.X, wl.y)
     ieee = effective_ops_ieee(o, wl.words, wl.offsets)
     hist, exact_prog, _ = compare_rows(outs, want)
     report("config2_sample", {"programs": 4096, "cases": 4096, "ieee_only_programs": int(ieee.sum()),
+                              "outputs_differing_from_device_trig_oracle": int((~dev_ok).sum()),
                               "programs_all_outputs_exact": int(exact_prog.sum()),
                               "ulp_histogram_per_case": hist,
                               "fitness_bit_exact_programs": int((bits(fo) == bits(wfit)).sum()),
                               "fitness_over_1e-4": int((np.abs(fo.astype(np.float64) - wfit) > 1e-4).sum())})
     assert np.array_equal(bits(outs), bits(plain))
+    assert dev_ok.all(), int((~dev_ok).sum())
+    assert np.array_equal(bits(fo), bits(dfit))
     assert exact_prog[ieee].all()
     assert np.array_equal(bits(fo)[exact_prog], bits(wfit)[exact_prog])
     assert reference_gate(fo, wfit, 4096)
@@ -212,6 +222,9 @@ def test_long_programs_against_oracle(native, oracle_lib, lo, hi, k, sigma, kind
     else:
         plain = gpu_outputs(words, off, ds, dispatch=2, prepass=False)
         assert np.array_equal(bits(outs), bits(plain))
+        od = oracle_lib.Oracle(oracle_lib.PROFILE_REF, 16, trig=oracle_lib.TRIG_DEVICE)
+        assert same_or_nan(outs, od.case_outputs_csr(words, off, X, effective_only=True)).all()
+        assert np.array_equal(bits(fo), bits(od.evaluate_csr_opt(words, off, X, y, effective_only=True)[0]))
         assert np.array_equal(bits(fo)[exact_prog], bits(wfit)[exact_prog])
         assert reference_gate(fo, wfit, 1024)
 
@@ -220,10 +233,12 @@ def test_long_programs_against_oracle(native, oracle_lib, lo, hi, k, sigma, kind
 def test_trace_replay_long_programs(native, oracle_lib, profile):
     """Programs of 700 to 2,048 instructions: every GPU instruction, fed the
     GPU's own register file, reproduces the CPU's apply_op (bit-exact for
-    IEEE ops, <= 2 ulp for SIN/COS/EXP/LOG); the production path's outputs
-    equal the trace's final output register bit for bit."""
+    IEEE ops and, against the device-trig oracle, for SIN/COS; <= 2 ulp
+    for SIN/COS against the C library and for EXP/LOG); the production
+    path's outputs equal the trace's final output register bit for bit."""
     rng = np.random.default_rng(70 + profile)
     o = oracle_lib.Oracle(profile, 16)
+    od = oracle_lib.Oracle(profile, 16, trig=oracle_lib.TRIG_DEVICE)
     X = rng.uniform(-3, 3, size=(128, 5)).astype(np.float32)
     ds = g.Dataset(X, np.zeros(128, np.float32))
     ieee = {0, 1, 2, 3, 6, 7} if profile == g.PROFILE_REF else {0, 1, 2, 3}
@@ -243,6 +258,8 @@ def test_trace_replay_long_programs(native, oracle_lib, profile):
                     assert same_or_nan(got, want).all(), (L, pc, op)
                 else:
                     assert ulp_dist(got, want).max() <= 2, (L, pc, op)
+                    if op in (4, 5):
+                        assert same_or_nan(got, od.apply_op_n(op, a, b)).all(), (L, pc, op)
             final = ev.case_outputs(prog, np.array([0, L], np.int64))[0][:n]
             assert np.array_equal(bits(final), bits(st[L, o.output_reg]))
 
@@ -254,8 +271,9 @@ def test_config4_magnitudes_kahan32_within_1e6(native, oracle_lib, kind):
     """2^22 cases of 4 features N(0, 10^2), targets a random program scaled
     to ~1e4 plus N(0,1), 192 programs of lengths log-uniform [8,2048]: the
     KAHAN32 fitness (compensated FP32 per lane, FP64 across lanes) is
-    within 1e-6 relative of the FP64 case-order oracle; for IEEE-only
-    programs the ORDERED SSE equals the oracle's bit for bit."""
+    within 1e-6 relative of the FP64 case-order oracle, and the ORDERED SSE
+    equals the oracle's bit for bit (for programs with SIN/COS, the oracle
+    with the device's sine and cosine)."""
     rng = np.random.default_rng(404)
     N = 1 << 22
     X = (rng.standard_normal((N, 4)) * 10.0).astype(np.float32)
@@ -271,10 +289,15 @@ def test_config4_magnitudes_kahan32_within_1e6(native, oracle_lib, kind):
     fo, so = gpu_fitness(words, off, ds, g.REDUCE_ORDERED)
     o = oracle_lib.Oracle(oracle_lib.PROFILE_REF, 16)
     wfit, wsse = o.evaluate_csr_opt(words, off, X, y_full, effective_only=True)
-    # IEEE-only: against the oracle itself; mixed: against the FP64
-    # case-order sum of the GPU's own outputs (ORDERED), which isolates the
-    # accumulation error from the transcendental ops' last-ulp differences
-    ref, ref_sse = (wfit, wsse) if kind == "ieee" else (fo, so)
+    # IEEE-only: against the oracle itself; mixed: against the oracle with
+    # the device's sine and cosine, whose outputs are the GPU's bit for bit,
+    # which isolates the accumulation error from the transcendental ops'
+    # last-ulp differences
+    if kind == "ieee":
+        ref, ref_sse = wfit, wsse
+    else:
+        od = oracle_lib.Oracle(oracle_lib.PROFILE_REF, 16, trig=oracle_lib.TRIG_DEVICE)
+        ref, ref_sse = od.evaluate_csr_opt(words, off, X, y_full, effective_only=True)
     fin = np.isfinite(ref_sse) & (ref > 0)
     rel = np.abs(fk[fin].astype(np.float64) - ref[fin]) / ref[fin]
     rel_sse = np.abs(sk[fin] - ref_sse[fin]) / ref_sse[fin]
@@ -284,7 +307,6 @@ def test_config4_magnitudes_kahan32_within_1e6(native, oracle_lib, kind):
     assert fin.sum() >= 50
     assert rel.max() <= 1e-6
     assert np.array_equal(fk[~fin] > 0, ref[~fin] > 0)
-    if kind == "ieee":
-        assert np.array_equal(so.view(np.uint64), wsse.view(np.uint64))
-    else:
+    assert np.array_equal(so.view(np.uint64), ref_sse.view(np.uint64))
+    if kind == "mixed":
         assert reference_gate(fo, wfit, 192)
