@@ -17,7 +17,10 @@ Emitted for K in {1, 2, 4, 8} and both ISA profiles:
            instructions (returns at the first unary op or window end), with
            the last result kept in registers: forwarded src1 operands are
            not loaded and results only reach the register file when the
-           next instruction's store_prev flag asks for it
+           next instruction's store_prev flag asks for it.  Its DIV arms
+           divide with a fast path of their own (div_group: rcp.approx, one
+           Newton-Raphson step, Markstein's correction) and take the exact
+           div.rn path only for a warp with an operand out of its range
   both wide forms also have the broadcast arm (table index 12): t[k] = the
   micro-op's constant, for instructions folded by the pre-pass
 where OP is one of the single-instruction ops: ADD, SUB, MUL (add/sub/mul
@@ -116,6 +119,81 @@ def wide_body(k: int, op: int, const: bool, a=None, b=None, t=None) -> list[str]
     return out
 
 
+# Fast path of protected DIV in the wide loop (div_group).
+DIV_TEMPS = (".reg .f32 fy, fe, fnb, fr, fab, fq; .reg .b32 fs, fw; "
+             ".reg .pred fz, fa, fb0, fall, funi, fbok;")
+DIV_LO, DIV_HI = "0f20000000", "0f5F000000"      # 2^-63, 2^63
+
+
+def div_divisor_lines(b: str) -> list[str]:
+    """The divisor's half of the fast path (once per instruction for a
+    constant divisor, per element otherwise): fy ~ 1/b refined by one
+    Newton-Raphson step, fnb = -b, fbok = 2^-63 <= |b| <= 2^63, fb0 = (b == 0)."""
+    return [f"rcp.approx.ftz.f32 fy, {b};",
+            f"neg.f32 fnb, {b};",
+            "fma.rn.f32 fe, fnb, fy, 0f3F800000;",
+            "fma.rn.f32 fy, fy, fe, fy;",
+            f"abs.f32 fab, {b};",
+            f"setp.ge.f32 fbok, fab, {DIV_LO};",
+            f"setp.le.and.f32 fbok, fab, {DIV_HI}, fbok;",
+            f"setp.eq.f32 fb0, {b}, 0f00000000;"]
+
+
+def div_fast_lines(a: str, out: str) -> list[str]:
+    """The dividend's half: q0 = a * fy, r = a - b q0 (exact), q = q0 + r fy
+    (the correction step of P. Markstein, "Computation of elementary
+    functions on the IBM RISC System/6000 processor", IBM J. Res. Dev.
+    34(1), 1990, which rounds correctly from a faithful q0 and an accurate
+    reciprocal), the sign of q0 kept on a zero quotient; out = q, or 1.0 for
+    a zero divisor.  fall &= this element is in the fast path's range:
+    2^-63 <= |a| <= 2^63 or a == 0, and the divisor's fbok, or b == 0."""
+    return [f"mul.rn.f32 fq, {a}, fy;",
+            "mov.b32 fs, fq;",
+            "and.b32 fs, fs, 0x80000000;",
+            f"fma.rn.f32 fr, fnb, fq, {a};",
+            "fma.rn.f32 fq, fr, fy, fq;",
+            "mov.b32 fw, fq;",
+            "or.b32 fw, fw, fs;",
+            "mov.b32 fq, fw;",
+            f"selp.f32 {out}, 0f3F800000, fq, fb0;",
+            f"setp.eq.f32 fz, {a}, 0f00000000;",
+            f"abs.f32 fab, {a};",
+            f"setp.ge.or.f32 fa, fab, {DIV_LO}, fz;",
+            f"setp.le.and.f32 fa, fab, {DIV_HI}, fa;",
+            "and.pred fa, fa, fbok;",
+            "or.pred fa, fa, fb0;",
+            "and.pred fall, fall, fa;"]
+
+
+def div_group(k: int, const: bool, a, b, nm: str) -> tuple[list[str], list[str]]:
+    """Protected DIV of the wide loop on the lane's K elements, in place
+    (a[q] = a[q] / b[q], or 1.0 for b[q] == 0): (hot lines, exact lines).
+
+    Hot: every element through the fast path into fo<q>; when every element
+    of every lane is in the fast path's range (vote.all, so the branch is
+    uniform), the results move into a[q] and the arm goes on at W<nm>.
+    Otherwise the exact lines (block V<nm>, placed away from the hot code)
+    evaluate all K elements with wide_body's div.rn path, which reads a[q]
+    and b[q] unchanged, and jump back to W<nm>.  Fast and exact agree bit
+    for bit wherever the fast path is in range (tests/test_gpu_division.py)."""
+    bq = (lambda q: "c") if const else b
+    hot = []
+    if const:
+        hot += div_divisor_lines("c")
+    for q in range(k):
+        if not const:
+            hot += div_divisor_lines(bq(q))
+        lines = div_fast_lines(a(q), f"fo{q}")
+        if q == 0:
+            lines[-1] = "mov.pred fall, fa;"
+        hot += lines
+    hot += ["vote.sync.all.pred funi, fall, 0xffffffff;", f"@!funi bra.uni V{nm};"]
+    hot += [f"mov.f32 {a(q)}, fo{q};" for q in range(k)]
+    hot.append(f"W{nm}:")
+    exact = wide_body(k, 3, const, a=a, b=b, t=a)
+    return hot, exact
+
+
 def _vec(regs: list[str]) -> str:
     return regs[0] if len(regs) == 1 else "{" + ", ".join(regs) + "}"
 
@@ -208,10 +286,11 @@ def wide_loop(k: int, profile: int) -> str:
                 for q in range(nq)]
 
     bregs = lambda q: f"b{q}"
-    L = [f".reg .f32 b<{k}>, c;", WIDE_TEMPS, ".reg .pred q;",
+    L = [f".reg .f32 b<{k}>, fo<{k}>, c;", WIDE_TEMPS, DIV_TEMPS, ".reg .pred q;",
          ".reg .u32 ux, uy, uz, uw, vx, vy, vz, vw, pa, pb;",
          f"mov.b32 ux, {CUR[0]}; mov.b32 uy, {CUR[1]}; mov.b32 uz, {CUR[2]}; mov.b32 uw, {CUR[3]};"]
     entry = {(1, 0): "S", (0, 0): "L", (0, 1): "F", (1, 1): "G"}
+    cold = []           # the DIV arms' exact paths, kept out of the hot code
     for cur, nxt, here, there in (("u", "v", "A", "B"), ("v", "u", "B", "A")):
         x, y, z, w = (f"{cur}{f}" for f in "xyzw")
         L += [f"L{here}%=: setp.lt.s32 q, {w}, 0;", f"@q bra.uni D{here}%=;",
@@ -234,11 +313,21 @@ def wide_loop(k: int, profile: int) -> str:
                 L.append(f"S{nm}: " + " ".join(st(PT)))
                 L.append(f"L{nm}: " + " ".join([f"add.u32 pa, {base}, {x};"] + ld(A, "pa")))
                 body = [] if cst else [f"add.u32 pb, {base}, {y};"] + ld(bregs, "pb")
-                body += wide_body(k, op, bool(cst), a=A, b=bregs, t=A)
+                if op == 3:
+                    hot, exact = div_group(k, bool(cst), A, bregs, nm)
+                    body += hot
+                    cold.append(f"V{nm}: " + " ".join(exact + [f"bra.uni W{nm};"]))
+                else:
+                    body += wide_body(k, op, bool(cst), a=A, b=bregs, t=A)
                 L.append(f"F{nm}: " + " ".join(body + nxt_jump))
                 L.append(f"G{nm}: " + " ".join(st(PT) + [f"bra.uni F{nm};"]))
         L.append(f"S{here}B_%=: " + " ".join(st(PT)))
         L.append(f"L{here}B_%=: " + " ".join([f"mov.f32 {A(q)}, c;" for q in range(k)] + nxt_jump))
+    # The DIV arms' exact paths: each block ends in a jump back into its arm.
+    # They sit between the loop bodies (whose lines all end in unconditional
+    # jumps) and the exit blocks, because DB falls through into D%= and
+    # nothing may fall into them.
+    L += cold
     # Table entries no micro-op uses (the pre-pass never writes them) leave
     # too, after the dispatch has already stepped to the next micro-op: X
     # steps back so that the caller gets this micro-op and %0 at it.
@@ -256,6 +345,23 @@ def wide_loop(k: int, profile: int) -> str:
             f"uint32_t base, uint4 cur, uint4& lv) {{\n"
             f'    asm volatile("{{\\n\\t{text}\\n\\t}}"\n'
             f'        : {outs}\n        : {ins}\n        : "memory");\n    }}\n')
+
+
+def div_fast_function() -> str:
+    """The wide loop's fast DIV path for one element as a standalone device
+    function, from the same generator lines.  The library does not call it;
+    tests/division_check.cu checks the fast path with it."""
+    L = [DIV_TEMPS] + div_divisor_lines("%3") + div_fast_lines("%2", "%0")
+    L[-1] = "mov.pred fall, fa;"
+    L += ["selp.u32 %1, 1, 0, fall;"]
+    text = "\\n\\t".join(L)
+    return ("struct DivFast {\n"
+            "    // q = a / b (1.0 for b == 0) when ok == 1, else q is not defined\n"
+            "    static __device__ __forceinline__ float run(float a, float b, uint32_t& ok) {\n"
+            "        float q;\n"
+            f'        asm volatile("{{\\n\\t{text}\\n\\t}}"\n'
+            '            : "=f"(q), "=r"(ok) : "f"(a), "f"(b));\n'
+            "        return q;\n    }\n};\n")
 
 
 HEADER_PATH = Path(__file__).resolve().parent / "dispatch_gen.cuh"
@@ -284,6 +390,7 @@ def render() -> str:
             out.append(f"template <>\nstruct WideLoop<{k}, {prof}> {{")
             out.append(wide_loop(k, prof))
             out.append("};\n")
+    out.append(div_fast_function())
     out.append("}  // namespace galop\n")
     return "\n".join(out)
 

@@ -21,11 +21,12 @@
 //     whose arm stores the previous result if the flags ask for it, loads
 //     src1 unless it is the previous result, loads src2 (register arms),
 //     and computes into the result registers, which are also the src1
-//     registers.
+//     registers (DIV with its own fast division, IEEE division only for a
+//     warp with an operand out of that path's range; gen_dispatch.py).
 // The result registers a[K] and the address of the register they belong to
-// live across the whole pass: the unary ops (SIN/COS, and EXP/LOG of the BJ
-// profile), which run in C++ on the slow branch with the CUDA math library,
-// read and write them too.  The last result is never stored: the output
+// live across the whole pass: the unary ops (SIN/COS from trig.cuh, EXP/LOG
+// of the BJ profile from the CUDA math library), which run in C++ after the
+// loop returns, read and write them too.  The last result is never stored: the output
 // is taken from it when the last instruction wrote the output register.
 // Each pass initialises only the values the program reads before writing
 // them (args.livein: registers, slots used, output slot).  The folding pass
@@ -443,18 +444,48 @@ interp_wide_kernel(InterpArgs args) {
                     for (int e = 0; e < V; ++e) t[q * V + e] = tv[e];
                 }
                 if constexpr (REDUCE == kReduceKahan32) {
+                    float ev[K];
+                    bool small = true;
 #pragma unroll
                     for (int k = 0; k < K; ++k) {
-                        const int64_t c = cb + (int64_t)((k / V) * 32 + lane) * V + (k % V);
-                        const float e = __fsub_rn(o[k], t[k]);
-                        const bool valid = c < w.cend;
-                        const bool huge = !(fabsf(e) <= kKahanMaxError);
-                        const float qv = (valid && !huge) ? __fmul_rn(e, e) : 0.0f;
-                        if (valid && huge) big = __dadd_rn(big, __dmul_rn((double)e, (double)e));
-                        const float yk = __fsub_rn(qv, kc);
+                        ev[k] = __fsub_rn(o[k], t[k]);
+                        small = small && fabsf(ev[k]) <= kKahanMaxError;
+                    }
+                    if (cb + kPass <= w.cend && small) {
+                        // every case of the pass counts and no square can
+                        // overflow: the lane's K squares summed pairwise
+                        // (each passes through at most four roundings at
+                        // K = 8), then one compensated step into the lane's sum
+                        float s[K / 2 > 0 ? K / 2 : 1];
+                        if constexpr (K == 1) {
+                            s[0] = __fmul_rn(ev[0], ev[0]);
+                        } else {
+#pragma unroll
+                            for (int h = 0; h < K / 2; ++h)
+                                s[h] = __fmaf_rn(ev[2 * h + 1], ev[2 * h + 1], __fmul_rn(ev[2 * h], ev[2 * h]));
+#pragma unroll
+                            for (int h = K / 4; h >= 1; h /= 2)
+#pragma unroll
+                                for (int j = 0; j < h; ++j) s[j] = __fadd_rn(s[j], s[j + h]);
+                        }
+                        const float yk = __fsub_rn(s[0], kc);
                         const float tt = __fadd_rn(ks, yk);
                         kc = __fsub_rn(__fsub_rn(tt, ks), yk);
                         ks = tt;
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < K; ++k) {
+                            const int64_t c = cb + (int64_t)((k / V) * 32 + lane) * V + (k % V);
+                            const float e = ev[k];
+                            const bool valid = c < w.cend;
+                            const bool huge = !(fabsf(e) <= kKahanMaxError);
+                            const float qv = (valid && !huge) ? __fmul_rn(e, e) : 0.0f;
+                            if (valid && huge) big = __dadd_rn(big, __dmul_rn((double)e, (double)e));
+                            const float yk = __fsub_rn(qv, kc);
+                            const float tt = __fadd_rn(ks, yk);
+                            kc = __fsub_rn(__fsub_rn(tt, ks), yk);
+                            ks = tt;
+                        }
                     }
                 } else if constexpr (REDUCE == kReduceFp64) {
 #pragma unroll
