@@ -834,8 +834,8 @@ def run_evo(args):
 
 
 def run_capacity(args):
-    """Largest device-resident population that evaluates (SURVEY §8(f) item 2,
-    after tests/cuda_capacity.cu): random-word programs of 30 instructions
+    """Largest device-resident population that evaluates (the capacity probe of
+    the reference's tests/cuda_capacity.cu): random-word programs of 30 instructions
     (the reference probe's evolved shape; ~16% effective), 8 registers, a
     32-case dataset, populations generated on the device (no host copy).
     The footprint per program is measured on 2^22 programs (caller's words,

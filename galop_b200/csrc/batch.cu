@@ -1,12 +1,13 @@
 // batch.cu -- resident datasets and batched evaluation of many populations.
 //
-// SURVEY build plan steps 6-7: populations of uneven sizes, program lengths
-// and datasets are evaluated by ONE persistent interpreter launch that pulls
-// (program, case chunk) items from a device queue, largest work first; each
+// Populations of uneven sizes, program lengths and datasets are evaluated
+// together: one persistent interpreter launch per register-file class (the
+// programs whose renamed values fit 8 slots, then the rest) pulls (program,
+// case chunk) items from a device queue, largest work first.  Each
 // generation's device work (intron pass, ordering, item list, interpreter,
 // chunk reduction) can be captured once as a CUDA graph and replayed.  Each
 // batch has its own stream, so several batches overlap on the device (the
-// serving loop in serve.cpp relies on this).
+// serving loop in serve.cu relies on this).
 //
 // Case chunking depends only on a population's own case count (at most
 // kChunkCases cases per work item), never on what else is in the batch, so a

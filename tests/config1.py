@@ -1,4 +1,4 @@
-"""The small-problem engine run as files for the
+"""The small-problem engine run (1 feature, 64 cases, 50 generations) as files for the
 reference engine drivers in oracle/_ref/lgp_run_c1_*: 1 feature x ~ U[-1,1],
 64 training and 64 test cases, y = a seeded random 8-effective-instruction
 program of the BJ op set {+,-,*,/p,sin,cos,exp,log_p}, 8 constants

@@ -1,4 +1,4 @@
-"""CSV datasets and the R^2 objective (SURVEY §8(f) item 3) against the
+"""CSV datasets and the R^2 objective against the
 reference's own loaders (load_csv_1d / load_csv_multi, src/Dataset.cpp:83-151)
 and its R^2 evaluator (src/Evaluator.cpp:49-97), compiled from its sources."""
 from __future__ import annotations
