@@ -859,11 +859,10 @@ def run_capacity(args):
         w = torch.randint(-2**31, 2**31 - 1, (P * L,), dtype=torch.int32, device=dev, generator=gen)
         off = torch.arange(P + 1, dtype=torch.int64, device=dev) * L
         fit = torch.empty(P, dtype=torch.float32, device=dev)
+        # torch generates on its (legacy default) stream; the device call runs
+        # on the evaluator's own non-blocking stream, so wait for the data
+        torch.cuda.synchronize()
         return w, off, fit
-
-    # the device call runs on the evaluator's stream after the work queued on
-    # the stream it is given, here torch's (which generated the population)
-    ts = torch.cuda.current_stream(dev).cuda_stream
 
     # dispatch 3 with dedup (the default), without it (its per-program sort
     # buffers are the price of interpreting identical programs once), and the
@@ -876,7 +875,7 @@ def run_capacity(args):
         ev = g.Evaluator(num_registers=8, dispatch=dispatch, dedup=dedup)
         ev.set_dataset(ds)
         w, off, fit = population(P0)
-        ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P0, P0 * L, fit.data_ptr(), stream=ts)
+        ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P0, P0 * L, fit.data_ptr())
         st0 = ev.stats
         used = before - torch.cuda.mem_get_info(dev)[0]
         # At this size the device call sizes its micro-op buffer for the raw
@@ -897,11 +896,11 @@ def run_capacity(args):
                 ev = g.Evaluator(num_registers=8, dispatch=dispatch, dedup=dedup)
                 ev.set_dataset(ds)
                 w, off, fit = population(P)
-                ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, P * L, fit.data_ptr(), stream=ts)   # the proof
+                ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, P * L, fit.data_ptr())   # the proof
                 ev.synchronize()
                 ms = []
                 for _ in range(2):
-                    ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, P * L, fit.data_ptr(), stream=ts)
+                    ev.evaluate_csr_device(w.data_ptr(), off.data_ptr(), P, P * L, fit.data_ptr())
                     st = ev.stats
                     ms.append(st.prepass_ms + st.interp_ms + st.finalize_ms)
                 st = ev.stats
