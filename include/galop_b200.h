@@ -322,7 +322,8 @@ GALOP_API int galop_evaluate_csr(galop_ctx* ctx, const uint32_t* words, const in
  * cudaStream_t, or NULL for the context's own stream, which is a
  * non-blocking stream: with NULL the call does not wait for work the caller
  * queued on other streams, so pass the stream that wrote the inputs, or
- * synchronize it first) and the call returns
+ * synchronize it first; the legacy default stream, whose handle is also
+ * NULL, cannot be named here) and the call returns
  * without waiting for the device; it only blocks when a working buffer must
  * grow (the first call, or a larger population), and waits once for the
  * effective instruction count when a buffer sized for total_words would take
