@@ -81,14 +81,15 @@ def parse():
                     help="headline only: skip the single-generation, batching and reference-GPU keys")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default="generation",
-                    choices=["generation", "single", "batch", "serve", "evo", "capacity"],
+                    choices=["generation", "single", "batch", "serve", "evo", "capacity", "lengths"],
                     help="generation: the headline (HBM-streaming configuration at full size); single: "
                          "the single-generation configuration alone; batch: many populations in one "
                          "persistent launch per generation (graph replay) vs one plain launch per population; "
                          "serve: continuous batching of Poisson-arriving GP runs; evo: a whole 100-generation "
                          "run of the reference engine with this backend, beside the reference's own whole-run "
                          "benchmark on the same GPU; capacity: the largest device-resident population that "
-                         "evaluates, and its footprint per program")
+                         "evaluates, and its footprint per program; lengths: every tile on populations of "
+                         "one fixed program length per class")
     ap.add_argument("--evo-pop", type=int, default=100000, choices=[10000, 100000, 1000000])
     ap.add_argument("--evo-cases", type=int, default=1024)
     ap.add_argument("--evo-seed", type=int, default=70)
@@ -935,6 +936,40 @@ def run_capacity(args):
     print(json.dumps(line), flush=True)
 
 
+def run_lengths(args):
+    """Every tile (cases per lane 1/2/4/8 x warps per block 2/4/8) on
+    populations of all-effective programs of one fixed length per class,
+    at 4,096 and 65,536 cases: does the best tile depend on the length?
+    One JSON line per (cases, length) with the rate of every tile (effective
+    GPop/s of the interpreter launches, best of two calls)."""
+    import galop_b200 as g
+    from galop_b200 import workloads as W
+    isa = W.IsaSpec(g.PROFILE_REF, 16)
+    for n_cases in (4096, 65536):
+        rng = np.random.default_rng(7)
+        X = rng.uniform(-3, 3, (n_cases, 5)).astype(np.float32)
+        y = np.sin(X[:, 0]).astype(np.float32)
+        ds = g.Dataset(X, y)
+        for L in (2, 4, 8, 16, 32, 64, 256, 1024):
+            n = int(min(65536, max(2048, 2**31 // (L * n_cases))))
+            words, off = W.structured_population(rng, np.full(n, L), isa, 1.0)
+            rates = {}
+            for k in (1, 2, 4, 8):
+                for wpb in (2, 4, 8):
+                    with g.Evaluator(num_registers=16, cases_per_lane=k, warps_per_block=wpb) as ev:
+                        ev.set_dataset(ds)
+                        ev.evaluate_csr(words, off)
+                        ms = []
+                        for _ in range(2):
+                            ev.evaluate_csr(words, off)
+                            ms.append(ev.stats.interp_ms)
+                        eff = ev.stats.eff_instructions
+                    rates[f"K{k}_w{wpb}"] = round(eff * n_cases / (min(ms) / 1e3) / 1e9, 1)
+            best = max(rates, key=rates.get)
+            print(json.dumps({"workload": "lengths", "cases": n_cases, "length": L, "programs": n,
+                              "best_tile": best, "best_gpops": rates[best], "gpops": rates}), flush=True)
+
+
 def main():
     args = parse()
     dist = Dist()
@@ -949,6 +984,8 @@ def main():
             run_evo(args)
         elif args.workload == "capacity":
             run_capacity(args)
+        elif args.workload == "lengths":
+            run_lengths(args)
         elif args.workload == "single":
             line = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
                     "data": "synthetic (seeded)", **single_generation_leg(args)}
