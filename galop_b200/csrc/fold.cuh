@@ -242,7 +242,9 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
 // before that instruction's result is stored (results are stored, if at
 // all, at the start of the next instruction, before it loads anything).
 // The forwarding flags, set on registers before renaming, stay valid: they
-// name the previous instruction's value, whatever slot it gets.
+// name the previous instruction's value, whatever slot it gets.  Renamed
+// SIN/COS micro-ops with a register operand take the loop's unary form
+// (isa.cuh).
 constexpr uint32_t kDies1 = 1u << 8;    // src1's value is not read after this instruction
 constexpr uint32_t kDies2 = 1u << 9;    // the same for a register src2
 
@@ -303,6 +305,14 @@ __device__ __forceinline__ uint32_t rename_slots(uint4* __restrict__ u, int64_t 
         if (p + 1u > top) top = p + 1u;
         w.z = p << sh;
         w.w &= ~(kDies1 | kDies2);
+        // SIN/COS of a register run inside the interpreter loop, which takes
+        // a unary operand the way it takes a binary op's src1: the operand's
+        // slot into x, fwd2 into fwd1, the unary bit cleared
+        const uint32_t op = w.w & 7u;
+        if ((w.w & kWideSpecial) && reads2 && (op == kSin || op == kCos)) {
+            w.x = w.y;
+            w.w = op | ((w.w & kWideFwd2) ? kWideFwd1 : 0u) | (w.w & kWideStorePrev);
+        }
         u[j] = w;
     }
     const uint32_t out = slot_of[output_reg] >= 0 ? (uint32_t)slot_of[output_reg] : 0u;

@@ -14,13 +14,16 @@ Emitted for K in {1, 2, 4, 8} and both ISA profiles:
            store t -- the table index is op | constant-src2 << 3, and
            protected DIV is one of the arms
   wide loop  the same ops as one PTX loop over consecutive binary
-           instructions (returns at the first unary op or window end), with
-           the last result kept in registers: forwarded src1 operands are
-           not loaded and results only reach the register file when the
-           next instruction's store_prev flag asks for it.  Its DIV arms
-           divide with a fast path of their own (div_group: rcp.approx, one
-           Newton-Raphson step, Markstein's correction) and take the exact
-           div.rn path only for a warp with an operand out of its range
+           instructions and SIN/COS of a register (returns at any other
+           unary op or the window end), with the last result kept in
+           registers: forwarded src1 operands are not loaded and results
+           only reach the register file when the next instruction's
+           store_prev flag asks for it.  Its DIV arms divide with a fast
+           path of their own (div_group: rcp.approx, one Newton-Raphson
+           step, Markstein's correction) and take the exact div.rn path
+           only for a warp with an operand out of its range; its SIN/COS
+           arms run trig.cuh's Cody-Waite path (trig_blocks) and leave the
+           loop to the caller for a warp with an argument beyond it
   both wide forms also have the broadcast arm (table index 12): t[k] = the
   micro-op's constant, for instructions folded by the pre-pass
 where OP is one of the single-instruction ops: ADD, SUB, MUL (add/sub/mul
@@ -165,6 +168,91 @@ def div_fast_lines(a: str, out: str) -> list[str]:
             "and.pred fall, fall, fa;"]
 
 
+TRIG_TEMPS = (".reg .f32 tax, tjr, tj, tr, tz, tp, trz, ts, tc, ty; .reg .b32 tq, tb, tt, tw, th, tcos, tmask; "
+              ".reg .pred tpq, tslow, tany;")
+
+
+def trig_constants() -> dict:
+    """The single-precision constants of trig.cuh's Cody-Waite path as PTX
+    immediates (0fXXXXXXXX), read from the header itself so the loop's copy
+    of the fast path cannot drift from it."""
+    import re
+    import struct
+    text = (Path(__file__).resolve().parent / "trig.cuh").read_text()
+    out = {}
+    for name, lit in re.findall(r"#define (GT_[A-Z0-9_]+|GALOP_TRIG_FAST_LIMIT) (-?0x[0-9a-fA-Fp.+-]+f|[0-9.]+f)\n", text):
+        v = float.fromhex(lit[:-1]) if "0x" in lit else float(lit[:-1])
+        out[name] = "0f%08X" % struct.unpack("<I", struct.pack("<f", v))[0]
+    return out
+
+
+def neg_imm(imm: str) -> str:
+    """The PTX immediate of -x for the float immediate x."""
+    return "0f%08X" % (int(imm[2:], 16) ^ 0x80000000)
+
+
+TRIG_OPS = (4, 5)      # SIN, COS: unary in both profiles
+
+
+def trig_blocks(k: int, a) -> list[str]:
+    """The wide loop's SIN and COS of the lane's K elements of the result
+    registers a(q), in place: trig.cuh's Cody-Waite path (galop_trig_fast)
+    restated operation for operation, so the bits are the same.  One block
+    (R) serves both ops and both copies of the loop body: the arms jump here
+    after putting the operand into a(q) and the destination address into the
+    result-address register, with th = 1 when they are copy A's and
+    tcos = 1 for COS (the quadrant moves by one, and the argument's sign
+    does not enter the result's: tmask = 0).
+
+    Each element goes into fo<q>.  When an element of any lane is out of
+    the fast path's range (|x| >= 2^17, infinities, NaN; vote.any, so the
+    branch is uniform) the warp jumps to block Z, which steps the micro-op
+    pointer back to the trig micro-op and leaves the loop through its
+    copy's exit, with a(q) still the operand: the caller evaluates the op
+    with galop_trig_k, which takes the Payne-Hanek path where needed.
+    Otherwise the results move into a(q) and the loop goes on with the next
+    micro-op, already loaded into the other copy's registers."""
+    c = trig_constants()
+    R = ["R_%=:", "sub.u32 tmask, tcos, 1;"]
+    for q in range(k):
+        x = a(q)
+        R += [f"abs.f32 tax, {x};",
+              f"fma.rn.f32 tjr, tax, {c['GT_TWO_OVER_PI']}, {c['GT_ROUND']};",
+              f"sub.rn.f32 tj, tjr, {c['GT_ROUND']};",
+              "mov.b32 tq, tjr;",
+              "add.u32 tq, tq, tcos;",
+              f"fma.rn.f32 tr, tj, {neg_imm(c['GT_P1'])}, tax;",
+              f"fma.rn.f32 tr, tj, {neg_imm(c['GT_P2'])}, tr;",
+              f"fma.rn.f32 tr, tj, {neg_imm(c['GT_P3'])}, tr;",
+              "mul.rn.f32 tz, tr, tr;",
+              f"fma.rn.f32 tp, tz, {c['GT_S3']}, {c['GT_S2']};",
+              f"fma.rn.f32 tp, tp, tz, {c['GT_S1']};",
+              "mul.rn.f32 trz, tr, tz;",
+              "fma.rn.f32 ts, trz, tp, tr;",
+              f"fma.rn.f32 tc, tz, {c['GT_C4']}, {c['GT_C3']};",
+              f"fma.rn.f32 tc, tc, tz, {c['GT_C2']};",
+              f"fma.rn.f32 tc, tc, tz, {c['GT_C1']};",
+              "fma.rn.f32 tc, tc, tz, 0f3F800000;",
+              "and.b32 tb, tq, 1;",
+              "setp.ne.u32 tpq, tb, 0;",
+              "selp.f32 ty, tc, ts, tpq;",
+              "shl.b32 tt, tq, 30;",
+              f"mov.b32 tw, {x};",
+              "and.b32 tw, tw, tmask;",
+              "xor.b32 tt, tt, tw;",
+              "and.b32 tt, tt, 0x80000000;",
+              "mov.b32 tw, ty;",
+              "xor.b32 tw, tw, tt;",
+              f"mov.b32 fo{q}, tw;",
+              f"setp.geu.f32 tslow, tax, {c['GALOP_TRIG_FAST_LIMIT']};" if q == 0 else
+              f"setp.geu.or.f32 tslow, tax, {c['GALOP_TRIG_FAST_LIMIT']}, tslow;"]
+    R += ["vote.sync.any.pred tany, tslow, 0xffffffff;", "@tany bra.uni Z_%=;"]
+    R += [f"mov.f32 {a(q)}, fo{q};" for q in range(k)]
+    R += ["setp.ne.u32 tpq, th, 0;", "@tpq bra.uni LB%=;", "bra.uni LA%=;"]
+    Z = ["Z_%=: sub.u32 %0, %0, 16;", "setp.ne.u32 tpq, th, 0;", "@tpq bra.uni DA%=;", "bra.uni DB%=;"]
+    return [" ".join(R), " ".join(Z)]
+
+
 def div_group(k: int, const: bool, a, b, nm: str) -> tuple[list[str], list[str]]:
     """Protected DIV of the wide loop on the lane's K elements, in place
     (a[q] = a[q] / b[q], or 1.0 for b[q] == 0): (hot lines, exact lines).
@@ -175,7 +263,9 @@ def div_group(k: int, const: bool, a, b, nm: str) -> tuple[list[str], list[str]]
     Otherwise the exact lines (block V<nm>, placed away from the hot code)
     evaluate all K elements with wide_body's div.rn path, which reads a[q]
     and b[q] unchanged, and jump back to W<nm>.  Fast and exact agree bit
-    for bit wherever the fast path is in range (tests/test_gpu_division.py)."""
+    for bit wherever the fast path is in range (tests/test_gpu_division.py).
+    (Leaving the loop for a division in C++ instead, to keep these blocks
+    out of the loop's code, was slower.)"""
     bq = (lambda q: "c") if const else b
     hot = []
     if const:
@@ -244,9 +334,11 @@ def wide_ops(k: int, profile: int) -> str:
 
 def wide_loop(k: int, profile: int) -> str:
     """The fast path of the 16-byte micro-op kernel as one PTX loop: execute
-    binary instructions from the staged micro-op at byte address %0 on,
-    until a micro-op whose word w is negative (a unary op or the window's end
-    marker); return with %0 pointing at it.
+    binary instructions (and SIN/COS of a register) from the staged micro-op
+    at byte address %0 on, until a micro-op whose word w is negative (an
+    other unary op or the window's end marker) or a SIN/COS whose argument
+    needs the caller's Payne-Hanek path; return with %0 pointing at it.
+    Such a SIN/COS leaves with its pending store done and a = its operand.
 
     Operands: %0 the micro-op address (in/out); %1..%K the lane's K values of
     the last result (in/out); %K+1 the register-file address that result
@@ -263,6 +355,13 @@ def wide_loop(k: int, profile: int) -> str:
       store_prev, not fwd1 -> S     neither -> L
       fwd1, not store_prev -> F     both    -> G
     The broadcast arm (index 12, | 32) has S and L only: a = the constant.
+    SIN and COS with a register operand (indices 4 and 5, | 16 | 32) are
+    arms too: the folding pass rewrites such a micro-op with its operand as
+    src1 and fwd2 as fwd1 (fold.cuh), so S/L/F/G load or forward it like a
+    src1 into a, and F jumps to the one block both ops and both copies
+    share (trig_blocks), which computes a = SIN(a) or COS(a) and goes on -- or
+    leaves the loop at that micro-op, a holding the operand, when an
+    argument needs trig.cuh's slow path.
 
     Two copies of the loop body alternate between two micro-op register sets
     (u, v): each body prefetches the next micro-op into the other set, so no
@@ -286,7 +385,7 @@ def wide_loop(k: int, profile: int) -> str:
                 for q in range(nq)]
 
     bregs = lambda q: f"b{q}"
-    L = [f".reg .f32 b<{k}>, fo<{k}>, c;", WIDE_TEMPS, DIV_TEMPS, ".reg .pred q;",
+    L = [f".reg .f32 b<{k}>, fo<{k}>, c;", WIDE_TEMPS, DIV_TEMPS, TRIG_TEMPS, ".reg .pred q;",
          ".reg .u32 ux, uy, uz, uw, vx, vy, vz, vw, pa, pb;",
          f"mov.b32 ux, {CUR[0]}; mov.b32 uy, {CUR[1]}; mov.b32 uz, {CUR[2]}; mov.b32 uw, {CUR[3]};"]
     entry = {(1, 0): "S", (0, 0): "L", (0, 1): "F", (1, 1): "G"}
@@ -302,6 +401,8 @@ def wide_loop(k: int, profile: int) -> str:
             op, cst, f1, sp = idx & 7, (idx >> 3) & 1, (idx >> 4) & 1, (idx >> 5) & 1
             if op == BCAST_OP and cst and not f1:
                 targets.append(f"{'S' if sp else 'L'}{here}B_%=")
+            elif op in TRIG_OPS and not cst:
+                targets.append(f"{entry[(sp, f1)]}{here}{op}0_%=")
             elif op in ops:
                 targets.append(f"{entry[(sp, f1)]}{here}{op}{cst}_%=")
             else:
@@ -321,13 +422,23 @@ def wide_loop(k: int, profile: int) -> str:
                     body += wide_body(k, op, bool(cst), a=A, b=bregs, t=A)
                 L.append(f"F{nm}: " + " ".join(body + nxt_jump))
                 L.append(f"G{nm}: " + " ".join(st(PT) + [f"bra.uni F{nm};"]))
+        for op in TRIG_OPS:
+            # unary: the operand comes in as src1 (x, fwd1); the math is shared
+            nm = f"{here}{op}0_%="
+            L.append(f"S{nm}: " + " ".join(st(PT)))
+            L.append(f"L{nm}: " + " ".join([f"add.u32 pa, {base}, {x};"] + ld(A, "pa")))
+            L.append(f"F{nm}: add.u32 {PT}, {base}, {z}; mov.u32 th, {1 if here == 'A' else 0}; "
+                     f"mov.u32 tcos, {op - 4}; bra.uni R_%=;")
+            L.append(f"G{nm}: " + " ".join(st(PT) + [f"bra.uni F{nm};"]))
         L.append(f"S{here}B_%=: " + " ".join(st(PT)))
         L.append(f"L{here}B_%=: " + " ".join([f"mov.f32 {A(q)}, c;" for q in range(k)] + nxt_jump))
-    # The DIV arms' exact paths: each block ends in a jump back into its arm.
-    # They sit between the loop bodies (whose lines all end in unconditional
-    # jumps) and the exit blocks, because DB falls through into D%= and
-    # nothing may fall into them.
+    # The DIV arms' exact paths (each block ends in a jump back into its arm)
+    # and the shared SIN/COS block and its exit (each ends in jumps to a loop
+    # head or an exit).  They sit between the loop bodies (whose lines all
+    # end in unconditional jumps) and the exit blocks, because DB falls
+    # through into D%= and nothing may fall into them.
     L += cold
+    L += trig_blocks(k, A)
     # Table entries no micro-op uses (the pre-pass never writes them) leave
     # too, after the dispatch has already stepped to the next micro-op: X
     # steps back so that the caller gets this micro-op and %0 at it.

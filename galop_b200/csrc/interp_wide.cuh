@@ -9,25 +9,29 @@
 // the folding pass renames each program's values into as few slots as it
 // keeps live at once (fold.cuh), and the runtime runs the programs that fit
 // in 8 slots on the 8-slot instance, which needs half the shared memory per
-// warp.  Runs of binary instructions execute inside one PTX loop (WideLoop);
-// per instruction the warp does:
+// warp.  Runs of binary instructions and of SIN/COS of a register execute
+// inside one PTX loop (WideLoop); per instruction the warp does:
 //   one broadcast 16-byte shared load of the micro-op (32-instruction
 //     windows are staged in shared memory with cp.async, the next window
 //     copied while the current one runs; the next micro-op is prefetched
 //     into a second register set, the loop body existing twice),
-//   a sign test (unary ops and the window end leave the loop),
-//   one jump table (16 arms: 8 ops x register/constant src2, each with
+//   a sign test (other unary ops and the window end leave the loop),
+//   one jump table (arms for the 8 ops x register/constant src2, each with
 //     entry points that skip what the micro-op's flags make unnecessary)
 //     whose arm stores the previous result if the flags ask for it, loads
 //     src1 unless it is the previous result, loads src2 (register arms),
 //     and computes into the result registers, which are also the src1
 //     registers (DIV with its own fast division, IEEE division only for a
-//     warp with an operand out of that path's range; gen_dispatch.py).
+//     warp with an operand out of that path's range; SIN/COS with
+//     trig.cuh's Cody-Waite path, their operand taken as src1;
+//     gen_dispatch.py).
 // The result registers a[K] and the address of the register they belong to
-// live across the whole pass: the unary ops (SIN/COS from trig.cuh, EXP/LOG
-// of the BJ profile from the CUDA math library), which run in C++ after the
-// loop returns, read and write them too.  The last result is never stored: the output
-// is taken from it when the last instruction wrote the output register.
+// live across the whole pass: the unary ops the loop leaves to C++ (EXP/LOG
+// of the BJ profile from the CUDA math library, a constant's SIN/COS when
+// folding is off, and SIN/COS for a warp with an argument that needs
+// trig.cuh's Payne-Hanek path) read and write them too.  The last result
+// is never stored: the output is taken from it when the last instruction
+// wrote the output register.
 // Each pass initialises only the values the program reads before writing
 // them (args.livein: registers, slots used, output slot).  The folding pass
 // sets the flags and these words (isa.cuh, fold.cuh).
@@ -391,24 +395,33 @@ interp_wide_kernel(InterpArgs args) {
                 } else {
                     uint4 cur = lds_u4(sp);
                     for (;;) {
-                        // Every binary instruction up to the next unary op or the
-                        // end marker; u is the micro-op that stopped the loop.
+                        // Every binary instruction and SIN/COS up to the next other
+                        // unary op, a SIN/COS with an argument for trig.cuh's slow
+                        // path, or the end marker; u is the micro-op that stopped
+                        // the loop.
                         uint4 u;
                         WideLoop<K, PROFILE>::run(sp, a, pt, base, cur, u);
                         if (u.w == kWideEnd) break;
                         const uint4 next = lds_u4(sp + 16u);   // the end marker at most
-                        // Unary op on src2 (register, constant or the previous result).
-                        if (u.w & kWideStorePrev) WR::store(pt, a);
                         float b[K];
-                        if (u.w & 8u) {
-                            const float c = __uint_as_float(u.y);
-#pragma unroll
-                            for (int k = 0; k < K; ++k) b[k] = c;
-                        } else if (u.w & kWideFwd2) {
+                        if (!(u.w & kWideSpecial)) {
+                            // a SIN/COS the loop left for trig.cuh's slow path:
+                            // the previous result is stored, a holds the operand
 #pragma unroll
                             for (int k = 0; k < K; ++k) b[k] = a[k];
                         } else {
-                            WR::load(base + u.y, b);
+                            // unary op on src2 (register, constant or the previous result)
+                            if (u.w & kWideStorePrev) WR::store(pt, a);
+                            if (u.w & 8u) {
+                                const float c = __uint_as_float(u.y);
+#pragma unroll
+                                for (int k = 0; k < K; ++k) b[k] = c;
+                            } else if (u.w & kWideFwd2) {
+#pragma unroll
+                                for (int k = 0; k < K; ++k) b[k] = a[k];
+                            } else {
+                                WR::load(base + u.y, b);
+                            }
                         }
                         unary_op<K, PROFILE>(u.w & 7u, b, a);
                         pt = base + u.z;

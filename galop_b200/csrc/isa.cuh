@@ -84,6 +84,10 @@ __host__ __device__ __forceinline__ uint32_t encode_uop(const Decoded& d) {
 //   store_prev  the previous result must reach the register file (something
 //               other than this instruction's forwarded operand reads it);
 //               it is stored before this instruction reads any operand.
+// Renamed streams (register-file slots, fold.cuh) carry SIN and COS of a
+// register in the interpreter loop's unary form: x = the operand's slot,
+// y unused, w = op | fwd1 << 4 | store_prev << 5 (fwd1: the operand is the
+// previous result), unary bit clear.
 constexpr uint32_t kWideSpecial = 0x80000000u;
 constexpr uint32_t kWideEnd = 0xFFFFFFFFu;
 constexpr uint32_t kWideFwd1 = 16u;

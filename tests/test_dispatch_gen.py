@@ -5,8 +5,9 @@ control flow must be closed: every branch target exists, and the only
 fall-through between labelled blocks is the one the loop is built on (an
 arm's S, L, F entry points fall into each other; DB falls into the exit).
 In particular, the DIV arms' exact paths (V blocks) are entered only by
-their arm's uniform branch and jump back into it (W), so no path falls into
-them and loops.
+their arm's uniform branch and jump back into it (W), and the shared SIN/COS
+block (R) and its exit (Z) end in jumps, so no path falls into them and
+loops.
 """
 from __future__ import annotations
 
@@ -68,6 +69,15 @@ def test_wide_loop_control_flow(k, profile):
         assert not falls_through(bl[i - 1][1]), (bl[i - 1][0], lab)
         assert stm.rstrip().endswith(f"bra.uni W{lab[1:]};"), lab
         assert f"@!funi bra.uni {lab};" in everything, lab
+    # SIN/COS: one block (R) shared by both ops and both copies' F arms, and
+    # its exit (Z), entered by the uniform slow-path branch; both end in
+    # jumps and nothing falls into them
+    for lab, entry in (("R_%=", "bra.uni R_%=;"), ("Z_%=", "@tany bra.uni Z_%=;")):
+        (i,) = [j for j, (lb, _) in enumerate(bl) if lb == lab]
+        assert not falls_through(bl[i - 1][1]), (bl[i - 1][0], lab)
+        assert not falls_through(bl[i][1]), lab
+        assert entry in everything, lab
+    assert everything.count("bra.uni R_%=;") == 2 * len(G.TRIG_OPS)
     # the exit: D%= is the last label and only DB (right before it) falls into it
     assert bl[-1][0] == "D%=" and bl[-2][0] == "DB%="
     for lab, stm in bl[:-2]:
