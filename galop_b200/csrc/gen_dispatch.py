@@ -23,7 +23,10 @@ Emitted for K in {1, 2, 4, 8} and both ISA profiles:
            step, Markstein's correction) and take the exact div.rn path
            only for a warp with an operand out of its range; its SIN/COS
            arms run trig.cuh's Cody-Waite path (trig_blocks) and leave the
-           loop to the caller for a warp with an argument beyond it
+           loop to the caller for a warp with an argument beyond it.  ADD,
+           SUB and MUL, the division's Newton-Raphson and Markstein steps
+           and the trig polynomials take two elements per instruction
+           (sm_100a's f32x2 forms, rounded per half like the f32 ones)
   both wide forms also have the broadcast arm (table index 12): t[k] = the
   micro-op's constant, for instructions folded by the pre-pass
 where OP is one of the single-instruction ops: ADD, SUB, MUL (add/sub/mul
@@ -126,6 +129,25 @@ def wide_body(k: int, op: int, const: bool, a=None, b=None, t=None) -> list[str]
 DIV_TEMPS = (".reg .f32 fy, fe, fnb, fr, fab, fq; .reg .b32 fs, fw; "
              ".reg .pred fz, fa, fb0, fall, funi, fbok;")
 DIV_LO, DIV_HI = "0f20000000", "0f5F000000"      # 2^-63, 2^63
+# Paired (f32x2) temporaries of the wide loop's arithmetic: sm_100a's
+# add/sub/mul/fma.rn.f32x2 round each half exactly as the f32 instruction
+# does, so two elements take one instruction with the same bits.
+PAIR_TEMPS = (".reg .b64 xa, xb, xc, xy, xnb, xe, xq, xr, xone; "
+              ".reg .f32 fy0, fy1, fnb0, fnb1, fq0, fq1, fg0, fg1;")
+X2 = {0: "add.rn.f32x2", 1: "sub.rn.f32x2", 2: "mul.rn.f32x2"}
+
+
+def pair_body(k: int, op: int, const: bool, a, b) -> list[str]:
+    """a[q] = OP(a[q], b[q]) for ADD/SUB/MUL, two elements per f32x2
+    instruction (b = the scalar c for a constant src2)."""
+    out = ["mov.b64 xc, {c, c};"] if const else []
+    for j in range(k // 2):
+        a0, a1 = a(2 * j), a(2 * j + 1)
+        out.append(f"mov.b64 xa, {{{a0}, {a1}}};")
+        if not const:
+            out.append(f"mov.b64 xb, {{{b(2 * j)}, {b(2 * j + 1)}}};")
+        out += [f"{X2[op]} xa, xa, {'xc' if const else 'xb'};", f"mov.b64 {{{a0}, {a1}}}, xa;"]
+    return out
 
 
 def div_divisor_lines(b: str) -> list[str]:
@@ -169,7 +191,19 @@ def div_fast_lines(a: str, out: str) -> list[str]:
 
 
 TRIG_TEMPS = (".reg .f32 tax, tjr, tj, tr, tz, tp, trz, ts, tc, ty; .reg .b32 tq, tb, tt, tw, th, tcos, tmask; "
-              ".reg .pred tpq, tslow, tany;")
+              ".reg .pred tpq, tslow, tany; "
+              ".reg .f32 tax0, tax1, tjr0, tjr1, ts0, ts1, tc0, tc1; "
+              ".reg .b64 k2pi, kround, knp1, knp2, knp3, ks3, ks2, ks1, kc4, kc3, kc2, kc1, kone, "
+              "xax, xjr, xj, xtr, xz, xp, xrz, xs, xtc;")
+
+
+def trig_pair_constants(c: dict) -> dict:
+    """The Cody-Waite path's constants by the register-pair names of the
+    paired (f32x2) form, which takes no immediate operands."""
+    return {"k2pi": c["GT_TWO_OVER_PI"], "kround": c["GT_ROUND"], "knp1": neg_imm(c["GT_P1"]),
+            "knp2": neg_imm(c["GT_P2"]), "knp3": neg_imm(c["GT_P3"]), "ks3": c["GT_S3"], "ks2": c["GT_S2"],
+            "ks1": c["GT_S1"], "kc4": c["GT_C4"], "kc3": c["GT_C3"], "kc2": c["GT_C2"], "kc1": c["GT_C1"],
+            "kone": "0f3F800000"}
 
 
 def trig_constants() -> dict:
@@ -204,6 +238,11 @@ def trig_blocks(k: int, a) -> list[str]:
     tcos = 1 for COS (the quadrant moves by one, and the argument's sign
     does not enter the result's: tmask = 0).
 
+    For K >= 2 the float steps run on element pairs (f32x2: each half
+    rounded as the f32 instruction rounds it, so the bits do not change),
+    with the constants in register pairs set at the block's start; the
+    quadrant, selection and sign stay per element.
+
     Each element goes into fo<q>.  When an element of any lane is out of
     the fast path's range (|x| >= 2^17, infinities, NaN; vote.any, so the
     branch is uniform) the warp jumps to block Z, which steps the micro-op
@@ -213,39 +252,68 @@ def trig_blocks(k: int, a) -> list[str]:
     Otherwise the results move into a(q) and the loop goes on with the next
     micro-op, already loaded into the other copy's registers."""
     c = trig_constants()
-    R = ["R_%=:", "sub.u32 tmask, tcos, 1;"]
-    for q in range(k):
+    lim = c["GALOP_TRIG_FAST_LIMIT"]
+
+    def tail(q: int, jr: str, sv: str, cv: str, ax: str) -> list[str]:
+        # quadrant, sine or cosine polynomial, sign; the range test
         x = a(q)
-        R += [f"abs.f32 tax, {x};",
-              f"fma.rn.f32 tjr, tax, {c['GT_TWO_OVER_PI']}, {c['GT_ROUND']};",
-              f"sub.rn.f32 tj, tjr, {c['GT_ROUND']};",
-              "mov.b32 tq, tjr;",
-              "add.u32 tq, tq, tcos;",
-              f"fma.rn.f32 tr, tj, {neg_imm(c['GT_P1'])}, tax;",
-              f"fma.rn.f32 tr, tj, {neg_imm(c['GT_P2'])}, tr;",
-              f"fma.rn.f32 tr, tj, {neg_imm(c['GT_P3'])}, tr;",
-              "mul.rn.f32 tz, tr, tr;",
-              f"fma.rn.f32 tp, tz, {c['GT_S3']}, {c['GT_S2']};",
-              f"fma.rn.f32 tp, tp, tz, {c['GT_S1']};",
-              "mul.rn.f32 trz, tr, tz;",
-              "fma.rn.f32 ts, trz, tp, tr;",
-              f"fma.rn.f32 tc, tz, {c['GT_C4']}, {c['GT_C3']};",
-              f"fma.rn.f32 tc, tc, tz, {c['GT_C2']};",
-              f"fma.rn.f32 tc, tc, tz, {c['GT_C1']};",
-              "fma.rn.f32 tc, tc, tz, 0f3F800000;",
-              "and.b32 tb, tq, 1;",
-              "setp.ne.u32 tpq, tb, 0;",
-              "selp.f32 ty, tc, ts, tpq;",
-              "shl.b32 tt, tq, 30;",
-              f"mov.b32 tw, {x};",
-              "and.b32 tw, tw, tmask;",
-              "xor.b32 tt, tt, tw;",
-              "and.b32 tt, tt, 0x80000000;",
-              "mov.b32 tw, ty;",
-              "xor.b32 tw, tw, tt;",
-              f"mov.b32 fo{q}, tw;",
-              f"setp.geu.f32 tslow, tax, {c['GALOP_TRIG_FAST_LIMIT']};" if q == 0 else
-              f"setp.geu.or.f32 tslow, tax, {c['GALOP_TRIG_FAST_LIMIT']}, tslow;"]
+        return [f"mov.b32 tq, {jr};",
+                "add.u32 tq, tq, tcos;",
+                "and.b32 tb, tq, 1;",
+                "setp.ne.u32 tpq, tb, 0;",
+                f"selp.f32 ty, {cv}, {sv}, tpq;",
+                "shl.b32 tt, tq, 30;",
+                f"mov.b32 tw, {x};",
+                "and.b32 tw, tw, tmask;",
+                "xor.b32 tt, tt, tw;",
+                "and.b32 tt, tt, 0x80000000;",
+                "mov.b32 tw, ty;",
+                "xor.b32 tw, tw, tt;",
+                f"mov.b32 fo{q}, tw;",
+                f"setp.geu.f32 tslow, {ax}, {lim};" if q == 0 else
+                f"setp.geu.or.f32 tslow, {ax}, {lim}, tslow;"]
+
+    R = ["R_%=:", "sub.u32 tmask, tcos, 1;"]
+    if k >= 2:
+        # two elements per f32x2 instruction; the constants as register pairs
+        R += [f"mov.b64 {n}, 0x{v[2:] * 2};" for n, v in trig_pair_constants(c).items()]
+        for j in range(k // 2):
+            R += [f"abs.f32 tax0, {a(2 * j)};", f"abs.f32 tax1, {a(2 * j + 1)};", "mov.b64 xax, {tax0, tax1};",
+                  "fma.rn.f32x2 xjr, xax, k2pi, kround;",
+                  "sub.rn.f32x2 xj, xjr, kround;",
+                  "fma.rn.f32x2 xtr, xj, knp1, xax;",
+                  "fma.rn.f32x2 xtr, xj, knp2, xtr;",
+                  "fma.rn.f32x2 xtr, xj, knp3, xtr;",
+                  "mul.rn.f32x2 xz, xtr, xtr;",
+                  "fma.rn.f32x2 xp, xz, ks3, ks2;",
+                  "fma.rn.f32x2 xp, xp, xz, ks1;",
+                  "mul.rn.f32x2 xrz, xtr, xz;",
+                  "fma.rn.f32x2 xs, xrz, xp, xtr;",
+                  "fma.rn.f32x2 xtc, xz, kc4, kc3;",
+                  "fma.rn.f32x2 xtc, xtc, xz, kc2;",
+                  "fma.rn.f32x2 xtc, xtc, xz, kc1;",
+                  "fma.rn.f32x2 xtc, xtc, xz, kone;",
+                  "mov.b64 {tjr0, tjr1}, xjr;", "mov.b64 {ts0, ts1}, xs;", "mov.b64 {tc0, tc1}, xtc;"]
+            for e in (0, 1):
+                R += tail(2 * j + e, f"tjr{e}", f"ts{e}", f"tc{e}", f"tax{e}")
+    else:
+        for q in range(k):
+            R += [f"abs.f32 tax, {a(q)};",
+                  f"fma.rn.f32 tjr, tax, {c['GT_TWO_OVER_PI']}, {c['GT_ROUND']};",
+                  f"sub.rn.f32 tj, tjr, {c['GT_ROUND']};",
+                  f"fma.rn.f32 tr, tj, {neg_imm(c['GT_P1'])}, tax;",
+                  f"fma.rn.f32 tr, tj, {neg_imm(c['GT_P2'])}, tr;",
+                  f"fma.rn.f32 tr, tj, {neg_imm(c['GT_P3'])}, tr;",
+                  "mul.rn.f32 tz, tr, tr;",
+                  f"fma.rn.f32 tp, tz, {c['GT_S3']}, {c['GT_S2']};",
+                  f"fma.rn.f32 tp, tp, tz, {c['GT_S1']};",
+                  "mul.rn.f32 trz, tr, tz;",
+                  "fma.rn.f32 ts, trz, tp, tr;",
+                  f"fma.rn.f32 tc, tz, {c['GT_C4']}, {c['GT_C3']};",
+                  f"fma.rn.f32 tc, tc, tz, {c['GT_C2']};",
+                  f"fma.rn.f32 tc, tc, tz, {c['GT_C1']};",
+                  "fma.rn.f32 tc, tc, tz, 0f3F800000;"]
+            R += tail(q, "tjr", "ts", "tc", "tax")
     R += ["vote.sync.any.pred tany, tslow, 0xffffffff;", "@tany bra.uni Z_%=;"]
     R += [f"mov.f32 {a(q)}, fo{q};" for q in range(k)]
     R += ["setp.ne.u32 tpq, th, 0;", "@tpq bra.uni LB%=;", "bra.uni LA%=;"]
@@ -264,24 +332,78 @@ def div_group(k: int, const: bool, a, b, nm: str) -> tuple[list[str], list[str]]
     evaluate all K elements with wide_body's div.rn path, which reads a[q]
     and b[q] unchanged, and jump back to W<nm>.  Fast and exact agree bit
     for bit wherever the fast path is in range (tests/test_gpu_division.py).
-    (Leaving the loop for a division in C++ instead, to keep these blocks
+    For K >= 2 the Newton-Raphson and Markstein steps run on element pairs
+    (div_pair_lines), the same operations two at a time.
+    (Leaving the loop for a division in C++ instead, to keep the V blocks
     out of the loop's code, was slower.)"""
     bq = (lambda q: "c") if const else b
     hot = []
-    if const:
-        hot += div_divisor_lines("c")
-    for q in range(k):
-        if not const:
-            hot += div_divisor_lines(bq(q))
-        lines = div_fast_lines(a(q), f"fo{q}")
-        if q == 0:
-            lines[-1] = "mov.pred fall, fa;"
-        hot += lines
+    if k >= 2:
+        hot += ["mov.b64 xone, 0x3F8000003F800000;"]
+        if const:
+            hot += div_divisor_lines("c")
+            hot += ["mov.b64 xy, {fy, fy};", "mov.b64 xnb, {fnb, fnb};"]
+        for j in range(k // 2):
+            hot += div_pair_lines(a(2 * j), a(2 * j + 1), bq(2 * j), bq(2 * j + 1), f"fo{2 * j}",
+                                  f"fo{2 * j + 1}", const, first=(j == 0))
+    else:
+        if const:
+            hot += div_divisor_lines("c")
+        for q in range(k):
+            if not const:
+                hot += div_divisor_lines(bq(q))
+            lines = div_fast_lines(a(q), f"fo{q}")
+            if q == 0:
+                lines[-1] = "mov.pred fall, fa;"
+            hot += lines
     hot += ["vote.sync.all.pred funi, fall, 0xffffffff;", f"@!funi bra.uni V{nm};"]
     hot += [f"mov.f32 {a(q)}, fo{q};" for q in range(k)]
     hot.append(f"W{nm}:")
     exact = wide_body(k, 3, const, a=a, b=b, t=a)
     return hot, exact
+
+
+def div_pair_lines(a0: str, a1: str, b0: str, b1: str, o0: str, o1: str, const: bool,
+                   first: bool) -> list[str]:
+    """div_divisor_lines and div_fast_lines for two elements, the float
+    steps as f32x2 pairs: the reciprocal refinement (register divisors; a
+    constant divisor's xy/xnb are set once), then q0 = a y, r = a - b q0,
+    q = q0 + r y.  The per-element rest (sign of a zero quotient, the zero
+    divisor's 1.0, the range tests) is div_fast_lines' own.  fall starts
+    with the first pair."""
+    L = []
+    if not const:
+        L += [f"rcp.approx.ftz.f32 fy0, {b0};", f"rcp.approx.ftz.f32 fy1, {b1};",
+              f"neg.f32 fnb0, {b0};", f"neg.f32 fnb1, {b1};",
+              "mov.b64 xy, {fy0, fy1};", "mov.b64 xnb, {fnb0, fnb1};",
+              "fma.rn.f32x2 xe, xnb, xy, xone;",
+              "fma.rn.f32x2 xy, xy, xe, xy;"]
+    L += [f"mov.b64 xa, {{{a0}, {a1}}};",
+          "mul.rn.f32x2 xq, xa, xy;",
+          "fma.rn.f32x2 xr, xnb, xq, xa;",
+          "fma.rn.f32x2 xr, xr, xy, xq;",
+          "mov.b64 {fq0, fq1}, xq;",
+          "mov.b64 {fg0, fg1}, xr;"]
+    for e, (ae, be, oe, fqe, fge) in enumerate(((a0, b0, o0, "fq0", "fg0"), (a1, b1, o1, "fq1", "fg1"))):
+        if not const:
+            L += [f"abs.f32 fab, {be};",
+                  f"setp.ge.f32 fbok, fab, {DIV_LO};",
+                  f"setp.le.and.f32 fbok, fab, {DIV_HI}, fbok;",
+                  f"setp.eq.f32 fb0, {be}, 0f00000000;"]
+        L += [f"mov.b32 fs, {fqe};",
+              "and.b32 fs, fs, 0x80000000;",
+              f"mov.b32 fw, {fge};",
+              "or.b32 fw, fw, fs;",
+              "mov.b32 fq, fw;",
+              f"selp.f32 {oe}, 0f3F800000, fq, fb0;",
+              f"setp.eq.f32 fz, {ae}, 0f00000000;",
+              f"abs.f32 fab, {ae};",
+              f"setp.ge.or.f32 fa, fab, {DIV_LO}, fz;",
+              f"setp.le.and.f32 fa, fab, {DIV_HI}, fa;",
+              "and.pred fa, fa, fbok;",
+              "or.pred fa, fa, fb0;",
+              "mov.pred fall, fa;" if first and e == 0 else "and.pred fall, fall, fa;"]
+    return L
 
 
 def _vec(regs: list[str]) -> str:
@@ -385,7 +507,7 @@ def wide_loop(k: int, profile: int) -> str:
                 for q in range(nq)]
 
     bregs = lambda q: f"b{q}"
-    L = [f".reg .f32 b<{k}>, fo<{k}>, c;", WIDE_TEMPS, DIV_TEMPS, TRIG_TEMPS, ".reg .pred q;",
+    L = [f".reg .f32 b<{k}>, fo<{k}>, c;", WIDE_TEMPS, DIV_TEMPS, PAIR_TEMPS, TRIG_TEMPS, ".reg .pred q;",
          ".reg .u32 ux, uy, uz, uw, vx, vy, vz, vw, pa, pb;",
          f"mov.b32 ux, {CUR[0]}; mov.b32 uy, {CUR[1]}; mov.b32 uz, {CUR[2]}; mov.b32 uw, {CUR[3]};"]
     entry = {(1, 0): "S", (0, 0): "L", (0, 1): "F", (1, 1): "G"}
@@ -418,6 +540,8 @@ def wide_loop(k: int, profile: int) -> str:
                     hot, exact = div_group(k, bool(cst), A, bregs, nm)
                     body += hot
                     cold.append(f"V{nm}: " + " ".join(exact + [f"bra.uni W{nm};"]))
+                elif op in X2 and k >= 2:
+                    body += pair_body(k, op, bool(cst), A, bregs)
                 else:
                     body += wide_body(k, op, bool(cst), a=A, b=bregs, t=A)
                 L.append(f"F{nm}: " + " ".join(body + nxt_jump))
