@@ -14,7 +14,12 @@ for K = 1, f32x2 pairs otherwise):
     operands in its range, register and constant divisors, and its vote
     fails for an operand out of range.  rcp.approx is taken here as the
     correctly rounded reciprocal (flushed like .ftz); the instruction itself
-    is checked on the B200 by tests/test_gpu_division.py.
+    is checked on the B200 by tests/test_gpu_division.py;
+  - the whole loop (jump tables, both copies, the S/L/F/G entry points,
+    the exact-division blocks, the trig exits, the window end), run with a
+    shared memory of words under a restatement of the kernel's pass for one
+    warp, gives the oracle's per-case outputs on random and chained
+    programs; a loop that does not end fails on a step limit.
 """
 from __future__ import annotations
 
@@ -360,3 +365,271 @@ def test_div_vote_fails_out_of_range(k):
         e = Ptx(n, regs)
         e.run(statements(hot))
         assert e.stopped == "VA30_%=", (k, bad_a, bad_b)
+
+
+# --- the whole loop -----------------------------------------------------------------------
+
+def loop_statements(k: int, profile: int):
+    """The WideLoop asm block of (k, profile): executable statements, the
+    statement index of every label, and the jump tables."""
+    text = G.wide_loop(k, profile)
+    body = text.split('asm volatile("{\\n\\t', 1)[1].split('\\n\\t}"', 1)[0]
+    prog, labels, tables = [], {}, {}
+    for ln in body.split("\\n\\t"):
+        for st in ln.split(";"):
+            st = st.strip()
+            while True:
+                m = re.match(r"^([A-Za-z_][\w%=]*):\s*(.*)$", st)
+                if not m:
+                    break
+                lab, st = m.group(1), m.group(2).strip()
+                if st.startswith(".branchtargets"):
+                    tables[lab] = [t.strip() for t in st[len(".branchtargets"):].split(",")]
+                    st = ""
+                    break
+                labels[lab] = len(prog)
+            if st and not st.startswith(".reg"):
+                prog.append(st)
+    return prog, labels, tables
+
+
+class Loop(Ptx):
+    """Ptx with control flow and a shared memory of 32-bit words."""
+
+    def __init__(self, k: int, profile: int, n: int, regs: dict, mem: np.ndarray):
+        super().__init__(n, regs)
+        self.prog, self.labels, self.tables = loop_statements(k, profile)
+        self.mem = mem
+        self.hits = set()                  # jump-table entries taken
+
+    def execute(self, limit: int = 100_000) -> None:
+        pc, steps = 0, 0
+        while pc < len(self.prog):
+            steps += 1
+            assert steps < limit, "the loop does not end"
+            st = self.prog[pc]
+            pc += 1
+            m = re.match(r"(@!?\w+\s+)?(\S+)\s*(.*)$", st)
+            guard, op, rest = m.group(1), m.group(2), m.group(3)
+            p = None
+            if guard:
+                g = guard.strip()
+                p = self.r[g[1:].lstrip("!")]
+                if g.startswith("@!"):
+                    p = ~p
+            if op.startswith("bra"):
+                if p is not None:
+                    assert p.all() or not p.any(), "a branch that is not uniform"
+                if p is None or p[0]:
+                    pc = self.labels[rest.strip()]
+                continue
+            args = [a.strip() for a in re.findall(r"\s*(\{[^}]*\}|\[[^\]]*\]|[^,{\[]+)", rest)]
+            if op == "brx.idx.uni":
+                idx = self.val(args[0])
+                assert (idx == idx[0]).all(), "a jump that is not uniform"
+                target = self.tables[args[1]][int(idx[0])]
+                self.hits.add(target)
+                pc = self.labels[target]
+                continue
+            if p is None:
+                getattr(self, "op_" + op.replace(".", "_"))(*args)
+            else:                           # a guarded instruction: per-lane result
+                old = self.r.get(args[0])
+                getattr(self, "op_" + op.replace(".", "_"))(*args)
+                self.r[args[0]] = np.where(p, self.r[args[0]], old).astype(np.uint32)
+
+    def _addr(self, a: str) -> np.ndarray:
+        reg, _, off = a.strip()[1:-1].partition("+")
+        return (self.val(reg).astype(np.int64) + int(off or 0)) // 4
+
+    def _regs(self, t: str) -> list[str]:
+        t = t.strip()
+        return [x.strip() for x in t[1:-1].split(",")] if t.startswith("{") else [t]
+
+    def _ld(self, d, a):
+        w = self._addr(a)
+        for i, name in enumerate(self._regs(d)):
+            self.r[name] = self.mem[w + i].copy()
+
+    def _st(self, a, s):
+        w = self._addr(a)
+        for i, name in enumerate(self._regs(s)):
+            self.mem[w + i] = self.val(name)
+
+    op_ld_shared_v4_u32 = op_ld_shared_v4_f32 = op_ld_shared_v2_f32 = op_ld_shared_f32 = _ld
+    op_st_shared_v4_f32 = op_st_shared_v2_f32 = op_st_shared_f32 = _st
+
+    def op_set_lt_f32_f32(self, d, a, b):
+        with np.errstate(all="ignore"):
+            self.r[d] = np.where(_f(self.val(a)) < _f(self.val(b)), np.uint32(0x3F800000), np.uint32(0))
+
+    def op_set_gt_f32_f32(self, d, a, b):
+        with np.errstate(all="ignore"):
+            self.r[d] = np.where(_f(self.val(a)) > _f(self.val(b)), np.uint32(0x3F800000), np.uint32(0))
+
+    def op_div_rn_f32(self, d, a, b): self._arith(lambda x, y: x / y, d, a, b)
+
+
+END = 0xFFFFFFFF
+
+
+def micro_ops(words: np.ndarray, S: int, consts: np.ndarray) -> np.ndarray:
+    """The 16-byte micro-ops of a raw REF program without folding or
+    renaming (register r at slot r): encode_wide, the forwarding flags as
+    the folding pass sets them (fwd1/fwd2 where the operand is the previous
+    destination; store_prev unless the next instruction is the previous
+    result's only reader, through its forwarded operand -- fold.cuh's
+    needs_store, with the output register read after the last
+    instruction), and SIN/COS of a register in the loop's unary form."""
+    ins = []
+    for w in (int(x) for x in words):
+        op, dest, s1, s2, c = w & 7, (w >> 8) & 15, (w >> 16) & 15, (w >> 24) & 15, w >> 31
+        ins.append((op, dest, s1, s2, c, op in (4, 5)))
+    n = len(ins)
+    live_after = [set() for _ in range(n)]
+    live = {0}
+    for j in range(n - 1, -1, -1):
+        live_after[j] = set(live)
+        op, dest, s1, s2, c, unary = ins[j]
+        live = (live - {dest}) | ({s1} if not unary else set()) | ({s2} if not c else set())
+    u = []
+    for j, (op, dest, s1, s2, c, unary) in enumerate(ins):
+        flags = 0
+        if j > 0:
+            d = ins[j - 1][1]
+            fwd = (not unary and s1 == d) or (unary and not c and s2 == d)
+            if fwd:
+                flags |= 64 if unary else 16
+            loads_d = not unary and not c and s2 == d
+            read_later = d != dest and d in live_after[j]
+            if not (fwd and not loads_d and not read_later):
+                flags |= 32
+        y = int(consts[s2].view(np.uint32)) if c else s2 * S
+        if unary and not c:
+            u.append([y, 0, dest * S, op | (16 if flags & 64 else 0) | (flags & 32)])
+        else:
+            u.append([0 if unary else s1 * S, y, dest * S, op | (c << 3) | flags | (0x80000000 if unary else 0)])
+    return np.array(u, dtype=np.uint32).reshape(-1, 4)
+
+
+def run_program(k: int, words: np.ndarray, X: np.ndarray, trig) -> np.ndarray:
+    """interp_wide_kernel's pass over 32*K cases for one warp (16-slot file,
+    the ISA's register layout), with the generated loop emulated."""
+    from galop_b200 import REF_CONSTANTS_16
+    nr, V, S = 16, min(k, 4), 128 * k
+    stage = nr * S
+    mem = np.zeros((stage + 34 * 16) // 4, dtype=np.uint32)
+    lanes = np.arange(32)
+    base = (lanes * V * 4).astype(np.uint32)
+
+    def slot_words(r):   # word index of element e of every lane in slot r
+        return [(base.astype(np.int64) + r * S + (e // V) * 128 * V + (e % V) * 4) // 4 for e in range(k)]
+
+    case = [(e // V) * 32 * V + lanes * V + (e % V) for e in range(k)]
+    for r in range(nr):
+        for e, w in enumerate(slot_words(r)):
+            mem[w] = _u(X[case[e], r]) if r < X.shape[1] else 0
+    u = micro_ops(words, S, REF_CONSTANTS_16)
+    hits = set()
+    A = [np.zeros(32, np.uint32) for _ in range(k)]
+    pt = np.zeros(32, np.uint32)
+    for w0 in range(0, len(u), 32):
+        win = u[w0:w0 + 32]
+        mem[stage // 4: stage // 4 + 4 * len(win)] = win.ravel()
+        mem[stage // 4 + 4 * len(win): stage // 4 + 4 * len(win) + 4] = [0, 0, 0, END]
+        sp = stage
+        while True:
+            cur = mem[sp // 4: sp // 4 + 4]
+            regs = {"%0": np.full(32, sp, np.uint32), f"%{k + 1}": pt, f"%{k + 6}": base}
+            regs.update({f"%{1 + q}": A[q] for q in range(k)})
+            regs.update({f"%{k + 7 + i}": np.full(32, cur[i], np.uint32) for i in range(4)})
+            e = Loop(k, 0, 32, regs, mem)
+            e.execute()
+            hits |= e.hits
+            sp = int(e.r["%0"][0])
+            A = [e.r[f"%{1 + q}"] for q in range(k)]
+            pt = e.r[f"%{k + 1}"]
+            lv = [int(e.r[f"%{k + 2 + i}"][0]) for i in range(4)]
+            if lv[3] == END:
+                break
+            op = lv[3] & 7
+            if not lv[3] & 0x80000000:     # a SIN/COS left for the slow path
+                b = A
+            else:
+                if lv[3] & 32:
+                    for q, wq in enumerate(slot_words(0)):
+                        mem[(pt.astype(np.int64) - base) // 4 + wq] = A[q]
+                if lv[3] & 8:
+                    b = [np.full(32, lv[1], np.uint32) for _ in range(k)]
+                elif lv[3] & 64:
+                    b = A
+                else:
+                    b = [mem[w + lv[1] // 4] for w in slot_words(0)]
+            A = [_u(trig(op, _f(b[q]))) for q in range(k)]
+            pt = (base + lv[2]).astype(np.uint32)
+            sp += 16
+    out_addr = base + 0 * S
+    if len(u) and (pt == out_addr).all():
+        o = A
+    else:
+        o = [mem[w] for w in slot_words(0)]
+    res = np.empty(32 * k, np.float32)
+    for e in range(k):
+        res[case[e]] = _f(o[e])
+    return res, hits
+
+
+def chained(rng, L: int) -> np.ndarray:
+    """L instructions over registers 0-5, each reading the previous result
+    with probability 0.6 (forwarded src1, or a unary op's operand) and
+    otherwise an earlier register, the last one writing the output
+    register: nearly every instruction reaches the output, stored results
+    are read again further down."""
+    from galop_b200 import workloads as W
+    prev, ins = 0, []
+    for _ in range(L):
+        s1 = prev if rng.random() < 0.6 else int(rng.integers(0, 6))
+        s2 = prev if rng.random() < 0.3 else int(rng.integers(0, 6))
+        ins.append([int(rng.integers(0, 8)), int(rng.integers(0, 6)), s1, s2, int(rng.random() < 0.2)])
+        prev = ins[-1][1]
+    ins[-1][1] = 0
+    return W.encode(*np.array(ins, dtype=np.int64).T)
+
+
+@pytest.mark.parametrize("k", G.KS)
+def test_whole_loop_against_the_oracle(oracle_lib, k):
+    """Random REF programs (every op, register and constant operands) and
+    chained ones (forwarded operands, deferred stores read back), of 1 to 80
+    instructions across 32-instruction windows, through the emulated loop
+    and its caller equal the oracle with trig.cuh's host build, per case,
+    bit for bit, until every jump-table entry of both loop copies that
+    these micro-ops can select has run.  A few cases hold arguments for the
+    slow trig path and operands for the exact division."""
+    from galop_b200 import workloads as W
+    rng = np.random.default_rng(90 + k)
+    dev = oracle_lib.Oracle(oracle_lib.PROFILE_REF, 16, trig=oracle_lib.TRIG_DEVICE)
+    trig = lambda op, x: dev.apply_op_n(op, x, x)
+    n = 32 * k
+    X = rng.uniform(-3, 3, (n, 4)).astype(np.float32)
+    X[rng.choice(n, 3, replace=False), 1] = np.float32([2e5, 1e-30, 0.0])
+    progs = [W.random_words(rng, L, 16) for L in (1, 2, 7, 31, 32, 33, 80)]
+    # every entry of both copies' tables that these micro-ops can select:
+    # no broadcast arms (nothing is folded here), and copy B's L entries
+    # (neither flag) never run -- such a micro-op is the first of a pass or
+    # the first after the loop was left, and those run in copy A
+    _, _, tables = loop_statements(k, 0)
+    reachable = {t for tab in tables.values() for t in tab
+                 if not t.startswith(("X", "LB")) and "B_" not in t}
+    hit = set()
+    i = 0
+    while True:
+        words = progs[i] if i < len(progs) else chained(rng, int(rng.integers(3, 80)))
+        i += 1
+        want = dev.case_outputs(words, X)
+        got, h = run_program(k, words, X, trig)
+        hit |= h
+        same = (bits(got) == bits(want)) | (np.isnan(got) & np.isnan(want))
+        assert same.all(), (k, len(words), int((~same).sum()))
+        if i >= len(progs) and hit >= reachable:
+            break
+        assert i < 400, sorted(reachable - hit)[:8]
