@@ -23,6 +23,7 @@ for K = 1, f32x2 pairs otherwise):
 """
 from __future__ import annotations
 
+import functools
 import re
 import sys
 
@@ -369,9 +370,11 @@ def test_div_vote_fails_out_of_range(k):
 
 # --- the whole loop -----------------------------------------------------------------------
 
+@functools.lru_cache(maxsize=None)
 def loop_statements(k: int, profile: int):
-    """The WideLoop asm block of (k, profile): executable statements, the
-    statement index of every label, and the jump tables."""
+    """The WideLoop asm block of (k, profile): executable statements as
+    (guard, op, operands), the statement index of every label, and the jump
+    tables."""
     text = G.wide_loop(k, profile)
     body = text.split('asm volatile("{\\n\\t', 1)[1].split('\\n\\t}"', 1)[0]
     prog, labels, tables = [], {}, {}
@@ -389,7 +392,9 @@ def loop_statements(k: int, profile: int):
                     break
                 labels[lab] = len(prog)
             if st and not st.startswith(".reg"):
-                prog.append(st)
+                m = re.match(r"(@!?\w+\s+)?(\S+)\s*(.*)$", st)
+                args = [a.strip() for a in re.findall(r"\s*(\{[^}]*\}|\[[^\]]*\]|[^,{\[]+)", m.group(3))]
+                prog.append(((m.group(1) or "").strip(), m.group(2), tuple(args)))
     return prog, labels, tables
 
 
@@ -407,23 +412,19 @@ class Loop(Ptx):
         while pc < len(self.prog):
             steps += 1
             assert steps < limit, "the loop does not end"
-            st = self.prog[pc]
+            guard, op, args = self.prog[pc]
             pc += 1
-            m = re.match(r"(@!?\w+\s+)?(\S+)\s*(.*)$", st)
-            guard, op, rest = m.group(1), m.group(2), m.group(3)
             p = None
             if guard:
-                g = guard.strip()
-                p = self.r[g[1:].lstrip("!")]
-                if g.startswith("@!"):
+                p = self.r[guard[1:].lstrip("!")]
+                if guard.startswith("@!"):
                     p = ~p
             if op.startswith("bra"):
                 if p is not None:
                     assert p.all() or not p.any(), "a branch that is not uniform"
                 if p is None or p[0]:
-                    pc = self.labels[rest.strip()]
+                    pc = self.labels[args[0]]
                 continue
-            args = [a.strip() for a in re.findall(r"\s*(\{[^}]*\}|\[[^\]]*\]|[^,{\[]+)", rest)]
             if op == "brx.idx.uni":
                 idx = self.val(args[0])
                 assert (idx == idx[0]).all(), "a jump that is not uniform"
@@ -473,8 +474,8 @@ class Loop(Ptx):
 END = 0xFFFFFFFF
 
 
-def micro_ops(words: np.ndarray, S: int, consts: np.ndarray) -> np.ndarray:
-    """The 16-byte micro-ops of a raw REF program without folding or
+def micro_ops(words: np.ndarray, S: int, consts: np.ndarray, profile: int = 0) -> np.ndarray:
+    """The 16-byte micro-ops of a raw program without folding or
     renaming (register r at slot r): encode_wide, the forwarding flags as
     the folding pass sets them (fwd1/fwd2 where the operand is the previous
     destination; store_prev unless the next instruction is the previous
@@ -484,7 +485,7 @@ def micro_ops(words: np.ndarray, S: int, consts: np.ndarray) -> np.ndarray:
     ins = []
     for w in (int(x) for x in words):
         op, dest, s1, s2, c = w & 7, (w >> 8) & 15, (w >> 16) & 15, (w >> 24) & 15, w >> 31
-        ins.append((op, dest, s1, s2, c, op in (4, 5)))
+        ins.append((op, dest, s1, s2, c, op in (4, 5) or (profile == 1 and op in (6, 7))))
     n = len(ins)
     live_after = [set() for _ in range(n)]
     live = {0}
@@ -505,14 +506,14 @@ def micro_ops(words: np.ndarray, S: int, consts: np.ndarray) -> np.ndarray:
             if not (fwd and not loads_d and not read_later):
                 flags |= 32
         y = int(consts[s2].view(np.uint32)) if c else s2 * S
-        if unary and not c:
+        if op in (4, 5) and not c:
             u.append([y, 0, dest * S, op | (16 if flags & 64 else 0) | (flags & 32)])
         else:
             u.append([0 if unary else s1 * S, y, dest * S, op | (c << 3) | flags | (0x80000000 if unary else 0)])
     return np.array(u, dtype=np.uint32).reshape(-1, 4)
 
 
-def run_program(k: int, words: np.ndarray, X: np.ndarray, trig) -> np.ndarray:
+def run_program(k: int, words: np.ndarray, X: np.ndarray, unary, profile: int = 0) -> np.ndarray:
     """interp_wide_kernel's pass over 32*K cases for one warp (16-slot file,
     the ISA's register layout), with the generated loop emulated."""
     from galop_b200 import REF_CONSTANTS_16
@@ -529,7 +530,7 @@ def run_program(k: int, words: np.ndarray, X: np.ndarray, trig) -> np.ndarray:
     for r in range(nr):
         for e, w in enumerate(slot_words(r)):
             mem[w] = _u(X[case[e], r]) if r < X.shape[1] else 0
-    u = micro_ops(words, S, REF_CONSTANTS_16)
+    u = micro_ops(words, S, REF_CONSTANTS_16, profile)
     hits = set()
     A = [np.zeros(32, np.uint32) for _ in range(k)]
     pt = np.zeros(32, np.uint32)
@@ -543,7 +544,7 @@ def run_program(k: int, words: np.ndarray, X: np.ndarray, trig) -> np.ndarray:
             regs = {"%0": np.full(32, sp, np.uint32), f"%{k + 1}": pt, f"%{k + 6}": base}
             regs.update({f"%{1 + q}": A[q] for q in range(k)})
             regs.update({f"%{k + 7 + i}": np.full(32, cur[i], np.uint32) for i in range(4)})
-            e = Loop(k, 0, 32, regs, mem)
+            e = Loop(k, profile, 32, regs, mem)
             e.execute()
             hits |= e.hits
             sp = int(e.r["%0"][0])
@@ -565,7 +566,7 @@ def run_program(k: int, words: np.ndarray, X: np.ndarray, trig) -> np.ndarray:
                     b = A
                 else:
                     b = [mem[w + lv[1] // 4] for w in slot_words(0)]
-            A = [_u(trig(op, _f(b[q]))) for q in range(k)]
+            A = [_u(unary(op, _f(b[q]))) for q in range(k)]
             pt = (base + lv[2]).astype(np.uint32)
             sp += 16
     out_addr = base + 0 * S
@@ -597,18 +598,21 @@ def chained(rng, L: int) -> np.ndarray:
 
 
 @pytest.mark.parametrize("k", G.KS)
-def test_whole_loop_against_the_oracle(oracle_lib, k):
+@pytest.mark.parametrize("profile", [0, 1])
+def test_whole_loop_against_the_oracle(oracle_lib, k, profile):
     """Random REF programs (every op, register and constant operands) and
     chained ones (forwarded operands, deferred stores read back), of 1 to 80
     instructions across 32-instruction windows, through the emulated loop
     and its caller equal the oracle with trig.cuh's host build, per case,
     bit for bit, until every jump-table entry of both loop copies that
     these micro-ops can select has run.  A few cases hold arguments for the
-    slow trig path and operands for the exact division."""
+    slow trig path and operands for the exact division.  The BJ profile's
+    EXP/LOG leave the loop for the caller, which evaluates them here with
+    the oracle's own functions."""
     from galop_b200 import workloads as W
-    rng = np.random.default_rng(90 + k)
-    dev = oracle_lib.Oracle(oracle_lib.PROFILE_REF, 16, trig=oracle_lib.TRIG_DEVICE)
-    trig = lambda op, x: dev.apply_op_n(op, x, x)
+    rng = np.random.default_rng(90 + k + 7 * profile)
+    dev = oracle_lib.Oracle(profile, 16, trig=oracle_lib.TRIG_DEVICE)
+    unary = lambda op, x: dev.apply_op_n(op, x, x)
     n = 32 * k
     X = rng.uniform(-3, 3, (n, 4)).astype(np.float32)
     X[rng.choice(n, 3, replace=False), 1] = np.float32([2e5, 1e-30, 0.0])
@@ -617,7 +621,7 @@ def test_whole_loop_against_the_oracle(oracle_lib, k):
     # no broadcast arms (nothing is folded here), and copy B's L entries
     # (neither flag) never run -- such a micro-op is the first of a pass or
     # the first after the loop was left, and those run in copy A
-    _, _, tables = loop_statements(k, 0)
+    _, _, tables = loop_statements(k, profile)
     reachable = {t for tab in tables.values() for t in tab
                  if not t.startswith(("X", "LB")) and "B_" not in t}
     hit = set()
@@ -626,7 +630,7 @@ def test_whole_loop_against_the_oracle(oracle_lib, k):
         words = progs[i] if i < len(progs) else chained(rng, int(rng.integers(3, 80)))
         i += 1
         want = dev.case_outputs(words, X)
-        got, h = run_program(k, words, X, trig)
+        got, h = run_program(k, words, X, unary, profile)
         hit |= h
         same = (bits(got) == bits(want)) | (np.isnan(got) & np.isnan(want))
         assert same.all(), (k, len(words), int((~same).sum()))
