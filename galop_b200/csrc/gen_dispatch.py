@@ -42,6 +42,8 @@ Run by hand: python galop_b200/csrc/gen_dispatch.py
 """
 from __future__ import annotations
 
+import re
+import struct
 from pathlib import Path
 
 KS = (1, 2, 4, 8)
@@ -190,6 +192,8 @@ def div_fast_lines(a: str, out: str) -> list[str]:
             "and.pred fall, fall, fa;"]
 
 
+# Scratch registers of the SIN/COS block (trig_blocks): per element, per
+# element pair, and the register pairs that hold the constants.
 TRIG_TEMPS = (".reg .f32 tax, tjr, tj, tr, tz, tp, trz, ts, tc, ty; .reg .b32 tq, tb, tt, tw, th, tcos, tmask; "
               ".reg .pred tpq, tslow, tany; "
               ".reg .f32 tax0, tax1, tjr0, tjr1, ts0, ts1, tc0, tc1; "
@@ -210,13 +214,15 @@ def trig_constants() -> dict:
     """The single-precision constants of trig.cuh's Cody-Waite path as PTX
     immediates (0fXXXXXXXX), read from the header itself so the loop's copy
     of the fast path cannot drift from it."""
-    import re
-    import struct
     text = (Path(__file__).resolve().parent / "trig.cuh").read_text()
     out = {}
     for name, lit in re.findall(r"#define (GT_[A-Z0-9_]+|GALOP_TRIG_FAST_LIMIT) (-?0x[0-9a-fA-Fp.+-]+f|[0-9.]+f)\n", text):
         v = float.fromhex(lit[:-1]) if "0x" in lit else float(lit[:-1])
         out[name] = "0f%08X" % struct.unpack("<I", struct.pack("<f", v))[0]
+    need = {"GALOP_TRIG_FAST_LIMIT", "GT_TWO_OVER_PI", "GT_ROUND", "GT_P1", "GT_P2", "GT_P3",
+            "GT_S1", "GT_S2", "GT_S3", "GT_C1", "GT_C2", "GT_C3", "GT_C4"}
+    if not need <= out.keys():
+        raise RuntimeError(f"trig.cuh: constants not found: {sorted(need - out.keys())}")
     return out
 
 
