@@ -54,13 +54,13 @@ struct FoldParams {
 };
 
 // Operand swap that keeps the result bits: ADD, MUL, and LT <-> GT of REF.
-__device__ __forceinline__ bool swaps(int profile, uint32_t op) {
+__host__ __device__ __forceinline__ bool swaps(int profile, uint32_t op) {
     return op == kAdd || op == kMul || (profile == kProfileRef && (op == kOp6 || op == kOp7));
 }
 
 // Registers a micro-op reads (broadcasts none, unary ops only src2, a
 // constant src2 none).
-__device__ __forceinline__ uint32_t uop_reads(const uint4& w, uint32_t sh) {
+__host__ __device__ __forceinline__ uint32_t uop_reads(const uint4& w, uint32_t sh) {
     if ((w.w & ~kWideFlags) == kWideBcast) return 0u;
     uint32_t r = 0u;
     if (!(w.w & kWideSpecial)) r |= 1u << (w.x >> sh);
@@ -71,7 +71,7 @@ __device__ __forceinline__ uint32_t uop_reads(const uint4& w, uint32_t sh) {
 // fwd1 / fwd2 on micro-op w whose predecessor wrote the register at byte
 // offset prev, swapping the operands of a binary op first when only src2
 // is that register and the swap keeps the result bits.
-__device__ __forceinline__ void set_fwd(uint4& w, uint32_t prev, int profile) {
+__host__ __device__ __forceinline__ void set_fwd(uint4& w, uint32_t prev, int profile) {
     if (w.w == kWideBcast) return;
     const bool reg2 = !(w.w & 8u);
     if (w.w & kWideSpecial) {
@@ -92,7 +92,7 @@ __device__ __forceinline__ void set_fwd(uint4& w, uint32_t prev, int profile) {
 // Whether the result of the instruction before nx (register d) must reach
 // the register file: unless nx takes it forwarded, loads no copy of it, and
 // nothing after nx reads it (live_after_next: registers live after nx).
-__device__ __forceinline__ bool needs_store(const uint4& nx, uint32_t d, uint32_t live_after_next, uint32_t sh) {
+__host__ __device__ __forceinline__ bool needs_store(const uint4& nx, uint32_t d, uint32_t live_after_next, uint32_t sh) {
     const uint32_t nd = nx.z >> sh;
     const bool fwd = (nx.w & (kWideFwd1 | kWideFwd2)) != 0;
     // a binary op loads src2 (never forwarded); src1 equal to d is forwarded
@@ -119,7 +119,7 @@ __device__ __forceinline__ bool needs_store(const uint4& nx, uint32_t d, uint32_
 // Returns the registers the program reads before writing them (the
 // output register counts as read after the last instruction): the only
 // ones the interpreter must initialise before each pass over the cases.
-__device__ __forceinline__ uint32_t mark_forwarding(uint4* __restrict__ u, int64_t n, uint32_t sh, int output_reg,
+__host__ __device__ __forceinline__ uint32_t mark_forwarding(uint4* __restrict__ u, int64_t n, uint32_t sh, int output_reg,
                                                     int profile) {
     for (int64_t j = 1; j < n; ++j) set_fwd(u[j], u[j - 1].z, profile);
     uint32_t live = 1u << output_reg;      // live after instruction j
@@ -136,7 +136,7 @@ __device__ __forceinline__ uint32_t mark_forwarding(uint4* __restrict__ u, int64
 
 // Folds one program in place (constants, dead code, packing, forwarding
 // flags), returns its interpreted length and sets its live-in registers.
-__device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L, const FoldParams& fp,
+__host__ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L, const FoldParams& fp,
                                                  int k_in, uint32_t& livein) {
     const uint32_t sh = fp.stride_shift;
     int64_t kept = 0;
@@ -156,14 +156,14 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
         const bool a_known = unary || ((known >> s1) & 1u);
         const bool b_known = is_const || ((known >> s2) & 1u);
         const float a = a_known && !unary ? vals[s1] : 0.0f;
-        const float b = is_const ? __uint_as_float(w.y) : (b_known ? vals[s2] : 0.0f);
+        const float b = is_const ? galop_float(w.y) : (b_known ? vals[s2] : 0.0f);
         // Results known whatever the other operand: protected division by a
         // zero (src/ISA.h:224: 1.0 for every dividend, NaN included), and
         // LT/GT of the REF profile with a NaN operand (0.0: ordered
         // comparisons with NaN are false).
         const bool div0 = !unary && op == kDiv && b_known && b == 0.0f;
         const bool cmp_nan = fp.profile == kProfileRef && (op == kOp6 || op == kOp7) &&
-                             ((a_known && isnan(a)) || (b_known && isnan(b)));
+                             ((a_known && a != a) || (b_known && b != b));
         if ((a_known && b_known) || div0 || cmp_nan) {
             const float v = div0 ? 1.0f
                           : cmp_nan ? 0.0f
@@ -171,13 +171,13 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
                                                      : apply_op<kProfileRef>(op, a, b);
             vals[d] = v;
             known |= 1u << d;
-            u[j] = make_uint4(0u, __float_as_uint(v), w.z, kWideBcast);
+            u[j] = make_uint4(0u, galop_bits(v), w.z, kWideBcast);
         } else {
             if (!unary && b_known && !is_const) {
-                u[j] = make_uint4(w.x, __float_as_uint(b), w.z, w.w | 8u);
+                u[j] = make_uint4(w.x, galop_bits(b), w.z, w.w | 8u);
             } else if (!unary && a_known && swaps(fp.profile, op)) {
                 const uint32_t sop = op == kOp6 ? (uint32_t)kOp7 : op == kOp7 ? (uint32_t)kOp6 : op;
-                u[j] = make_uint4(w.y, __float_as_uint(a), w.z, (w.w & ~7u) | sop | 8u);
+                u[j] = make_uint4(w.y, galop_bits(a), w.z, (w.w & ~7u) | sop | 8u);
             }
             known &= ~(1u << d);
         }
@@ -248,7 +248,7 @@ __device__ __forceinline__ int64_t fold_program(uint4* __restrict__ u, int64_t L
 constexpr uint32_t kDies1 = 1u << 8;    // src1's value is not read after this instruction
 constexpr uint32_t kDies2 = 1u << 9;    // the same for a register src2
 
-__device__ __forceinline__ uint32_t rename_slots(uint4* __restrict__ u, int64_t n, uint32_t sh, int output_reg,
+__host__ __device__ __forceinline__ uint32_t rename_slots(uint4* __restrict__ u, int64_t n, uint32_t sh, int output_reg,
                                                  uint32_t livein) {
     // backward: mark the reads whose values end at their instruction
     uint32_t live = 1u << output_reg;   // registers live after instruction j
@@ -273,7 +273,7 @@ __device__ __forceinline__ uint32_t rename_slots(uint4* __restrict__ u, int64_t 
     for (int r = 0; r < kMaxRegisters; ++r) slot_of[r] = -1;
     uint32_t used = 0u, top = 0u;
     for (uint32_t m = livein & 0xFFFFu; m != 0u; m &= m - 1u) {
-        const int r = __ffs(m) - 1;
+        const int r = galop_ffs(m) - 1;
         slot_of[r] = (int8_t)top;
         used |= 1u << top;
         ++top;
@@ -299,7 +299,7 @@ __device__ __forceinline__ uint32_t rename_slots(uint4* __restrict__ u, int64_t 
             used &= ~(1u << slot_of[d]);
             slot_of[d] = -1;
         }
-        const uint32_t p = (uint32_t)(__ffs(~used) - 1);
+        const uint32_t p = (uint32_t)(galop_ffs(~used) - 1);
         used |= 1u << p;
         slot_of[d] = (int8_t)p;
         if (p + 1u > top) top = p + 1u;
@@ -320,6 +320,25 @@ __device__ __forceinline__ uint32_t rename_slots(uint4* __restrict__ u, int64_t 
     return pack_livein(livein, top, out);
 }
 
+// One program of fold_kernel: folds u[0, L) in place (forwarding flags only
+// when fp.fold is 0), sets its live-in word and returns its interpreted
+// length.  Host builds run the same code (tests).
+__host__ __device__ __forceinline__ int64_t fold_one(uint4* __restrict__ u, int64_t L, const FoldParams& fp,
+                                                     int k_in, uint32_t& livein) {
+    const uint32_t sh = fp.stride_shift;
+    uint32_t in = 0u;
+    int64_t kept;
+    if (!fp.fold) {
+        in = mark_forwarding(u, L, sh, fp.output_reg, fp.profile);
+        kept = L;
+    } else {
+        kept = fold_program(u, L, fp, k_in, in);
+    }
+    livein = fp.rename ? rename_slots(u + (L - kept), kept, sh, fp.output_reg, in)
+                       : pack_livein(in, (uint32_t)fp.num_registers, (uint32_t)fp.output_reg);
+    return kept;
+}
+
 static __global__ void fold_kernel(uint4* __restrict__ uops, const int64_t* __restrict__ eff_off, int64_t n,
                                    FoldParams fp, int32_t* __restrict__ interp_len,
                                    uint32_t* __restrict__ livein, unsigned long long* __restrict__ total) {
@@ -328,18 +347,10 @@ static __global__ void fold_kernel(uint4* __restrict__ uops, const int64_t* __re
     if (i < n) {
         const int64_t p0 = eff_off[i];
         const int64_t L = eff_off[i + 1] - p0;
-        uint4* __restrict__ u = uops + p0;
-        const uint32_t sh = fp.stride_shift;
         const int k_in = fp.pops ? fp.pops[fp.prog_pop[i]].num_inputs : fp.num_inputs;
-        uint32_t in = 0u;
-        if (!fp.fold) {
-            in = mark_forwarding(u, L, sh, fp.output_reg, fp.profile);
-            kept = L;
-        } else {
-            kept = fold_program(u, L, fp, k_in, in);
-        }
-        livein[i] = fp.rename ? rename_slots(u + (L - kept), kept, sh, fp.output_reg, in)
-                              : pack_livein(in, (uint32_t)fp.num_registers, (uint32_t)fp.output_reg);
+        uint32_t lv;
+        kept = fold_one(uops + p0, L, fp, k_in, lv);
+        livein[i] = lv;
         interp_len[i] = (int32_t)kept;
         if (!fp.fold) kept = 0;
     }

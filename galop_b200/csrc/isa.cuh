@@ -12,6 +12,8 @@
 // ops, so the interpreter decodes with plain byte extracts.
 #pragma once
 #include <cstdint>
+#include <cstring>
+#include <cmath>
 #include <cuda_runtime.h>
 
 #include "trig.cuh"
@@ -131,18 +133,55 @@ __device__ __forceinline__ uint32_t uop_src1(uint32_t u) { return (u >> 16) & 0x
 __device__ __forceinline__ uint32_t uop_src2(uint32_t u) { return (u >> 24) & 0x7fu; }
 __device__ __forceinline__ bool uop_is_const(uint32_t u) { return (u >> 31) != 0u; }
 
+// Bit casts and find-first-set for code that also runs on the host (the
+// folding pass, which tests build for the CPU).
+__host__ __device__ __forceinline__ uint32_t galop_bits(float f) {
+#if defined(__CUDA_ARCH__)
+    return __float_as_uint(f);
+#else
+    uint32_t u;
+    std::memcpy(&u, &f, sizeof u);
+    return u;
+#endif
+}
+__host__ __device__ __forceinline__ float galop_float(uint32_t u) {
+#if defined(__CUDA_ARCH__)
+    return __uint_as_float(u);
+#else
+    float f;
+    std::memcpy(&f, &u, sizeof f);
+    return f;
+#endif
+}
+__host__ __device__ __forceinline__ int galop_ffs(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return __ffs(x);
+#else
+    return __builtin_ffs((int)x);
+#endif
+}
+
 // Op semantics, src/ISA.h:219-231 (REF) and the BJ profile's EXP/LOG.
 // Explicit round-to-nearest intrinsics: no FMA contraction, IEEE division,
 // matching the CPU build (ISO C++, no contraction, SSE2 arithmetic).  SIN
 // and COS are trig.cuh's (within 1.56 ulp of the exact value, as the C
-// library's are within 1 ulp); EXP and LOG are CUDA's.
+// library's are within 1 ulp); EXP and LOG are CUDA's.  A host build
+// (tests) computes the IEEE ops with the host's single-precision
+// arithmetic, the same bits, and EXP/LOG with the C library.
 template <int PROFILE>
-__device__ __forceinline__ float apply_op(uint32_t op, float a, float b) {
+__host__ __device__ __forceinline__ float apply_op(uint32_t op, float a, float b) {
     switch (op) {
+#if defined(__CUDA_ARCH__)
         case kAdd: return __fadd_rn(a, b);
         case kSub: return __fsub_rn(a, b);
         case kMul: return __fmul_rn(a, b);
         case kDiv: return (b != 0.0f) ? __fdiv_rn(a, b) : 1.0f;
+#else
+        case kAdd: return a + b;
+        case kSub: return a - b;
+        case kMul: return a * b;
+        case kDiv: return (b != 0.0f) ? a / b : 1.0f;
+#endif
         case kSin: return galop_sinf(b);
         case kCos: return galop_cosf(b);
         case kOp6:

@@ -513,12 +513,16 @@ def micro_ops(words: np.ndarray, S: int, consts: np.ndarray, profile: int = 0) -
     return np.array(u, dtype=np.uint32).reshape(-1, 4)
 
 
-def run_program(k: int, words: np.ndarray, X: np.ndarray, unary, profile: int = 0) -> np.ndarray:
-    """interp_wide_kernel's pass over 32*K cases for one warp (16-slot file,
-    the ISA's register layout), with the generated loop emulated."""
-    from galop_b200 import REF_CONSTANTS_16
-    nr, V, S = 16, min(k, 4), 128 * k
-    stage = nr * S
+def emulate(k: int, u: np.ndarray, X: np.ndarray, init: dict, out_slot: int, unary, profile: int = 0):
+    """interp_wide_kernel's pass over 32*K cases for one warp, with the
+    generated loop emulated: a 16-slot register file whose slot s starts as
+    input column init[s] (-1: zero), the micro-ops u staged in 32-entry
+    windows, the caller's handling of the micro-ops that leave the loop, and
+    the output taken from the result registers when the last instruction
+    wrote the output slot.  Returns the per-case outputs and the jump-table
+    entries taken."""
+    nslot, V, S = 16, min(k, 4), 128 * k
+    stage = nslot * S
     mem = np.zeros((stage + 34 * 16) // 4, dtype=np.uint32)
     lanes = np.arange(32)
     base = (lanes * V * 4).astype(np.uint32)
@@ -527,10 +531,9 @@ def run_program(k: int, words: np.ndarray, X: np.ndarray, unary, profile: int = 
         return [(base.astype(np.int64) + r * S + (e // V) * 128 * V + (e % V) * 4) // 4 for e in range(k)]
 
     case = [(e // V) * 32 * V + lanes * V + (e % V) for e in range(k)]
-    for r in range(nr):
+    for r, col in init.items():
         for e, w in enumerate(slot_words(r)):
-            mem[w] = _u(X[case[e], r]) if r < X.shape[1] else 0
-    u = micro_ops(words, S, REF_CONSTANTS_16, profile)
+            mem[w] = _u(X[case[e], col]) if col >= 0 else 0
     hits = set()
     A = [np.zeros(32, np.uint32) for _ in range(k)]
     pt = np.zeros(32, np.uint32)
@@ -569,15 +572,24 @@ def run_program(k: int, words: np.ndarray, X: np.ndarray, unary, profile: int = 
             A = [_u(unary(op, _f(b[q]))) for q in range(k)]
             pt = (base + lv[2]).astype(np.uint32)
             sp += 16
-    out_addr = base + 0 * S
+    out_addr = base + out_slot * S
     if len(u) and (pt == out_addr).all():
         o = A
     else:
-        o = [mem[w] for w in slot_words(0)]
+        o = [mem[w] for w in slot_words(out_slot)]
     res = np.empty(32 * k, np.float32)
     for e in range(k):
         res[case[e]] = _f(o[e])
     return res, hits
+
+
+def run_program(k: int, words: np.ndarray, X: np.ndarray, unary, profile: int = 0):
+    """A raw program without folding or renaming (register r in slot r)
+    through emulate()."""
+    from galop_b200 import REF_CONSTANTS_16
+    u = micro_ops(words, 128 * k, REF_CONSTANTS_16, profile)
+    init = {r: (r if r < X.shape[1] else -1) for r in range(16)}
+    return emulate(k, u, X, init, 0, unary, profile)
 
 
 def chained(rng, L: int) -> np.ndarray:
