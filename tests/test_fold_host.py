@@ -43,35 +43,38 @@ def fold_lib(tmp_path_factory):
     return lib
 
 
-def effective_uops(o, words: np.ndarray, S: int, consts: np.ndarray) -> np.ndarray:
-    """The intron pre-pass's output for one REF program: its effective
+def effective_uops(o, words: np.ndarray, S: int, consts: np.ndarray, profile: int) -> np.ndarray:
+    """The intron pre-pass's output for one program: its effective
     instructions in order as wide micro-ops (no flags)."""
     keep = o.effective_mask(words).astype(bool)
     u = []
     for w in (int(x) for x, m in zip(words, keep) if m):
         op, dest, s1, s2, c = w & 7, (w >> 8) & 15, (w >> 16) & 15, (w >> 24) & 15, w >> 31
-        unary = op in (4, 5)
+        unary = op in (4, 5) or (profile == 1 and op in (6, 7))
         u.append([0 if unary else s1 * S, int(consts[s2].view(np.uint32)) if c else s2 * S, dest * S,
                   op | (c << 3) | (0x80000000 if unary else 0)])
     return np.array(u, dtype=np.uint32).reshape(-1, 4)
 
 
-def fold(lib, u: np.ndarray, k: int, k_in: int):
+def fold(lib, u: np.ndarray, k: int, k_in: int, profile: int):
     """(interpreted micro-ops, live-in word) of one program."""
     buf = np.ascontiguousarray(u.copy())
     lv = C.c_uint32()
-    kept = lib.fold_host(buf.ctypes.data_as(C.POINTER(C.c_uint32)), len(u), 0, 16, 0, 7 + (k.bit_length() - 1),
-                         k_in, 1, 1, C.byref(lv))
+    kept = lib.fold_host(buf.ctypes.data_as(C.POINTER(C.c_uint32)), len(u), profile, 16, 0,
+                         7 + (k.bit_length() - 1), k_in, 1, 1, C.byref(lv))
     assert 0 <= kept <= len(u)
     return buf[len(u) - kept:], lv.value
 
 
 @pytest.mark.parametrize("k", [1, 8])
-def test_folded_programs_through_the_loop(oracle_lib, fold_lib, k):
+@pytest.mark.parametrize("profile", [0, 1])
+def test_folded_programs_through_the_loop(oracle_lib, fold_lib, k, profile):
+    """REF and BJ (whose EXP/LOG fold here with the host's C library, the
+    oracle's own functions, and leave the loop for the caller)."""
     from galop_b200 import REF_CONSTANTS_16
     from galop_b200 import workloads as W
-    rng = np.random.default_rng(400 + k)
-    dev = oracle_lib.Oracle(oracle_lib.PROFILE_REF, 16, trig=oracle_lib.TRIG_DEVICE)
+    rng = np.random.default_rng(400 + k + 50 * profile)
+    dev = oracle_lib.Oracle(profile, 16, trig=oracle_lib.TRIG_DEVICE)
     unary = lambda op, x: dev.apply_op_n(op, x, x)
     n, k_in = 32 * k, 3
     X = rng.uniform(-3, 3, (n, k_in)).astype(np.float32)
@@ -80,15 +83,15 @@ def test_folded_programs_through_the_loop(oracle_lib, fold_lib, k):
     progs += [chained(rng, int(L)) for L in rng.integers(2, 80, 40)]
     folded = bcast = 0
     for words in progs:
-        u = effective_uops(dev, words, 128 * k, REF_CONSTANTS_16)
+        u = effective_uops(dev, words, 128 * k, REF_CONSTANTS_16, profile)
         if len(u) == 0:
             continue
-        ui, lv = fold(fold_lib, u, k, k_in)
+        ui, lv = fold(fold_lib, u, k, k_in, profile)
         folded += len(u) - len(ui)
         bcast += int(((ui[:, 3] & ~np.uint32(0x70)) == 12).sum())
         regs = [r for r in range(16) if (lv >> r) & 1]
         init = {i: (r if r < k_in else -1) for i, r in enumerate(regs)}
-        got, _ = emulate(k, ui, X, init, (lv >> 24) & 15, unary)
+        got, _ = emulate(k, ui, X, init, (lv >> 24) & 15, unary, profile)
         want = dev.case_outputs(words, X)
         same = (bits(got) == bits(want)) | (np.isnan(got) & np.isnan(want))
         assert same.all(), (k, len(words), int((~same).sum()))
