@@ -249,6 +249,7 @@ def roofline(eff_instr: float, interp_instr: float, n_cases: int, kernel_ms: flo
             "hbm_view": hbm_view(traffic, kernel_ms, peaks),
             "issue_slots_active": prof.get("issue_slots_active"),
             "achieved_occupancy": prof.get("achieved_occupancy"),
+            "profile_note": prof.get("captured"),
             "traffic_source": (f"ncu capture of {prof.get('programs')} programs x {prof.get('cases')} cases, "
                                f"scaled to {programs_per_launch} programs") if traffic else None}
 
