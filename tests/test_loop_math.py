@@ -372,11 +372,15 @@ def test_div_vote_fails_out_of_range(k):
 
 @functools.lru_cache(maxsize=None)
 def loop_statements(k: int, profile: int):
-    """The WideLoop asm block of (k, profile): executable statements as
+    """The WideLoop asm block of (k, profile), parsed by parse_asm."""
+    return parse_asm(G.wide_loop(k, profile))
+
+
+def parse_asm(text: str):
+    """The one asm block of a generated function: executable statements as
     (guard, op, operands), the statement index of every label, and the jump
     tables."""
-    text = G.wide_loop(k, profile)
-    body = text.split('asm volatile("{\\n\\t', 1)[1].split('\\n\\t}"', 1)[0]
+    body = re.split(r'asm(?: volatile)?\("\{\\n\\t', text, maxsplit=1)[1].split('\\n\\t}"', 1)[0]
     prog, labels, tables = [], {}, {}
     for ln in body.split("\\n\\t"):
         for st in ln.split(";"):
@@ -401,9 +405,9 @@ def loop_statements(k: int, profile: int):
 class Loop(Ptx):
     """Ptx with control flow and a shared memory of 32-bit words."""
 
-    def __init__(self, k: int, profile: int, n: int, regs: dict, mem: np.ndarray):
+    def __init__(self, k: int, profile: int, n: int, regs: dict, mem: np.ndarray, parsed=None):
         super().__init__(n, regs)
-        self.prog, self.labels, self.tables = loop_statements(k, profile)
+        self.prog, self.labels, self.tables = parsed or loop_statements(k, profile)
         self.mem = mem
         self.hits = set()                  # jump-table entries taken
 
@@ -425,7 +429,7 @@ class Loop(Ptx):
                 if p is None or p[0]:
                     pc = self.labels[args[0]]
                 continue
-            if op == "brx.idx.uni":
+            if op in ("brx.idx.uni", "brx.idx"):
                 idx = self.val(args[0])
                 assert (idx == idx[0]).all(), "a jump that is not uniform"
                 target = self.tables[args[1]][int(idx[0])]
@@ -649,3 +653,34 @@ def test_whole_loop_against_the_oracle(oracle_lib, k, profile):
         if i >= len(progs) and hit >= reachable:
             break
         assert i < 400, sorted(reachable - hit)[:8]
+
+
+@pytest.mark.parametrize("k", G.KS)
+@pytest.mark.parametrize("profile", [0, 1])
+def test_cheap_tables(k, profile):
+    """The 32-bit micro-op interpreter's jump tables (CheapOps, dispatch 2 and
+    the no-allocation entry point): each single-instruction op of the
+    profile gives IEEE single-precision ADD/SUB/MUL and the 1.0/0.0 LT/GT
+    (false on NaN), per element."""
+    parsed = parse_asm(G.cheap_table(k, profile))
+    rng = np.random.default_rng(k + 10 * profile)
+    n = 64
+    a = [rng.standard_normal(n).astype(np.float32) * 10 for _ in range(k)]
+    b = [rng.standard_normal(n).astype(np.float32) * 10 for _ in range(k)]
+    for q in range(k):
+        a[q][:4] = np.float32([np.nan, 0.0, -0.0, np.inf])
+        b[q][2:6] = np.float32([0.0, np.nan, 1e-45, -np.inf])
+    want = {0: lambda x, y: x + y, 1: lambda x, y: x - y, 2: lambda x, y: x * y,
+            6: lambda x, y: np.where(x < y, np.float32(1), np.float32(0)),
+            7: lambda x, y: np.where(x > y, np.float32(1), np.float32(0))}
+    for op in G.PROFILES[profile]:
+        regs = {f"%{k}": np.full(n, op, np.uint32)}
+        regs.update({f"%{k + 1 + q}": _u(a[q]) for q in range(k)})
+        regs.update({f"%{2 * k + 1 + q}": _u(b[q]) for q in range(k)})
+        e = Loop(k, profile, n, regs, np.zeros(4, np.uint32), parsed=parsed)
+        e.execute()
+        for q in range(k):
+            with np.errstate(all="ignore"):
+                w = want[op](a[q], b[q]).astype(np.float32)
+            got = _f(e.r[f"%{q}"])
+            assert ((bits(got) == bits(w)) | (np.isnan(got) & np.isnan(w))).all(), (k, profile, op, q)
