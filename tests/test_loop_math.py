@@ -684,3 +684,54 @@ def test_cheap_tables(k, profile):
                 w = want[op](a[q], b[q]).astype(np.float32)
             got = _f(e.r[f"%{q}"])
             assert ((bits(got) == bits(w)) | (np.isnan(got) & np.isnan(w))).all(), (k, profile, op, q)
+
+
+@pytest.mark.parametrize("k", G.KS)
+@pytest.mark.parametrize("profile", [0, 1])
+def test_one_instruction_tables(k, profile):
+    """The trace interpreter's one-instruction tables (WideOps): every arm of
+    the profile, register and constant src2, and the broadcast arm, read the
+    operands from the shared-memory register file and store the IEEE result
+    (DIV: b != 0 ? a / b : 1.0) in the destination's slot."""
+    parsed = parse_asm(G.wide_ops(k, profile))
+    rng = np.random.default_rng(200 + k + 10 * profile)
+    V, S = min(k, 4), 128 * k
+    lanes = np.arange(32)
+    base = (lanes * V * 4).astype(np.uint32)
+
+    def words(slot):
+        return [(base.astype(np.int64) + slot * S + (e // V) * 128 * V + (e % V) * 4) // 4 for e in range(k)]
+
+    def div(x, y):
+        with np.errstate(all="ignore"):
+            return np.where(y != 0, x / y, np.float32(1.0)).astype(np.float32)
+
+    want = {0: lambda x, y: x + y, 1: lambda x, y: x - y, 2: lambda x, y: x * y, 3: div,
+            6: lambda x, y: np.where(x < y, np.float32(1), np.float32(0)),
+            7: lambda x, y: np.where(x > y, np.float32(1), np.float32(0))}
+    c = np.float32(-2.5)
+    for op in sorted(G.PROFILES[profile] + (3,)):
+        for const in (0, 1):
+            mem = np.zeros(4 * S // 4, np.uint32)
+            a = [rng.standard_normal(32).astype(np.float32) * 4 for _ in range(k)]
+            b = [rng.standard_normal(32).astype(np.float32) * 4 for _ in range(k)]
+            for q in range(k):
+                a[q][:3] = np.float32([0.0, -0.0, np.nan])
+                b[q][1:5] = np.float32([0.0, np.nan, -0.0, np.inf])
+                mem[words(1)[q]] = _u(a[q])
+                mem[words(2)[q]] = _u(b[q])
+            regs = {"%0": np.full(32, op | (const << 3), np.uint32), "%1": base + 1 * S, "%2": base + 2 * S,
+                    "%3": base + 3 * S, "%4": np.full(32, int(np.float32(c).view(np.uint32)), np.uint32)}
+            e = Loop(k, profile, 32, regs, mem, parsed=parsed)
+            e.execute()
+            for q in range(k):
+                with np.errstate(all="ignore"):
+                    w = want[op](a[q], np.full(32, c, np.float32) if const else b[q]).astype(np.float32)
+                got = _f(mem[words(3)[q]])
+                assert ((bits(got) == bits(w)) | (np.isnan(got) & np.isnan(w))).all(), (k, profile, op, const, q)
+    mem = np.zeros(4 * S // 4, np.uint32)
+    regs = {"%0": np.full(32, G.BCAST_OP | 8, np.uint32), "%1": base + S, "%2": base + 2 * S, "%3": base + 3 * S,
+            "%4": np.full(32, int(np.float32(c).view(np.uint32)), np.uint32)}
+    Loop(k, profile, 32, regs, mem, parsed=parsed).execute()
+    for q in range(k):
+        assert (_f(mem[words(3)[q]]) == c).all()
